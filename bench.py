@@ -1,0 +1,357 @@
+"""Benchmark of the per-timestep GRMHD update: zone-updates/s on the 3-D magnetised torus.
+
+A "step" is one full RK2 timestep (two advance() substeps with bounds and fixups) of the
+Fishbone-Moncrief torus on one grid.  Default workload: 384 x 192 x 128 zones (r, theta,
+phi), HLL, Toth flux-CT, mixed precision (FP32 reconstruction/HLL/CT, FP64 update and
+inversion), initial state built on the host (synthetic, seeded).  The plain FP64 device path
+is timed on the same grid beside it.
+
+Multi-GPU: the torus update does not shard in this build (one GPU per grid), so
+`--gpus N` runs N independent replicas, one per rank, and reports their aggregate.
+
+`--impl reference` times the CPU restatement of the reference algorithm (oracle/, OpenMP
+on all host cores) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+CONFIGS = {
+    # name: (n1, n2, n3, lim)
+    "torus3d_384x192x128": (384, 192, 128, 0),
+    "torus3d_256x128x64": (256, 128, 64, 0),
+    "torus3d_192x96x64": (192, 96, 64, 0),
+    "torus2d_128x128": (128, 128, 1, 0),
+}
+LIMNAME = {0: "mc", 1: "ppm", 2: "weno5"}
+METRIC = "zone-updates/s on 3D torus: learned+mixed vs plain FP64 GPU at L1 err≤1e-6"
+
+
+def bytes_per_zone_update(n3: int) -> float:
+    """Algorithmic HBM bytes of one zone-update of the full RK2 step: FP64 state traffic
+    322 B (substep 0: read P^n, write P^(n+1/2); substep 1: read P^n, P^(n+1/2), write
+    P^(n+1); two flag writes) plus the per-(i,j) metric tables (~1400 B per substep, reused
+    along phi) divided by n3."""
+    return 322.0 + 2800.0 / n3
+
+
+def update_kernel_bytes_per_cell(n3: int, precision: int) -> float:
+    """Algorithmic bytes of the update+inversion kernel per active cell: p_i, p_b (64 B
+    each), the five non-field fluxes of three directions and three EMFs (FP64: 8 B, mixed:
+    4 B each), p_f (64 B), the flag (1 B) and the CENT metric, connection and floors
+    (94 doubles per (i,j), reused along phi)."""
+    w = 8 if precision == 0 else 4
+    return 64 + 64 + 15 * w + 3 * w + 64 + 1 + 94 * 8 / n3
+
+
+def clock_sampler(stop: threading.Event, out: list, dev: int):
+    cmd = ["nvidia-smi", "-i", str(dev), "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+           "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+           "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+           "--format=csv,noheader,nounits", "-lms", "200"]
+    try:
+        p = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    except OSError:
+        return
+    try:
+        while not stop.is_set():
+            line = p.stdout.readline()
+            if not line:
+                break
+            out.append(line.strip())
+    finally:
+        p.terminate()
+        try:
+            p.wait(timeout=2)
+        except Exception:
+            p.kill()
+
+
+def summarize_clocks(lines: list) -> dict:
+    sm, mx, reasons = [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for ln in lines:
+        f = [x.strip() for x in ln.split(",")]
+        if len(f) < 7:
+            continue
+        try:
+            sm.append(float(f[0]))
+            mx.append(float(f[1]))
+        except ValueError:
+            continue
+        for nm, v in zip(names, f[3:7]):
+            if v.lower().startswith("active"):
+                reasons.add(nm)
+    return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+            "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "src": "measured"}
+    return {"hbm_gbs": 6650.0, "src": "fallback"}
+
+
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference(args, ws, rank):
+    """CPU baseline: the oracle restatement with OpenMP on all host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    from harm_harm_b200 import Grid
+    from oracle import oracle as O
+    n1, n2, n3, lim = CONFIGS[args.config]
+    sn3 = min(n3, args.cpu_sample_n3)
+    g = Grid.torus(n1, n2, sn3, lim=lim)
+    geom, conn, aux = g.geometry()
+    P = g.torus_init(geom, aux, seed=args.seed)
+    cores = os.cpu_count() or 1
+    orc = O.Oracle(g, geom, conn, aux, nthreads=cores)
+    orc.bound_prim(P)
+    F = [np.zeros_like(P) for _ in range(3)]
+    ndt = orc.fluxcalc(P, *F)
+    dt = 1.0 / sum(1.0 / x for x in ndt if x < 1e99)
+    for _ in range(args.warmup):
+        dt, _ = orc.step_ch(P, dt)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        dt, _ = orc.step_ch(P, dt)
+    el = time.perf_counter() - t0
+    zones = n1 * n2 * sn3
+    value = zones * args.steps / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "zone-updates/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Fishbone-Moncrief torus, host-built)",
+        "config": {"workload": args.config + f"_{LIMNAME[lim]}_hll_fluxct", "sample_n3": sn3},
+        "cpu_baseline": {"value": value, "unit": "zone-updates/s", "cores": cores, "kind": "port",
+                         "sample": f"{n1}x{n2}x{sn3} zones of the same torus, full RK2 steps, FP64"},
+        "e2e": {"value": value, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample(args, lim) -> dict:
+    """Bounded timing of the CPU port on a slab of the workload (for our own line)."""
+    from harm_harm_b200 import Grid
+    from oracle import oracle as O
+    n1, n2, n3, _ = CONFIGS[args.config]
+    sn3 = min(n3, 4)
+    g = Grid.torus(n1, n2, sn3, lim=lim)
+    geom, conn, aux = g.geometry()
+    P = g.torus_init(geom, aux, seed=args.seed)
+    cores = os.cpu_count() or 1
+    orc = O.Oracle(g, geom, conn, aux, nthreads=cores)
+    orc.bound_prim(P)
+    F = [np.zeros_like(P) for _ in range(3)]
+    ndt = orc.fluxcalc(P, *F)
+    dt = 1.0 / sum(1.0 / x for x in ndt if x < 1e99)
+    dt, _ = orc.step_ch(P, dt)
+    nst, t0 = 0, time.perf_counter()
+    while True:
+        dt, _ = orc.step_ch(P, dt)
+        nst += 1
+        el = time.perf_counter() - t0
+        if el > args.cpu_seconds or nst >= 50:
+            break
+    return {"value": n1 * n2 * sn3 * nst / el, "unit": "zone-updates/s", "cores": cores, "kind": "port",
+            "sample": f"{nst} RK2 steps of a {n1}x{n2}x{sn3} slab of the torus, FP64, OpenMP ({el:.1f} s)"}
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    from harm_harm_b200 import HARM_PREC_FP64, HARM_PREC_MIXED, Grid, Harm
+    torch.cuda.set_device(local)
+    n1, n2, n3, lim = CONFIGS[args.config]
+    g = Grid.torus(n1, n2, n3, lim=lim)
+    geom, conn, aux = g.geometry()
+    P0 = g.torus_init(geom, aux, seed=args.seed + rank)
+    dev = Harm(g, geom, conn, aux, device=local)
+    prec = HARM_PREC_MIXED if args.precision == "mixed" else HARM_PREC_FP64
+    Pd = torch.from_numpy(P0).cuda()
+    dev.bound_prim(Pd)
+    torch.cuda.synchronize()
+    # initial dt from the fluxes of the initial state
+    F = [torch.empty_like(Pd) for _ in range(3)]
+    ndt = dev.fluxcalc(Pd, *F)
+    del F
+    dt0 = 1.0 / sum(1.0 / x for x in ndt if x < 1e99)
+    stream = torch.cuda.ExternalStream(dev.stream_ptr)
+    zones = n1 * n2 * n3
+
+    def timed(precision, P, K, W):
+        dt = dt0
+        dt, _ = dev.step_ch(P, dt, precision=precision, nsteps=W, stats=False)
+        barrier(ws)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = dev.launches
+        e0.record(stream)
+        dt, st = dev.step_ch(P, dt, precision=precision, nsteps=K, stats=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(ws)
+        ms = e0.elapsed_time(e1)
+        return ms, st, dev.launches - l0
+
+    # plain FP64 path on the same grid
+    Pf = Pd.clone()
+    ms64, st64, _ = timed(HARM_PREC_FP64, Pf, max(1, args.steps // 2), args.warmup)
+    del Pf
+    # headline path, with clocks sampled during the timed region
+    stop, clines = threading.Event(), []
+    th = threading.Thread(target=clock_sampler, args=(stop, clines, local), daemon=True)
+    th.start()
+    Pm = Pd.clone()
+    ms, st, launches = timed(prec, Pm, args.steps, args.warmup)
+    stop.set()
+    th.join(timeout=5)
+    ms = max_over_ranks(ms, ws)
+    ms64 = max_over_ranks(ms64, ws)
+    value = ws * zones * args.steps / (ms * 1e-3)
+    value64 = ws * zones * max(1, args.steps // 2) / (ms64 * 1e-3)
+    # accuracy of the headline path against the FP64 path after the same steps
+    Pa, Pb = Pd.clone(), Pd.clone()
+    dev.step_ch(Pa, dt0, precision=HARM_PREC_FP64, nsteps=args.err_steps, stats=False)
+    dev.step_ch(Pb, dt0, precision=prec, nsteps=args.err_steps, stats=False)
+    act = (slice(None),) + g.active
+    a, b = Pa.cpu().numpy()[act], Pb.cpu().numpy()[act]
+    l1 = {nm: float(np.abs(a[pl] - b[pl]).mean() / max(np.abs(a[pl]).mean(), 1e-300))
+          for nm, pl in (("rho", 0), ("u", 1), ("B1", 5), ("B2", 6), ("B3", 7))}
+    del Pa, Pb
+    # stage times and roofline of the dominant kernel (update + inversion)
+    stages = dev.time_stages(Pm, dt0, precision=prec, reps=3)
+    peaks = measured_peaks()
+    upd_bytes = update_kernel_bytes_per_cell(n3, prec) * zones
+    ach = upd_bytes / (stages["update_invert"] * 1e-3) / 1e9
+    # end to end through the host-buffer entry point: H2D of P, step, D2H of P every step
+    Ph = torch.from_numpy(P0.copy()).pin_memory()
+    dev.step_ch_host(Ph.numpy(), dt0, precision=prec)
+    torch.cuda.synchronize()
+    ke = max(2, args.steps // 4)
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    dte = dt0
+    for _ in range(ke):
+        dte, _ = dev.step_ch_host(Ph.numpy(), dte, precision=prec)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall_e2e = time.perf_counter() - t0
+    ms_e2e = max(e0.elapsed_time(e1), 1e3 * wall_e2e)
+    ms_e2e = max_over_ranks(ms_e2e, ws)
+    e2e_value = ws * zones * ke / (ms_e2e * 1e-3)
+    pbytes = 8 * g.cells * 8
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(args, lim)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "zone-updates/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 flux / f64 update+inversion" if prec == HARM_PREC_MIXED else "f64",
+            "data": "synthetic (seeded Fishbone-Moncrief torus, host-built)",
+            "config": {"workload": f"{args.config}_{LIMNAME[lim]}_hll_fluxct_{args.precision}",
+                       "grid": [n1, n2, n3], "reconstruction": LIMNAME[lim], "riemann": "hll", "ct": "toth",
+                       "precision": args.precision, "guess": args.guess,
+                       "l2": "inputs larger than L2 (P is %.0f MB)" % (pbytes / 1e6),
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
+            "fp64_value": value64, "speedup_vs_fp64": value / value64,
+            "l1_rel_err_vs_fp64": l1, "l1_steps": args.err_steps,
+            "newton_iters_per_cell": st["newton_iters"] / max(st["cells_inverted"], 1.0),
+            "newton_iters_per_cell_fp64": st64["newton_iters"] / max(st64["cells_inverted"], 1.0),
+            "inversion_failures": st["inversion_failures"], "mlp_fallbacks": st["mlp_fallbacks"],
+            "stage_ms": stages,
+            "roofline": {"bound": "hbm", "kernel": "k_update (update + FP64 inversion)",
+                         "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": ach / peaks["hbm_gbs"],
+                         "peak_src": peaks["src"], "traffic": None,
+                         "algorithmic_bytes_per_cell": update_kernel_bytes_per_cell(n3, prec)},
+            "step_roofline": {"bytes_per_zone_update": bytes_per_zone_update(n3),
+                              "achieved_gbs": value / ws * bytes_per_zone_update(n3) / 1e9,
+                              "frac": value / ws * bytes_per_zone_update(n3) / 1e9 / peaks["hbm_gbs"]},
+            "e2e": {"value": e2e_value, "unit": "zone-updates/s", "h2d_bytes_per_step": pbytes,
+                    "d2h_bytes_per_step": pbytes},
+            "gpu_launches": launches,
+            "clocks": summarize_clocks(clines),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    dev.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="torus3d_384x192x128", choices=list(CONFIGS))
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--guess", default="prev", choices=["prev", "mlp"])
+    ap.add_argument("--seed", type=int, default=12345)
+    ap.add_argument("--err-steps", type=int, default=10)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-sample-n3", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    ws, rank, local = dist_init(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

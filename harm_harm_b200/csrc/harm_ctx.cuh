@@ -1,0 +1,43 @@
+// harm_ctx.cuh -- device context of libharm_b200.so (opaque to callers).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "harm_b200.h"
+
+struct harm_ctx {
+  harm_grid g;
+  int device;
+  cudaStream_t stream;
+  size_t plane, cells;
+  // metric tables (FP64, plus an FP32 copy for the mixed-precision flux path)
+  double* d_geom;
+  float* d_geomf;
+  double* d_conn;
+  double* d_aux;
+  // scratch of one substep
+  double* d_F[3];
+  float* d_Ff[3];
+  double* d_emf;
+  float* d_emff;
+  double* d_pk;     // midpoint primitives of the RK2 step
+  int8_t* d_pflag;  // inversion flags
+  void* d_fixrec;   // fixup records
+  unsigned int fix_cap;
+  // device scalars: dt slots, dt, ndt, stats, fixup counter
+  double* d_scal;
+  unsigned long long* d_dtslots;
+  double* d_dt;
+  double* d_ndt;
+  double* d_stats;
+  unsigned int* d_nrec;
+  double* h_scal;   // pinned host mirror
+  double* d_Pdev;   // device state used by the host-buffer entry point
+  // learned guess
+  float* d_mlp;        // inference parameters (BF16 packed as float words) + normalisation
+  float* d_mlp_master; // FP32 master parameters
+  float* d_mlp_adam;   // Adam moments
+  float* d_mlp_work;   // training workspace
+  size_t mlp_work_n;
+  int mlp_step;
+  unsigned long long launches;  // kernels launched by this context
+};

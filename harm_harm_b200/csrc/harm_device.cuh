@@ -1,0 +1,221 @@
+// harm_device.cuh -- per-point device physics of the GRMHD step (sm_100a).
+//
+// Templated on the arithmetic type T: the flux path (state, fluxes, wave speeds) runs in
+// T = float for the mixed-precision step and T = double for the FP64 step; the
+// conserved update, source terms and the inversion always run in double.
+//
+// Reference formulas (HARM, WHICHVEL=VELREL4, REMOVERESTMASSFROMUU=2, PRIMMAXWELL):
+//   ucon from relative 4-velocity ....... phys.tools.c:1900 (ucon_calc_rel4vel_fromuconrel)
+//   1+u_t ............................... phys.tools.c:1272 (compute_1plusud0_rel4vel)
+//   b^2 ................................. phys.tools.c:1392 (bsq_calc_fromq_rel4vel)
+//   fluxes / conserved .................. phys.tools.c:30, :1071, :1133, :392
+//   fast speeds ......................... vchar.c:34, simplefast vchar.c:260
+//   connection source ................... phys.c:132 (source_conn)
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "harm_b200.h"
+
+namespace hb {
+
+constexpr int NPR = HARM_NPR;
+
+// One metric record in registers.  Symmetric tensors as 10 entries 00,01,02,03,11,12,13,22,23,33.
+template <typename T>
+struct Geo {
+  T gcov[10], gcon[10];
+  T gcovpert_tt, alpha, betasqoalphasq, beta1, beta2, beta3, gdet, igdet;
+};
+
+__host__ __device__ constexpr int sym(int m, int n) {
+  return (m <= n) ? ((m == 0) ? n : (m == 1) ? 3 + n : (m == 2) ? 5 + n : 9)
+                  : ((n == 0) ? m : (n == 1) ? 3 + m : (n == 2) ? 5 + m : 9);
+}
+
+// Load a record from a plane-major table tab[field][plane] at 2-D offset c.
+template <typename T, typename S>
+__device__ __forceinline__ void load_geo(const S* __restrict__ tab, size_t plane, size_t c, Geo<T>& g) {
+#pragma unroll
+  for (int f = 0; f < 10; f++) g.gcov[f] = (T)__ldg(tab + (size_t)(HARM_G_GCOV + f) * plane + c);
+#pragma unroll
+  for (int f = 0; f < 10; f++) g.gcon[f] = (T)__ldg(tab + (size_t)(HARM_G_GCON + f) * plane + c);
+  g.gcovpert_tt = (T)__ldg(tab + (size_t)HARM_G_GCOVPERT_TT * plane + c);
+  g.alpha = (T)__ldg(tab + (size_t)HARM_G_ALPHA * plane + c);
+  g.betasqoalphasq = (T)__ldg(tab + (size_t)HARM_G_BETASQOALPHASQ * plane + c);
+  g.beta1 = (T)__ldg(tab + (size_t)(HARM_G_BETA + 0) * plane + c);
+  g.beta2 = (T)__ldg(tab + (size_t)(HARM_G_BETA + 1) * plane + c);
+  g.beta3 = (T)__ldg(tab + (size_t)(HARM_G_BETA + 2) * plane + c);
+  g.gdet = (T)__ldg(tab + (size_t)HARM_G_GDET * plane + c);
+  g.igdet = (T)__ldg(tab + (size_t)HARM_G_IGDET * plane + c);
+}
+
+template <typename T>
+struct State {
+  T ucon[4], ucov[4], bsq, pressure, plus1ud0, gamma, qsq;
+};
+
+template <typename T>
+__device__ __forceinline__ void lower(const T* u, const Geo<T>& g, T* d) {
+  d[0] = g.gcov[0] * u[0] + g.gcov[1] * u[1] + g.gcov[2] * u[2] + g.gcov[3] * u[3];
+  d[1] = g.gcov[1] * u[0] + g.gcov[4] * u[1] + g.gcov[5] * u[2] + g.gcov[6] * u[3];
+  d[2] = g.gcov[2] * u[0] + g.gcov[5] * u[1] + g.gcov[7] * u[2];
+  d[3] = g.gcov[3] * u[0] + g.gcov[6] * u[1] + g.gcov[9] * u[3];
+}
+template <typename T>
+__device__ __forceinline__ void raise(const T* d, const Geo<T>& g, T* u) {
+  u[0] = g.gcon[0] * d[0] + g.gcon[1] * d[1] + g.gcon[2] * d[2] + g.gcon[3] * d[3];
+  u[1] = g.gcon[1] * d[0] + g.gcon[4] * d[1] + g.gcon[5] * d[2] + g.gcon[6] * d[3];
+  u[2] = g.gcon[2] * d[0] + g.gcon[5] * d[1] + g.gcon[7] * d[2] + g.gcon[8] * d[3];
+  u[3] = g.gcon[3] * d[0] + g.gcon[6] * d[1] + g.gcon[8] * d[2] + g.gcon[9] * d[3];
+}
+
+template <typename T>
+__device__ __forceinline__ T qsq_of(const T* pr, const Geo<T>& g) {
+  T u1 = pr[HARM_U1], u2 = pr[HARM_U2], u3 = pr[HARM_U3];
+  return g.gcov[4] * u1 * u1 + g.gcov[7] * u2 * u2 + g.gcov[9] * u3 * u3 +
+         T(2.) * (g.gcov[5] * u1 * u2 + g.gcov[6] * u1 * u3);
+}
+
+template <typename T>
+__device__ __forceinline__ void ucon_of(const T* pr, const Geo<T>& g, T* ucon, T& gamma, T& qsq) {
+  T q = qsq_of(pr, g);
+  q = (q >= T(0)) ? q : T(0);
+  qsq = q;
+  gamma = sqrt(T(1) + q);
+  ucon[0] = gamma / g.alpha;
+  ucon[1] = pr[HARM_U1] - ucon[0] * g.beta1;
+  ucon[2] = pr[HARM_U2] - ucon[0] * g.beta2;
+  ucon[3] = pr[HARM_U3] - ucon[0] * g.beta3;
+}
+
+// B^i B_i and B^i u_i
+template <typename T>
+__device__ __forceinline__ void bdots(const T* pr, const Geo<T>& g, const T* ucov, T* Bcov, T& Bsq, T& udotB) {
+  const T B1 = pr[HARM_B1], B2 = pr[HARM_B2], B3 = pr[HARM_B3];
+  Bcov[0] = B1 * g.gcov[1] + B2 * g.gcov[2] + B3 * g.gcov[3];
+  Bcov[1] = B1 * g.gcov[4] + B2 * g.gcov[5] + B3 * g.gcov[6];
+  Bcov[2] = B1 * g.gcov[5] + B2 * g.gcov[7] + B3 * g.gcov[8];
+  Bcov[3] = B1 * g.gcov[6] + B2 * g.gcov[8] + B3 * g.gcov[9];
+  Bsq = B1 * Bcov[1] + B2 * Bcov[2] + B3 * Bcov[3];
+  udotB = B1 * ucov[1] + B2 * ucov[2] + B3 * ucov[3];
+}
+
+template <typename T>
+__device__ __forceinline__ void get_state(const T* pr, const Geo<T>& g, T gam, State<T>& q) {
+  ucon_of(pr, g, q.ucon, q.gamma, q.qsq);
+  lower(q.ucon, g, q.ucov);
+  T ud0tilde = pr[HARM_U1] * g.gcov[1] + pr[HARM_U2] * g.gcov[2] + pr[HARM_U3] * g.gcov[3];
+  T alphasq = g.alpha * g.alpha;
+  q.plus1ud0 = ud0tilde + (g.gcovpert_tt - alphasq * (g.betasqoalphasq + q.qsq)) / (T(1) + q.gamma * g.alpha);
+  T Bcov[4], Bsq, udotB;
+  bdots(pr, g, q.ucov, Bcov, Bsq, udotB);
+  q.bsq = (Bsq + udotB * udotB) / (q.ucon[0] * q.ucon[0]);
+  q.pressure = (gam - T(1)) * pr[HARM_UU];
+}
+
+// Flux in direction dir (0 = conserved variables), times gd (sqrt(-g) for UEVOLVE, 1 for
+// geometry-free U).
+template <typename T>
+__device__ __forceinline__ void primtoflux(const T* pr, const State<T>& q, int dir, const Geo<T>& g, T gd, T* F) {
+  const T rho = pr[HARM_RHO], u = pr[HARM_UU], P = q.pressure, w = P + rho + u;
+  const T ud = q.ucon[dir];
+  T ma[4], em[4];
+  ma[0] = (P + u) * ud * q.ucov[0] + rho * ud * q.plus1ud0;
+  ma[1] = w * ud * q.ucov[1];
+  ma[2] = w * ud * q.ucov[2];
+  ma[3] = w * ud * q.ucov[3];
+  ma[dir] += P;
+  T Bcov[4], Bsq, udotB;
+  bdots(pr, g, q.ucov, Bcov, Bsq, udotB);
+  const T Bd = (dir == 0) ? T(0) : pr[HARM_B1 + dir - 1];
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++)
+    em[mu] = Bsq * ud * q.ucov[mu] - Bd * Bcov[mu] - udotB * (Bd * q.ucov[mu] + Bcov[mu] * ud);
+  em[dir] += T(0.5) * (Bsq + udotB * udotB);
+  const T ig2 = T(1) / (q.ucon[0] * q.ucon[0]);
+  F[HARM_RHO] = rho * ud * gd;
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++) F[HARM_UU + mu] = (ma[mu] + em[mu] * ig2) * gd;
+  if (dir > 0) {
+    F[HARM_B1] = ((pr[HARM_B1] * ud - Bd * q.ucon[1]) / q.ucon[0]) * gd;
+    F[HARM_B2] = ((pr[HARM_B2] * ud - Bd * q.ucon[2]) / q.ucon[0]) * gd;
+    F[HARM_B3] = ((pr[HARM_B3] * ud - Bd * q.ucon[3]) / q.ucon[0]) * gd;
+  } else {
+    F[HARM_B1] = pr[HARM_B1] * gd;
+    F[HARM_B2] = pr[HARM_B2] * gd;
+    F[HARM_B3] = pr[HARM_B3] * gd;
+  }
+}
+
+template <typename T>
+struct Eps;
+template <>
+struct Eps<double> {
+  static constexpr double eps = 2.220446049250313e-16, small = 1e-300;
+};
+template <>
+struct Eps<float> {
+  static constexpr float eps = 1.1920929e-07f, small = 1e-35f;
+};
+
+// vchar + simplefast (USESASHAREWRITE form of the discriminant)
+template <typename T>
+__device__ __forceinline__ void vchar(const T* pr, const State<T>& q, int dir, const Geo<T>& g, T gam, T& vmax, T& vmin) {
+  T rho = pr[HARM_RHO], u = pr[HARM_UU];
+  if (u < T(0)) u = T(0);
+  if (rho < T(0)) rho = Eps<T>::small;
+  T P = q.pressure, WW = rho + u + P, cs2;
+  if (WW > T(0)) {
+    T pp = (gam - T(1)) * u, h = rho + u + pp;
+    cs2 = gam * pp / h;
+  } else {
+    WW = cs2 = Eps<T>::small;
+  }
+  if (cs2 >= T(1)) cs2 = T(1) - Eps<T>::eps * T(10);
+  else if (cs2 <= T(0)) cs2 = Eps<T>::small;
+  T EF = Eps<T>::small + fabs(q.bsq + WW);
+  T va2 = q.bsq / EF;
+  T cms2 = cs2 + va2 - cs2 * va2;
+  if (cms2 < T(0) && cms2 / (cs2 + va2) > -Eps<T>::eps * T(100)) cms2 = T(0);
+  if (cms2 > T(1) && (cms2 < T(1) + Eps<T>::eps * T(100) || rho < T(0))) cms2 = T(1);
+  const T Asq = g.gcon[sym(dir, dir)], Bsq = g.gcon[0], AB = g.gcon[dir];
+  const T Au = q.ucon[dir], Bu = q.ucon[0];
+  const T Au2 = Au * Au, Bu2 = Bu * Bu, AuBu = Au * Bu;
+  const T B = T(2) * (AuBu * (T(1) - cms2) - AB * cms2);
+  const T A = Bu2 * (T(1) - cms2) - Bsq * cms2;
+  T discr = T(4) * cms2 * ((AB * AB - Asq * Bsq) * cms2 + (T(2) * AB * Au * Bu - Asq * Bu2 - Bsq * Au2) * (cms2 - T(1)));
+  if (discr < T(0)) discr = T(0);
+  discr = sqrt(discr);
+  const T vm = -(-B + discr) / (T(2) * A), vp = -(-B - discr) / (T(2) * A);
+  if (vp < vm) { vmax = vm; vmin = vp; }
+  else { vmax = vp; vmin = vm; }
+}
+
+// limit_gamma (fixup.c:2723).  Returns true if the velocity was rescaled.
+template <typename T>
+__device__ __forceinline__ bool limit_gamma(T gammamax, T* pr, const Geo<T>& g) {
+  if (gammamax <= T(1)) return false;
+  T q = qsq_of(pr, g);
+  q = (q >= T(0)) ? q : T(0);
+  T gamma = sqrt(T(1) + q);
+  if (gamma > gammamax && gamma != T(1)) {
+    T pref = (gammamax * gammamax - T(1)) / (gamma * gamma - T(1));
+    if (pref < T(0)) return false;
+    T f = sqrt(pref);
+    pr[HARM_U1] *= f;
+    pr[HARM_U2] *= f;
+    pr[HARM_U3] *= f;
+    return true;
+  }
+  return false;
+}
+
+// MINMOD-limited MC slope (interppoint.c:753-775)
+template <typename T>
+__device__ __forceinline__ T mc_slope(T yl, T yc, T yr) {
+  T Dqm = T(2) * (yc - yl), Dqp = T(2) * (yr - yc), Dqc = T(0.5) * (yr - yl);
+  T m1 = (Dqm * Dqp <= T(0)) ? T(0) : ((fabs(Dqm) < fabs(Dqp)) ? Dqm : Dqp);
+  return (Dqc * m1 <= T(0)) ? T(0) : ((fabs(Dqc) < fabs(m1)) ? Dqc : m1);
+}
+
+}  // namespace hb

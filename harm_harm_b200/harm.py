@@ -1,0 +1,175 @@
+"""Host-side mirror of HARM's per-timestep interface over the B200 device path.
+
+The names follow the reference's entry points so that a caller of HARM's hot path finds
+the same operations:
+
+    Grid / geometry / torus_init   set_points+set_grid+init (coord.c:2038, set_grid.c:114,
+                                   initboundcode/init.fishmon.c:403)
+    Harm.bound_prim                bound_prim (step_ch.c:1332)
+    Harm.fluxcalc                  fluxcalc (flux.c:38)
+    Harm.advance                   advance (advance.c:85)
+    Harm.post_fixup                post_fixup (fixup.c:53)
+    Harm.Utoprimgen                Utoprimgen (utoprimgen.c:32), over a batch of points
+    Harm.step_ch                   step_ch_full (step_ch.c:35): one full RK2 step
+
+Device arrays are torch CUDA tensors (torch is only the allocator and stream owner here);
+every numeric routine runs in libharm_b200.so.  Errors are raised as RuntimeError with the
+library's message (HARM's MYFUN/FAILSTATEMENT convention of non-zero returns).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+
+RK2_CUF = ((1.0, 0.0, 0.5, 0.0), (1.0, 0.0, 1.0, 0.0))   # setup_rktimestep step_ch.c:1244-1266
+RK2_CUNEW = ((0.0, 0.0, 0.0, 0.0), (0.0, 0.0, 1.0, 0.5))
+
+
+def _ptr(a) -> int:
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    raise TypeError(type(a))
+
+
+@dataclass
+class Grid:
+    g: N.harm_grid
+
+    @classmethod
+    def torus(cls, n1: int, n2: int, n3: int, lim: int = N.HARM_LIM_MC, a: float = 0.9375,
+              hslope: float = 0.3, Rout: float = 40.0, cour: float = 0.8) -> "Grid":
+        g = N.harm_grid()
+        rc = N.host_lib().harm_grid_setup(C.byref(g), n1, n2, n3, lim, a, hslope, Rout, cour)
+        if rc:
+            raise RuntimeError(f"harm_grid_setup failed ({rc})")
+        return cls(g)
+
+    @property
+    def shape(self):
+        return (N.HARM_NPR, self.g.n3e, self.g.n2e, self.g.n1e)
+
+    @property
+    def cells(self) -> int:
+        return self.g.n1e * self.g.n2e * self.g.n3e
+
+    @property
+    def active(self):
+        """slices of the active cells in a [pl][k][j][i] array"""
+        g = self.g
+        return (slice(g.ng3, g.ng3 + g.n3), slice(g.ng, g.ng + g.n2), slice(g.ng, g.ng + g.n1))
+
+    def geometry(self):
+        g = self.g
+        plane = g.n1e * g.n2e
+        geom = np.zeros((N.HARM_NLOC, N.HARM_NGF, g.n2e, g.n1e))
+        conn = np.zeros((64, g.n2e, g.n1e))
+        aux = np.zeros((N.HARM_NAUX, g.n2e, g.n1e))
+        rc = N.host_lib().harm_geometry_build(C.byref(g), _ptr(geom), _ptr(conn), _ptr(aux))
+        if rc:
+            raise RuntimeError("harm_geometry_build failed")
+        assert geom.size == N.HARM_NLOC * N.HARM_NGF * plane
+        return geom, conn, aux
+
+    def torus_init(self, geom, aux, beta_min: float = 100.0, seed: int = 12345) -> np.ndarray:
+        P = np.zeros(self.shape)
+        rc = N.host_lib().harm_torus_init(C.byref(self.g), _ptr(geom), _ptr(aux), beta_min, seed, _ptr(P))
+        if rc:
+            raise RuntimeError(f"harm_torus_init failed ({rc})")
+        return P
+
+
+class Harm:
+    """One grid on one GPU: the device context of libharm_b200.so."""
+
+    def __init__(self, grid: Grid, geom: np.ndarray, conn: np.ndarray, aux: np.ndarray, device: int = 0):
+        self.grid = grid
+        self.lib = N.device_lib()
+        self._ctx = C.c_void_p()
+        geom = np.ascontiguousarray(geom, dtype=np.float64)
+        conn = np.ascontiguousarray(conn, dtype=np.float64)
+        aux = np.ascontiguousarray(aux, dtype=np.float64)
+        rc = self.lib.harm_b200_create(C.byref(grid.g), _ptr(geom), _ptr(conn), _ptr(aux), device,
+                                       C.byref(self._ctx))
+        self._check(rc, "harm_b200_create")
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc:
+            raise RuntimeError(f"{what} failed ({rc}): {self.lib.harm_b200_last_error().decode()}")
+
+    def close(self) -> None:
+        if self._ctx:
+            self.lib.harm_b200_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.harm_b200_launch_count(self._ctx))
+
+    @property
+    def stream_ptr(self) -> int:
+        return self.lib.harm_b200_stream(self._ctx)
+
+    # ---------------------------------------------------------------- reference API
+    def bound_prim(self, P) -> None:
+        self._check(self.lib.harm_b200_bound(self._ctx, _ptr(P)), "bound_prim")
+
+    def fluxcalc(self, pb, F1, F2, F3, precision: int = N.HARM_PREC_FP64):
+        ndt = (C.c_double * 3)()
+        self._check(self.lib.harm_b200_fluxcalc(self._ctx, precision, _ptr(pb), _ptr(F1), _ptr(F2), _ptr(F3), ndt),
+                    "fluxcalc")
+        return tuple(ndt)
+
+    def advance(self, timeorder: int, pi, pb, pf, pflag, dt: float, precision: int = N.HARM_PREC_FP64,
+                guess: int = N.HARM_GUESS_PREV, numtimeorders: int = 2):
+        CUf = (C.c_double * 4)(*RK2_CUF[timeorder])
+        Cun = (C.c_double * 4)(*RK2_CUNEW[timeorder])
+        ndt = C.c_double()
+        st = N.harm_stats()
+        self._check(self.lib.harm_b200_advance(self._ctx, precision, guess, timeorder, numtimeorders, _ptr(pi), _ptr(pb),
+                                               _ptr(pf), _ptr(pflag), dt, CUf, Cun, C.byref(ndt), C.byref(st)),
+                    "advance")
+        return ndt.value, st.as_dict()
+
+    def post_fixup(self, pf, pflag) -> None:
+        self._check(self.lib.harm_b200_post_fixup(self._ctx, _ptr(pf), _ptr(pflag)), "post_fixup")
+
+    def step_ch(self, P, dt: float, precision: int = N.HARM_PREC_FP64, guess: int = N.HARM_GUESS_PREV,
+                nsteps: int = 1, stats: bool = True):
+        d = C.c_double(dt)
+        st = N.harm_stats()
+        self._check(self.lib.harm_b200_step_n(self._ctx, precision, guess, _ptr(P), nsteps, C.byref(d),
+                                              C.byref(st) if stats else None), "step_ch")
+        return d.value, st.as_dict()
+
+    def step_ch_host(self, P_host: np.ndarray, dt: float, precision: int = N.HARM_PREC_FP64,
+                     guess: int = N.HARM_GUESS_PREV):
+        d = C.c_double(dt)
+        st = N.harm_stats()
+        self._check(self.lib.harm_b200_step_host(self._ctx, precision, guess, _ptr(P_host), C.byref(d), C.byref(st)),
+                    "step_ch_host")
+        return d.value, st.as_dict()
+
+    def Utoprimgen(self, U, geomrec, P, pflag, iters=None, guess: int = N.HARM_GUESS_PREV) -> None:
+        n = U.shape[-1]
+        self._check(self.lib.harm_b200_utoprimgen_points(self._ctx, n, guess, _ptr(U), _ptr(geomrec), _ptr(P),
+                                                         _ptr(pflag), _ptr(iters)), "Utoprimgen")
+
+    def time_stages(self, P, dt: float, precision: int = N.HARM_PREC_FP64, guess: int = N.HARM_GUESS_PREV,
+                    reps: int = 5) -> dict:
+        ms = (C.c_double * 5)()
+        self._check(self.lib.harm_b200_time_stages(self._ctx, precision, guess, _ptr(P), dt, reps, ms), "time_stages")
+        return dict(zip(("flux", "emf", "update_invert", "bound", "post_fixup"), list(ms)))

@@ -1,0 +1,224 @@
+/*
+ * harm_b200.h -- C ABI of the B200 implementation of HARM's per-timestep GRMHD update.
+ *
+ * Two shared libraries implement this header:
+ *   libharm_host.so  host-side producers of the inputs (grid, metric tables, torus
+ *                    initial state).  In HARM these are set_grid() (set_grid.c:114),
+ *                    set_connection() (set_grid.c:1033) and init() (initbase.c:7).
+ *   libharm_b200.so  the device path: reconstruction (MC / PPM / WENO5), HLL fluxes,
+ *                    flux-CT, conserved update with connection sources, Utoprimgen
+ *                    Newton inversion and floors/fixups, boundary conditions, and the
+ *                    learned initial-guess network.  Every numeric routine of the
+ *                    step runs on the GPU; there is no CPU fallback in this library.
+ *
+ * Conventions (shared by every entry point):
+ *   - Primitive order RHO,UU,U1,U2,U3,B1,B2,B3 (global.nondepnmemonics.h:883-890);
+ *     U1..U3 are the relative 4-velocity \tilde u^i (WHICHVEL=VELREL4), B^i = *F^{it}.
+ *   - State arrays are structure-of-arrays FP64: P[pl][k][j][i] with i fastest, over the
+ *     extended grid n1e x n2e x n3e (ghost zones included).  Index (i,j,k) of an active
+ *     cell maps to (i+ng, j+ng, k+ng3) with ng3 = (n3>1 ? ng : 0).
+ *   - Conserved arrays U[pl][k][j][i] are in HARM's UEVOLVE form: sqrt(-g) times
+ *     (rho u^t, T^t_t + rho u^t, T^t_i, B^i)  (REMOVERESTMASSFROMUU=2, phys.tools.c:1071).
+ *   - Flux arrays F1/F2/F3[pl][k][j][i]: F_d at index i lives on the lower face of cell i
+ *     in direction d (flux.c:852 "face" convention; dU = -(F[i+1]-F[i])/dx).
+ *   - The Kerr-Schild metric in modified Kerr-Schild coordinates does not depend on x3,
+ *     so metric tables are stored per (i,j) only: geom[loc][field][j][i] over n2e x n1e.
+ *     FACE3 shares CENT, CORN1 shares FACE2, CORN2 shares FACE1 (HARM stores all eight
+ *     locations per (i,j,k): superdefs.h:382).
+ *   - Return value: 0 on success, >0 on error (HARM's MYFUN convention,
+ *     global.variousmacros.h:43).  Per-cell inversion failures are not return codes;
+ *     they are written to an int8 pflag array with HARM's codes
+ *     (global.nondepnmemonics.h:824-844).
+ */
+#ifndef HARM_B200_H
+#define HARM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HARM_B200_ABI_VERSION 1
+
+/* primitive / conserved indices */
+#define HARM_NPR 8
+enum { HARM_RHO = 0, HARM_UU = 1, HARM_U1 = 2, HARM_U2 = 3, HARM_U3 = 4,
+       HARM_B1 = 5, HARM_B2 = 6, HARM_B3 = 7 };
+
+/* reconstruction choices (HARM lim[]: MC, PARA, WENO5BND; init.tools.c:128) */
+enum { HARM_LIM_MC = 0, HARM_LIM_PARA = 1, HARM_LIM_WENO5 = 2 };
+
+/* arithmetic of the flux path: FP64 everywhere, or FP32 reconstruction/HLL/CT with the
+   conserved update, inversion and metric kept in FP64 */
+enum { HARM_PREC_FP64 = 0, HARM_PREC_MIXED = 1 };
+
+/* initial guess of the Newton inversion: the previous primitive (set_guess_Wp,
+   utoprim_jon.c:890) or the learned network with fallback to the previous primitive */
+enum { HARM_GUESS_PREV = 0, HARM_GUESS_MLP = 1 };
+
+/* metric table locations (per (i,j)) */
+enum { HARM_LOC_CENT = 0, HARM_LOC_FACE1 = 1, HARM_LOC_FACE2 = 2, HARM_LOC_CORN3 = 3,
+       HARM_NLOC = 4 };
+
+/* fields of one metric table location (struct of_compgeom, global.structs.h:20-85).
+   Symmetric 4x4 tensors are stored as 10 entries in the order
+   00,01,02,03,11,12,13,22,23,33. */
+enum {
+  HARM_G_GCOV = 0,            /* 10 entries g_{mu nu} */
+  HARM_G_GCON = 10,           /* 10 entries g^{mu nu} */
+  HARM_G_GCOVPERT_TT = 20,    /* g_tt + 1 (gcovpert[TT]) */
+  HARM_G_ALPHA = 21,          /* lapse 1/sqrt(-g^{tt}) (metric.tools.c:1250) */
+  HARM_G_BETASQOALPHASQ = 22, /* sum_j g_{tj} g^{tj} (metric.tools.c:1260) */
+  HARM_G_BETA = 23,           /* 3 entries beta^j = g^{tj} alpha^2 (metric.tools.c:1275) */
+  HARM_G_GDET = 26,           /* sqrt(-g) */
+  HARM_G_IGDET = 27,          /* sign(gdet)/(|gdet|+SMALL) (metric.tools.c:1195) */
+  HARM_NGF = 28
+};
+
+/* per-(i,j) auxiliary table at CENT: Boyer-Lindquist r and the two density floors
+   (set_density_floors_default, rescaletype 0: fixup.c:2485-2486) */
+enum { HARM_AUX_R = 0, HARM_AUX_RHOFLOOR = 1, HARM_AUX_UFLOOR = 2, HARM_NAUX = 3 };
+
+/* inversion failure codes (global.nondepnmemonics.h:824-844) */
+enum {
+  HARM_UTOPRIMFAILFIXEDCOLD = -3, HARM_UTOPRIMFAILFIXEDUTOPRIM = -1,
+  HARM_UTOPRIMNOFAIL = 0, HARM_UTOPRIMFAILCONV = 1, HARM_UTOPRIMFAILCONVW = 2,
+  HARM_UTOPRIMFAILCONVUTSQ = 3, HARM_UTOPRIMFAILCONVGUESSUTSQ = 4,
+  HARM_UTOPRIMFAILCONVUTSQVERYBAD = 5, HARM_UTOPRIMFAILNANGUESS = 7,
+  HARM_UTOPRIMFAILNANRESULT = 8, HARM_UTOPRIMFAILRHONEG = 9, HARM_UTOPRIMFAILUNEG = 10,
+  HARM_UTOPRIMFAILRHOUNEG = 11, HARM_UTOPRIMFAILU2AVG1 = 14, HARM_UTOPRIMFAILU2AVG2 = 15,
+  HARM_UTOPRIMFAILCONVRET = 50
+};
+
+/* Run-time configuration of one grid (the globals HARM's hot path reads:
+   defs.general.h, superdefs.h).  Filled by harm_grid_setup(). */
+typedef struct harm_grid {
+  int n1, n2, n3;          /* active cells */
+  int ng;                  /* ghost cells per side (MAXBND) */
+  int n1e, n2e, n3e;       /* extended sizes */
+  int ng3;                 /* ghost cells in x3: ng if n3>1 else 0 */
+  int lim;                 /* HARM_LIM_* */
+  int pad0;
+  double startx[4], dx[4]; /* x^mu of the lower corner of active cell (0,0,0), spacings */
+  double a;                /* black-hole spin */
+  double hslope, R0, Rin, Rout, Rhor;
+  double gam;              /* ideal-gas adiabatic index */
+  double cour;             /* Courant factor */
+  double defcon, safe;     /* dt = defcon*wavedt, dt <= safe*dt_old (initbase.c:1029-1031) */
+  double rho_floor_coef;   /* prfloorcoef[RHO] */
+  double u_floor_coef;     /* prfloorcoef[UU] */
+  double gammamax;         /* GAMMAMAX (initbase.c:1178) */
+  double gammafail;        /* GAMMAFAIL = 100 GAMMAMAX */
+} harm_grid;
+
+/* Counters accumulated by the device step (the reference's nstroke and debug counters). */
+typedef struct harm_stats {
+  double newton_iters;     /* sum over inverted cells of Newton iterations (nstroke) */
+  double cells_inverted;   /* number of cell inversions */
+  double mlp_fallbacks;    /* cells whose learned guess failed and were re-solved */
+  double inversion_failures; /* cells whose final pflag was a failure before fixup */
+  double floor_hits;       /* cells where fixup1zone raised rho or u */
+} harm_stats;
+
+/* ------------------------------------------------------------------------------------
+ * libharm_host.so : input producers (host C)
+ * ------------------------------------------------------------------------------------ */
+
+/* Fill a harm_grid for the modified-Kerr-Schild torus grid (LOGRSINTH coordinates,
+   coord.c:930 and set_points coord.c:2038; Rin from setRin(setihor()), coord.c:2334-2359).
+   Returns 0, or 1 on bad sizes. */
+int harm_grid_setup(harm_grid *g, int n1, int n2, int n3, int lim, double a,
+                    double hslope, double Rout, double cour);
+
+/* Metric tables at CENT/FACE1/FACE2/CORN3 per (i,j): geom[HARM_NLOC][HARM_NGF][n2e][n1e];
+   connection at CENT conn[64][n2e][n1e] with conn[(k*4+l)*4+j] = Gamma^k_{l j}
+   (HARM conn[i][j][k][k][l][j], superdefs.h:423); aux[HARM_NAUX][n2e][n1e]. */
+int harm_geometry_build(const harm_grid *g, double *geom, double *conn, double *aux);
+
+/* Fishbone-Moncrief torus with a single poloidal loop, normalised to beta_min, internal
+   energy perturbed by (1+0.04(U-1/2)) from `seed`; atmosphere at the floors.
+   Writes P[8][n3e][n2e][n1e] (active cells; ghost zones are left to harm_b200_bound). */
+int harm_torus_init(const harm_grid *g, const double *geom, const double *aux,
+                    double beta_min, uint64_t seed, double *P);
+
+/* ------------------------------------------------------------------------------------
+ * libharm_b200.so : device path
+ * ------------------------------------------------------------------------------------ */
+
+typedef struct harm_ctx harm_ctx;
+
+/* Create a context on CUDA device `device`: uploads the metric tables (once, as
+   set_grid does once) and allocates the scratch of the step (fluxes, EMFs, U arrays).
+   The caller owns the primitive arrays. */
+int harm_b200_create(const harm_grid *g, const double *geom_h, const double *conn_h,
+                     const double *aux_h, int device, harm_ctx **out);
+int harm_b200_destroy(harm_ctx *ctx);
+
+/* CUDA stream the context launches on (cudaStream_t as void*). */
+void *harm_b200_stream(harm_ctx *ctx);
+
+/* Number of kernels this context has launched so far. */
+unsigned long long harm_b200_launch_count(harm_ctx *ctx);
+
+/* bound_prim() (step_ch.c:1332, bounds.fishmon.c): fill the ghost zones of d_P:
+   x1 outflow (inner free, outer no-inflow), x2 polar axis, x3 periodic. */
+int harm_b200_bound(harm_ctx *ctx, double *d_P);
+
+/* fluxcalc() (flux.c:38): reconstruct d_pb at faces, HLL fluxes, Toth flux-CT.
+   Writes d_F1/d_F2/d_F3 (UEVOLVE form) and ndt[3] = cour*dx/ctop minimised per
+   direction (host array). */
+int harm_b200_fluxcalc(harm_ctx *ctx, int precision, const double *d_pb,
+                       double *d_F1, double *d_F2, double *d_F3, double ndt[3]);
+
+/* advance() (advance.c:85 -> advance_standard advance.c:140) for one RK substep:
+   fluxes of d_pb, U_i = primtoU(d_pi), source(d_pb), U_f = CUf0 U_i + CUf1 U_f +
+   CUf2 dt dU, ucum, then Utoprimgen (utoprimgen.c:32) into d_pf with d_pb as guess,
+   then fixup1zone (fixup.c:561).  ndt = defcon*wavedt (prepare_globaldt advance.c:1558).
+   d_pflag[k][j][i] (active and ghost layout of P) receives the inversion codes. */
+int harm_b200_advance(harm_ctx *ctx, int precision, int guess, int timeorder,
+                      int numtimeorders, const double *d_pi, const double *d_pb,
+                      double *d_pf, int8_t *d_pflag, double dt, const double CUf[4],
+                      const double Cunew[4], double *ndt, harm_stats *stats);
+
+/* post_fixup() (fixup.c:53 -> fixup_utoprim fixup.c:1061): replace failed-inversion
+   cells by the average of their successful neighbours, then limit_gamma. */
+int harm_b200_post_fixup(harm_ctx *ctx, double *d_pf, int8_t *d_pflag);
+
+/* One full RK2 step (step_ch_full step_ch.c:35 with TIMEORDER=2, setup_rktimestep
+   step_ch.c:1244-1266): two advance() substeps, each followed by bound, post_fixup,
+   bound; then dt <- min(ndt, safe*dt) (post_stepch step_ch.c:213).  d_P is updated in
+   place; *dt is the step used on input and the next step on output. */
+int harm_b200_step(harm_ctx *ctx, int precision, int guess, double *d_P, double *dt,
+                   harm_stats *stats);
+
+/* nsteps full steps back to back with dt kept on the device between steps (one host
+   synchronisation at the end).  *dt in: first step; out: the next step. */
+int harm_b200_step_n(harm_ctx *ctx, int precision, int guess, double *d_P, int nsteps,
+                     double *dt, harm_stats *stats);
+
+/* Same step over a HOST primitive array: copies h_P in, steps, copies it back. */
+int harm_b200_step_host(harm_ctx *ctx, int precision, int guess, double *h_P, double *dt,
+                        harm_stats *stats);
+
+/* Utoprimgen() (utoprimgen.c:32) over n independent points: d_U[8][n] in UEVOLVE form,
+   d_geom[HARM_NGF][n] CENT metric of each point, d_P[8][n] guess in / primitives out,
+   d_pflag[n] codes out, d_iters[n] Newton iterations out (may be NULL). */
+int harm_b200_utoprimgen_points(harm_ctx *ctx, size_t n, int guess, const double *d_U,
+                                const double *d_geom, double *d_P, int8_t *d_pflag,
+                                int32_t *d_iters);
+
+/* Stage times of one RK substep on d_P (unchanged), averaged over `reps` runs, measured
+   with CUDA events on the context stream: ms[0] flux kernels (all directions), ms[1] EMF
+   kernel, ms[2] update+inversion kernel, ms[3] one bound_prim, ms[4] post_fixup. */
+int harm_b200_time_stages(harm_ctx *ctx, int precision, int guess, const double *d_P,
+                          double dt, int reps, double ms[5]);
+
+/* Last CUDA error text of this thread's most recent failing call. */
+const char *harm_b200_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HARM_B200_H */

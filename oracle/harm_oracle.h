@@ -1,0 +1,67 @@
+/*
+ * harm_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU restatement (plain C, FP64, OpenMP) of HARM's per-timestep GRMHD update, used as
+ * the checker of the device path in tests/, in __graft_entry__.smoke() and as the
+ * timed CPU baseline of bench.py.  Nothing in the product library links or calls it.
+ *
+ * Parity status: the reference needs generated headers (decs.h from makedecs.h.sh,
+ * global.defnprs.h from generatenprs.c) and its own build system, so it is not built
+ * here; the reference's tests hold no golden vectors for this path.  Parity of this
+ * oracle with the reference is therefore UNPINNED: each function cites the reference
+ * file:line it restates, and tests/test_oracle_*.py check it against physics
+ * known-answer properties (P->U->P round trips, free-stream fluxes, div B) instead.
+ *
+ * Every array is in the layout of include/harm_b200.h (SoA over the extended grid).
+ */
+#ifndef HARM_ORACLE_H
+#define HARM_ORACLE_H
+#include <stdint.h>
+#include <stddef.h>
+#include "harm_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc {
+  harm_grid g;
+  const double *geom, *conn, *aux;
+  size_t plane, cells;
+  int nthreads;
+} orc;
+
+void orc_init(orc *o, const harm_grid *g, const double *geom, const double *conn,
+              const double *aux, int nthreads);
+
+/* single-point routines (geomrec = one CENT record of HARM_NGF doubles) */
+void orc_primtoU_point(const double *geomrec, const double *pr, double *U);
+void orc_primtoflux_point(const double *geomrec, const double *pr, int dir, double *F);
+int orc_utoprimgen_point(const harm_grid *g, const double *geomrec, const double *U,
+                         double *pr, int8_t *pflag, int32_t *iters);
+void orc_vchar_point(const harm_grid *g, const double *geomrec, const double *pr, int dir,
+                     double *vmax, double *vmin);
+
+/* grid routines */
+int orc_bound(orc *o, double *P);
+int orc_fluxcalc(orc *o, const double *pb, double *F1, double *F2, double *F3, double ndt[3]);
+int orc_advance(orc *o, int timeorder, int numtimeorders, const double *pi, const double *pb,
+                double *pf, int8_t *pflag, double dt, const double CUf[4],
+                const double Cunew[4], double *ndt, harm_stats *st);
+int orc_post_fixup(orc *o, double *pf, int8_t *pflag);
+int orc_step(orc *o, double *P, double *dt, harm_stats *st);
+
+/* reconstruction of one line (tests): y[n] -> left/right face states of faces 3..n-3 */
+void orc_reconstruct_line(int lim, int n, const double *y, double *pl, double *pr);
+
+/* learned-guess network oracle (double precision; same parameter layout as the device) */
+int orc_mlp_nparams(void);
+void orc_mlp_features(const harm_grid *g, const double *geomrec, const double *U,
+                      const double *P, float *feat, float *targ);
+double orc_mlp_loss_grad(int n, const float *feat, const float *targ, const float *params,
+                         const float *norm, double *pred, double *grad);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,142 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes binding of the CPU oracle (oracle/build/liborc.so).
+
+Imported by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg, never by the
+product package.  See oracle/harm_oracle.h for what the oracle restates and its parity status.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "build", "liborc.so")
+
+
+class orc(C.Structure):
+    pass
+
+
+def _import_grid():
+    import sys
+    sys.path.insert(0, os.path.dirname(HERE))
+    from harm_harm_b200 import _native as N  # noqa
+    return N
+
+
+N = _import_grid()
+
+orc._fields_ = [("g", N.harm_grid), ("geom", C.c_void_p), ("conn", C.c_void_p), ("aux", C.c_void_p),
+                ("plane", C.c_size_t), ("cells", C.c_size_t), ("nthreads", C.c_int)]
+
+_lib = None
+
+
+def build() -> str:
+    r = subprocess.run(["make", "-s", "-C", HERE], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
+    return LIB
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        P, D, I = C.c_void_p, C.c_double, C.c_int
+        sigs = {
+            "orc_init": (None, [C.POINTER(orc), C.POINTER(N.harm_grid), P, P, P, I]),
+            "orc_primtoU_point": (None, [P, P, P]),
+            "orc_primtoflux_point": (None, [P, P, I, P]),
+            "orc_utoprimgen_point": (I, [C.POINTER(N.harm_grid), P, P, P, P, P]),
+            "orc_vchar_point": (None, [C.POINTER(N.harm_grid), P, P, I, C.POINTER(D), C.POINTER(D)]),
+            "orc_bound": (I, [C.POINTER(orc), P]),
+            "orc_fluxcalc": (I, [C.POINTER(orc), P, P, P, P, P]),
+            "orc_advance": (I, [C.POINTER(orc), I, I, P, P, P, P, D, P, P, C.POINTER(D), C.POINTER(N.harm_stats)]),
+            "orc_post_fixup": (I, [C.POINTER(orc), P, P]),
+            "orc_step": (I, [C.POINTER(orc), P, C.POINTER(D), C.POINTER(N.harm_stats)]),
+            "orc_reconstruct_line": (None, [I, I, P, P, P]),
+        }
+        for fn, (res, args) in sigs.items():
+            f = getattr(L, fn)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray) -> int:
+    assert a.flags.c_contiguous
+    return a.ctypes.data
+
+
+class Oracle:
+    """CPU restatement of the step over the same inputs as the device path."""
+
+    def __init__(self, grid, geom, conn, aux, nthreads: int | None = None):
+        self.grid = grid
+        self._keep = (np.ascontiguousarray(geom), np.ascontiguousarray(conn), np.ascontiguousarray(aux))
+        self.o = orc()
+        nt = nthreads or os.cpu_count() or 1
+        lib().orc_init(C.byref(self.o), C.byref(grid.g), _p(self._keep[0]), _p(self._keep[1]), _p(self._keep[2]), nt)
+
+    def bound_prim(self, P):
+        lib().orc_bound(C.byref(self.o), _p(P))
+
+    def fluxcalc(self, pb, F1, F2, F3):
+        ndt = (C.c_double * 3)()
+        lib().orc_fluxcalc(C.byref(self.o), _p(pb), _p(F1), _p(F2), _p(F3), ndt)
+        return tuple(ndt)
+
+    def advance(self, timeorder, pi, pb, pf, pflag, dt):
+        from harm_harm_b200.harm import RK2_CUF, RK2_CUNEW
+        CUf = np.array(RK2_CUF[timeorder])
+        Cun = np.array(RK2_CUNEW[timeorder])
+        ndt = C.c_double()
+        st = N.harm_stats()
+        lib().orc_advance(C.byref(self.o), timeorder, 2, _p(pi), _p(pb), _p(pf), _p(pflag), dt, _p(CUf), _p(Cun),
+                          C.byref(ndt), C.byref(st))
+        return ndt.value, st.as_dict()
+
+    def post_fixup(self, pf, pflag):
+        lib().orc_post_fixup(C.byref(self.o), _p(pf), _p(pflag))
+
+    def step_ch(self, P, dt):
+        d = C.c_double(dt)
+        st = N.harm_stats()
+        lib().orc_step(C.byref(self.o), _p(P), C.byref(d), C.byref(st))
+        return d.value, st.as_dict()
+
+
+def utoprimgen_point(grid, geomrec, U, pr):
+    pr = np.ascontiguousarray(pr, dtype=np.float64).copy()
+    flag = np.zeros(1, dtype=np.int8)
+    it = np.zeros(1, dtype=np.int32)
+    lib().orc_utoprimgen_point(C.byref(grid.g), _p(np.ascontiguousarray(geomrec)), _p(np.ascontiguousarray(U)),
+                               _p(pr), _p(flag), _p(it))
+    return pr, int(flag[0]), int(it[0])
+
+
+def primtoU_point(geomrec, pr):
+    U = np.zeros(8)
+    lib().orc_primtoU_point(_p(np.ascontiguousarray(geomrec)), _p(np.ascontiguousarray(pr, dtype=np.float64)), _p(U))
+    return U
+
+
+def primtoflux_point(geomrec, pr, d):
+    F = np.zeros(8)
+    lib().orc_primtoflux_point(_p(np.ascontiguousarray(geomrec)), _p(np.ascontiguousarray(pr, dtype=np.float64)), d,
+                               _p(F))
+    return F
+
+
+def reconstruct_line(lim, y):
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    yl = np.zeros_like(y)
+    yr = np.zeros_like(y)
+    lib().orc_reconstruct_line(lim, len(y), _p(y), _p(yl), _p(yr))
+    return yl, yr

@@ -1,0 +1,293 @@
+/*
+ * orc_advance.c -- TEST INFRASTRUCTURE ONLY (CPU oracle; see harm_oracle.h).
+ *
+ * advance_standard (advance.c:140) for one RK substep, post_fixup/fixup_utoprim
+ * (fixup.c:53, :1061, general_average :1830), the boundary conditions of the torus
+ * problem (bound_prim, bounds.fishmon.c, bounds.tools.c) and the full RK2 step
+ * (step_ch_simplempi step_ch.c:524, setup_rktimestep :1244-1266, post_stepch :150).
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include "harm_oracle.h"
+#include "orc_internal.h"
+
+void orc_init(orc *o, const harm_grid *g, const double *geom, const double *conn,
+              const double *aux, int nthreads) {
+  o->g = *g;
+  o->geom = geom;
+  o->conn = conn;
+  o->aux = aux;
+  o->plane = (size_t)g->n1e * g->n2e;
+  o->cells = o->plane * g->n3e;
+  o->nthreads = nthreads > 0 ? nthreads : 1;
+}
+
+/* Ghost zones: x1 inner FREEOUTFLOW copy, x1 outer OUTFLOW copy with the inflow check
+   and limit_gamma (bound_x1up_outflow bounds.tools.c), x2 POLARAXIS reflection with U2,B2
+   sign flips (bound_x2dn_polaraxis bounds.tools.c:751; with n3>1 the source column is
+   the one across the pole, phi+pi, as in the full-3D polar transfer :618), x3 periodic.
+   Applied in the order x1, x2, x3 over the full transverse extent. */
+static void bound_generic(orc *o, double *P, int8_t *flag) {
+  const harm_grid *g = &o->g;
+  const int n1e = g->n1e, n2e = g->n2e, n3e = g->n3e, ng = g->ng, ng3 = g->ng3;
+  const size_t cells = o->cells;
+#pragma omp parallel for collapse(2) num_threads(o->nthreads)
+  for (int kk = 0; kk < n3e; kk++)
+    for (int jj = 0; jj < n2e; jj++) {
+      for (int ii = 0; ii < ng; ii++) {
+        size_t d = oidx(o, ii, jj, kk), s = oidx(o, ng, jj, kk);
+        if (P) for (int p = 0; p < HARM_NPR; p++) P[p * cells + d] = P[p * cells + s];
+        if (flag) flag[d] = flag[s];
+      }
+      for (int ii = ng + g->n1; ii < n1e; ii++) {
+        size_t d = oidx(o, ii, jj, kk), s = oidx(o, ng + g->n1 - 1, jj, kk);
+        if (flag) flag[d] = flag[s];
+        if (!P) continue;
+        double pr[HARM_NPR];
+        for (int p = 0; p < HARM_NPR; p++) pr[p] = P[p * cells + s];
+        ogeom gc;
+        og_load(o, HARM_LOC_CENT, ii, jj, &gc);
+        o_inflow_check_x1up(pr, &gc, g->gammamax);
+        o_limit_gamma(g->gammamax, pr, &gc);
+        for (int p = 0; p < HARM_NPR; p++) P[p * cells + d] = pr[p];
+      }
+    }
+  const int n3 = g->n3;
+#pragma omp parallel for collapse(2) num_threads(o->nthreads)
+  for (int kk = 0; kk < n3e; kk++)
+    for (int ii = 0; ii < n1e; ii++) {
+      int k = kk - ng3;
+      int ks = (n3 > 1) ? ((k + n3 / 2) % n3 + n3) % n3 + ng3 : kk;
+      for (int jj = 0; jj < ng; jj++) {
+        int js = 2 * ng - 1 - jj;
+        size_t d = oidx(o, ii, jj, kk), s = oidx(o, ii, js, ks);
+        if (flag) flag[d] = flag[s];
+        if (!P) continue;
+        for (int p = 0; p < HARM_NPR; p++) {
+          double v = P[p * cells + s];
+          if (p == HARM_U2 || p == HARM_B2) v = -v;
+          P[p * cells + d] = v;
+        }
+      }
+      for (int jj = ng + g->n2; jj < n2e; jj++) {
+        int js = 2 * (ng + g->n2) - 1 - jj;
+        size_t d = oidx(o, ii, jj, kk), s = oidx(o, ii, js, ks);
+        if (flag) flag[d] = flag[s];
+        if (!P) continue;
+        for (int p = 0; p < HARM_NPR; p++) {
+          double v = P[p * cells + s];
+          if (p == HARM_U2 || p == HARM_B2) v = -v;
+          P[p * cells + d] = v;
+        }
+      }
+    }
+  if (n3 > 1) {
+#pragma omp parallel for collapse(2) num_threads(o->nthreads)
+    for (int jj = 0; jj < n2e; jj++)
+      for (int ii = 0; ii < n1e; ii++) {
+        for (int kk = 0; kk < ng3; kk++) {
+          size_t d = oidx(o, ii, jj, kk), s = oidx(o, ii, jj, kk + n3);
+          if (P) for (int p = 0; p < HARM_NPR; p++) P[p * cells + d] = P[p * cells + s];
+          if (flag) flag[d] = flag[s];
+        }
+        for (int kk = ng3 + n3; kk < n3e; kk++) {
+          size_t d = oidx(o, ii, jj, kk), s = oidx(o, ii, jj, kk - n3);
+          if (P) for (int p = 0; p < HARM_NPR; p++) P[p * cells + d] = P[p * cells + s];
+          if (flag) flag[d] = flag[s];
+        }
+      }
+  }
+}
+
+int orc_bound(orc *o, double *P) {
+  bound_generic(o, P, NULL);
+  return 0;
+}
+
+int orc_advance(orc *o, int timeorder, int numtimeorders, const double *pi, const double *pb,
+                double *pf, int8_t *pflag, double dt, const double CUf[4],
+                const double Cunew[4], double *ndt, harm_stats *st) {
+  (void)timeorder;
+  const harm_grid *g = &o->g;
+  const size_t cells = o->cells, plane = o->plane;
+  const int finalstep = (timeorder == numtimeorders - 1);
+  double *F1 = (double *)calloc(HARM_NPR * cells, sizeof(double));
+  double *F2 = (double *)calloc(HARM_NPR * cells, sizeof(double));
+  double *F3 = (double *)calloc(HARM_NPR * cells, sizeof(double));
+  double *Uinv = (double *)calloc(HARM_NPR * cells, sizeof(double));
+  double ndt3[3];
+  orc_fluxcalc(o, pb, F1, F2, F3, ndt3);
+  const int ng = g->ng, ng3 = g->ng3, has3 = g->n3 > 1;
+  const double idx1 = 1.0 / g->dx[1], idx2 = 1.0 / g->dx[2], idx3 = 1.0 / g->dx[3];
+  /* update loop (advance.c:420-575) */
+#pragma omp parallel for collapse(2) schedule(static) num_threads(o->nthreads)
+  for (int k = 0; k < g->n3; k++)
+    for (int j = 0; j < g->n2; j++)
+      for (int i = 0; i < g->n1; i++) {
+        int ii = i + ng, jj = j + ng, kk = k + ng3;
+        size_t id = oidx(o, ii, jj, kk);
+        ogeom gc;
+        og_load(o, HARM_LOC_CENT, ii, jj, &gc);
+        double pri[HARM_NPR], prb[HARM_NPR], Ui[HARM_NPR], dUg[HARM_NPR];
+        for (int p = 0; p < HARM_NPR; p++) { pri[p] = pi[p * cells + id]; prb[p] = pb[p * cells + id]; }
+        ostate qi, qb;
+        o_get_state(pri, &gc, g->gam, &qi);
+        o_primtoflux(pri, &qi, 0, &gc, Ui);
+        double dU[HARM_NPR];
+        size_t ip = oidx(o, ii + 1, jj, kk), jp = oidx(o, ii, jj + 1, kk), kp = has3 ? oidx(o, ii, jj, kk + 1) : id;
+        for (int p = 0; p < HARM_NPR; p++) {
+          double d1 = -(F1[p * cells + ip] - F1[p * cells + id]) * idx1;
+          double d2 = -(F2[p * cells + jp] - F2[p * cells + id]) * idx2;
+          double d3 = has3 ? -(F3[p * cells + kp] - F3[p * cells + id]) * idx3 : 0.0;
+          dU[p] = d1 + d2 + d3;
+        }
+        double conn[64];
+        for (int c = 0; c < 64; c++) conn[c] = o->conn[(size_t)c * plane + (size_t)jj * g->n1e + ii];
+        o_get_state(prb, &gc, g->gam, &qb);
+        o_source(prb, &qb, &gc, conn, dUg);
+        for (int p = 0; p < HARM_NPR; p++) {
+          /* UFSET / UCUMUPDATE (global.stepch.h:5,10) with CUf[1]=0 and, for the
+             midpoint RK2, ucum starting from zero on the first substep */
+          double Uf = CUf[0] * Ui[p] + CUf[2] * dt * (dU[p] + dUg[p]);
+          double ucum = Cunew[0] * Ui[p] + Cunew[1] * dt * (dU[p] + dUg[p]) + Cunew[2] * Uf;
+          Uinv[p * cells + id] = finalstep ? ucum : Uf;
+        }
+      }
+  /* pf = pb everywhere (copy_3dnpr_fullloop advance.c:654), then invert active cells */
+  for (size_t c = 0; c < HARM_NPR * cells; c++) pf[c] = pb[c];
+  double iters = 0.0, fails = 0.0, floors = 0.0;
+#pragma omp parallel for collapse(2) schedule(dynamic, 4) reduction(+ : iters, fails, floors) num_threads(o->nthreads)
+  for (int k = 0; k < g->n3; k++)
+    for (int j = 0; j < g->n2; j++)
+      for (int i = 0; i < g->n1; i++) {
+        int ii = i + ng, jj = j + ng, kk = k + ng3;
+        size_t id = oidx(o, ii, jj, kk);
+        ogeom gc;
+        og_load(o, HARM_LOC_CENT, ii, jj, &gc);
+        double U[HARM_NPR], pr[HARM_NPR];
+        for (int p = 0; p < HARM_NPR; p++) { U[p] = Uinv[p * cells + id]; pr[p] = pf[p * cells + id]; }
+        int8_t fl = 0;
+        int nst = 0;
+        o_utoprimgen(U, &gc, pr, &fl, g->gam, g->gammafail, &nst);
+        if (fl > 0) fails += 1.0;
+        size_t c2 = (size_t)jj * g->n1e + ii;
+        floors += o_fixup1zone(pr, &gc, o->aux[HARM_AUX_RHOFLOOR * plane + c2], o->aux[HARM_AUX_UFLOOR * plane + c2],
+                               g->gam, g->gammamax, g->gammafail, &fl, &nst);
+        iters += nst;
+        pflag[id] = fl;
+        for (int p = 0; p < HARM_NPR; p++) pf[p * cells + id] = pr[p];
+      }
+  /* prepare_globaldt (advance.c:1558), accdt = BIG (LIMITDTWITHSOURCETERM=0) */
+  double wavedt = 1. / (1. / ndt3[0] + 1. / ndt3[1] + 1. / ndt3[2]);
+  *ndt = g->defcon * fmin(wavedt, 1.e100);
+  if (st) {
+    st->newton_iters += iters;
+    st->cells_inverted += (double)g->n1 * g->n2 * g->n3;
+    st->inversion_failures += fails;
+    st->floor_hits += floors;
+  }
+  free(F1); free(F2); free(F3); free(Uinv);
+  return 0;
+}
+
+/* fixup_utoprim (fixup.c:1061) with general_average (fixup.c:1830), CAUSALAVG=0,
+   HOWTOAVG_WHEN_U2AVG=MAXUPOSAVG; cells with no usable neighbour keep their value. */
+int orc_post_fixup(orc *o, double *pf, int8_t *pflag) {
+  const harm_grid *g = &o->g;
+  const size_t cells = o->cells;
+  bound_generic(o, NULL, pflag);
+  double *ptoavg = (double *)malloc(HARM_NPR * cells * sizeof(double));
+  int8_t *forig = (int8_t *)malloc(cells);
+  memcpy(ptoavg, pf, HARM_NPR * cells * sizeof(double));
+  memcpy(forig, pflag, cells);
+  const int s1 = g->n1 > 1, s2 = g->n2 > 1, s3 = g->n3 > 1;
+  const int rnx = s1 ? 3 : 1, rny = s2 ? 3 : 1;
+  const int npairs = ((int)pow(3, s1 + s2 + s3) - 1) / 2;
+#pragma omp parallel for collapse(2) schedule(static) num_threads(o->nthreads)
+  for (int k = 0; k < g->n3; k++)
+    for (int j = 0; j < g->n2; j++)
+      for (int i = 0; i < g->n1; i++) {
+        int ii = i + g->ng, jj = j + g->ng, kk = k + g->ng3;
+        size_t id = oidx(o, ii, jj, kk);
+        int8_t f = forig[id];
+        if (f <= 0) continue;
+        int startpl, endpl, looptype;
+        if (f == HARM_UTOPRIMFAILU2AVG1 || f == HARM_UTOPRIMFAILU2AVG2 || f == 13) {
+          startpl = endpl = HARM_UU;
+        } else {
+          startpl = HARM_RHO;
+          endpl = HARM_U3;
+        }
+        looptype = (f == HARM_UTOPRIMFAILU2AVG1 || f == HARM_UTOPRIMFAILU2AVG2) ? 1 : 0;
+        double mysum[2][HARM_NPR] = {{0}}, lastmin[HARM_NPR];
+        for (int p = 0; p < HARM_NPR; p++) lastmin[p] = 1E50;
+        int numavg0 = 0, numavg1 = 0;
+        double ref = ptoavg[HARM_UU * cells + id];
+        for (int qq = 0; qq < npairs; qq++) {
+          int di = (qq % rnx) - s1, dj = ((qq % (rnx * rny)) / rnx) - s2, dk = (qq / (rnx * rny)) - s3;
+          size_t a = oidx(o, ii + di, jj + dj, kk + dk), b = oidx(o, ii - di, jj - dj, kk - dk);
+          int thisok = forig[a] <= 0, thatok = forig[b] <= 0;
+          numavg0 += thisok + thatok;
+          for (int p = startpl; p <= endpl; p++) {
+            if (looptype == 0) {
+              mysum[qq % 2][p] += ptoavg[p * cells + a] * thisok + ptoavg[p * cells + b] * thatok;
+            } else {
+              double f1 = ptoavg[p * cells + a], f2 = ptoavg[p * cells + b];
+              if (f1 >= ref && f2 >= ref) {
+                lastmin[p] = fmin(fmin(lastmin[p], f1), f2);
+                numavg1++;
+              }
+            }
+          }
+        }
+        if (looptype == 0) {
+          if (numavg0 != 0)
+            for (int p = startpl; p <= endpl; p++) pf[p * cells + id] = (mysum[0][p] + mysum[1][p]) / (double)numavg0;
+        } else {
+          if (numavg1 != 0)
+            for (int p = startpl; p <= endpl; p++) pf[p * cells + id] = lastmin[p];
+        }
+        if (startpl <= HARM_U1 && endpl >= HARM_U3) {
+          ogeom gc;
+          og_load(o, HARM_LOC_CENT, ii, jj, &gc);
+          double pa[HARM_NPR], pv[HARM_NPR], ucon[4], gamma, qsq;
+          for (int p = 0; p < HARM_NPR; p++) { pa[p] = ptoavg[p * cells + id]; pv[p] = pf[p * cells + id]; }
+          o_ucon(pa, &gc, ucon, &gamma, &qsq);
+          if (gamma > g->gammamax) gamma = g->gammamax;
+          o_limit_gamma(gamma, pv, &gc);
+          for (int p = 0; p < HARM_NPR; p++) pf[p * cells + id] = pv[p];
+        }
+      }
+  free(ptoavg);
+  free(forig);
+  return 0;
+}
+
+/* One RK2 midpoint step (TIMEORDER=2): CUf = {1,0,1/2},{1,0,1}; Cunew = {0,0,0},{0,0,1} */
+int orc_step(orc *o, double *P, double *dt, harm_stats *st) {
+  const size_t n = HARM_NPR * o->cells;
+  double *pk = (double *)malloc(n * sizeof(double));
+  int8_t *pflag = (int8_t *)calloc(o->cells, 1);
+  const double CUf[2][4] = {{1.0, 0.0, 0.5, 0.0}, {1.0, 0.0, 1.0, 0.0}};
+  const double Cun[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 1.0, 0.5}};
+  double ndt, lastndt = 1.e100;
+  /* substep 0: pi=P, pb=P, pf=pk */
+  orc_advance(o, 0, 2, P, P, pk, pflag, *dt, CUf[0], Cun[0], &ndt, st);
+  if (ndt < lastndt) lastndt = ndt;
+  orc_bound(o, pk);
+  orc_post_fixup(o, pk, pflag);
+  orc_bound(o, pk);
+  /* substep 1: pi=P, pb=pk, pf=P */
+  orc_advance(o, 1, 2, P, pk, P, pflag, *dt, CUf[1], Cun[1], &ndt, st);
+  if (ndt < lastndt) lastndt = ndt;
+  orc_bound(o, P);
+  orc_post_fixup(o, P, pflag);
+  orc_bound(o, P);
+  /* post_stepch (step_ch.c:213) */
+  if (lastndt > o->g.safe * (*dt)) lastndt = o->g.safe * (*dt);
+  *dt = lastndt;
+  free(pk);
+  free(pflag);
+  return 0;
+}

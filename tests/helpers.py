@@ -1,0 +1,58 @@
+"""Shared helpers of the test suite: grids, comparisons, divergence of B."""
+from __future__ import annotations
+
+import numpy as np
+
+from harm_harm_b200 import Grid
+
+
+def make_torus(n1=64, n2=64, n3=1, lim=0, seed=12345, beta=100.0):
+    g = Grid.torus(n1, n2, n3, lim=lim)
+    geom, conn, aux = g.geometry()
+    P = g.torus_init(geom, aux, beta_min=beta, seed=seed)
+    return g, geom, conn, aux, P
+
+
+def rel_err(a, b, floor_frac=1e-12):
+    """max |a-b| / (|a|+|b| + floor), floor = floor_frac * max(|a|) (per array)"""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    floor = floor_frac * max(np.abs(a).max(), np.abs(b).max(), 1e-300)
+    return float((np.abs(a - b) / (np.abs(a) + np.abs(b) + floor)).max())
+
+
+def per_field_close(a, b, rtol, floor_frac=1e-10):
+    """rel_err per primitive field; returns dict pl -> err"""
+    return {pl: rel_err(a[pl], b[pl], floor_frac) for pl in range(a.shape[0])}
+
+
+def divb_corner(grid, geom, P):
+    """Toth corner divergence of sqrt(-g) B (the quantity flux-CT preserves), active corners."""
+    g = grid.g
+    gd = geom[0, 26]  # CENT gdet [j][i]
+    U = P[5:8] * gd[None, None, :, :]
+    ng, ng3 = g.ng, g.ng3
+    dx1, dx2, dx3 = g.dx[1], g.dx[2], g.dx[3]
+    if g.n3 == 1:
+        k = 0
+        u1, u2 = U[0, k], U[1, k]
+        j0, j1, i0, i1 = ng, ng + g.n2 + 1, ng, ng + g.n1 + 1
+        J, I = np.mgrid[j0:j1, i0:i1]
+        d1 = 0.5 * (u1[J, I] + u1[J - 1, I] - u1[J, I - 1] - u1[J - 1, I - 1]) / dx1
+        d2 = 0.5 * (u2[J, I] + u2[J, I - 1] - u2[J - 1, I] - u2[J - 1, I - 1]) / dx2
+        return np.abs(d1 + d2)
+    u1, u2, u3 = U[0], U[1], U[2]
+    K, J, I = np.mgrid[ng3:ng3 + g.n3 + 1, ng:ng + g.n2 + 1, ng:ng + g.n1 + 1]
+    d1 = 0.25 * (u1[K, J, I] + u1[K, J - 1, I] + u1[K - 1, J, I] + u1[K - 1, J - 1, I]
+                 - u1[K, J, I - 1] - u1[K, J - 1, I - 1] - u1[K - 1, J, I - 1] - u1[K - 1, J - 1, I - 1]) / dx1
+    d2 = 0.25 * (u2[K, J, I] + u2[K, J, I - 1] + u2[K - 1, J, I] + u2[K - 1, J, I - 1]
+                 - u2[K, J - 1, I] - u2[K, J - 1, I - 1] - u2[K - 1, J - 1, I] - u2[K - 1, J - 1, I - 1]) / dx2
+    d3 = 0.25 * (u3[K, J, I] + u3[K, J, I - 1] + u3[K, J - 1, I] + u3[K, J - 1, I - 1]
+                 - u3[K - 1, J, I] - u3[K - 1, J, I - 1] - u3[K - 1, J - 1, I] - u3[K - 1, J - 1, I - 1]) / dx3
+    return np.abs(d1 + d2 + d3)
+
+
+def geom_records(geom, grid, idx2d):
+    """CENT records [HARM_NGF][n] at flattened (j*n1e+i) positions"""
+    cent = geom[0].reshape(geom.shape[1], -1)
+    return np.ascontiguousarray(cent[:, idx2d])

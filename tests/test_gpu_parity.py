@@ -1,0 +1,159 @@
+"""Parity of the device path (libharm_b200.so, through the C ABI) with the CPU oracle.
+
+FP64 path: every entry point matches the oracle to 1e-12 relative (floor 1e-12 of the
+field's maximum) on the same inputs; multi-step runs to 1e-10.  Mixed precision: FP32
+reconstruction/HLL/CT with FP64 update and inversion, compared with the FP64 path in L1.
+"""
+import numpy as np
+import pytest
+
+from helpers import divb_corner, make_torus, rel_err
+from harm_harm_b200 import HARM_PREC_FP64, HARM_PREC_MIXED, Harm
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+CASES = {"2d": (64, 64, 1), "3d": (32, 24, 8)}
+
+
+@pytest.fixture(scope="module", params=list(CASES))
+def setup(request, cuda):
+    g, geom, conn, aux, P = make_torus(*CASES[request.param])
+    orc = O.Oracle(g, geom, conn, aux)
+    orc.bound_prim(P)
+    dev = Harm(g, geom, conn, aux)
+    return g, geom, conn, aux, P, orc, dev
+
+
+def dev_array(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def faces_of_active(g, d):
+    """slices of the faces whose fluxes enter the update (field fluxes final there)"""
+    gg = g.g
+    k = slice(gg.ng3, gg.ng3 + gg.n3 + (1 if d == 3 else 0))
+    j = slice(gg.ng, gg.ng + gg.n2 + (1 if d == 2 else 0))
+    i = slice(gg.ng, gg.ng + gg.n1 + (1 if d == 1 else 0))
+    return (slice(None), k, j, i)
+
+
+def test_bound_parity(setup, cuda):
+    g, geom, conn, aux, P, orc, dev = setup
+    Pc = P.copy()
+    Pc[:, :, :, : g.g.ng] = 7.0  # stale ghosts to be overwritten
+    Po = Pc.copy()
+    orc.bound_prim(Po)
+    Pd = dev_array(cuda, Pc)
+    dev.bound_prim(Pd)
+    cuda.cuda.synchronize()
+    assert rel_err(Pd.cpu().numpy(), Po) < 1e-14
+
+
+def test_fluxcalc_parity_fp64(setup, cuda):
+    g, geom, conn, aux, P, orc, dev = setup
+    Fo = [np.zeros_like(P) for _ in range(3)]
+    ndt_o = orc.fluxcalc(P, *Fo)
+    Pd = dev_array(cuda, P)
+    Fd = [cuda.zeros_like(Pd) for _ in range(3)]
+    ndt_d = dev.fluxcalc(Pd, *Fd)
+    for d in range(3 if g.g.n3 > 1 else 2):
+        sl = faces_of_active(g, d + 1)
+        a = Fd[d].cpu().numpy()[sl]
+        b = Fo[d][sl]
+        for pl in range(8):
+            e = rel_err(a[pl], b[pl])
+            assert e < 1e-12, (d + 1, pl, e)
+    for d in range(3 if g.g.n3 > 1 else 2):
+        assert abs(ndt_d[d] - ndt_o[d]) <= 1e-12 * ndt_o[d], (d, ndt_d, ndt_o)
+
+
+def test_advance_parity_fp64(setup, cuda):
+    g, geom, conn, aux, P, orc, dev = setup
+    Fo = [np.zeros_like(P) for _ in range(3)]
+    ndt = orc.fluxcalc(P, *Fo)
+    dt = 1.0 / sum(1.0 / x for x in ndt[: (3 if g.g.n3 > 1 else 2)])
+    pf_o = np.zeros_like(P)
+    fl_o = np.zeros(P.shape[1:], dtype=np.int8)
+    ndt_o, st_o = orc.advance(0, P, P, pf_o, fl_o, dt)
+    Pd = dev_array(cuda, P)
+    pf_d = cuda.zeros_like(Pd)
+    fl_d = cuda.zeros(P.shape[1:], dtype=cuda.int8, device="cuda")
+    ndt_d, st_d = dev.advance(0, Pd, Pd, pf_d, fl_d, dt)
+    act = (slice(None),) + g.active
+    a = pf_d.cpu().numpy()[act]
+    b = pf_o[act]
+    for pl in range(8):
+        assert rel_err(a[pl], b[pl]) < 1e-12, (pl, rel_err(a[pl], b[pl]))
+    assert np.array_equal(fl_d.cpu().numpy()[g.active], fl_o[g.active])
+    assert abs(ndt_d - ndt_o) <= 1e-12 * ndt_o
+    assert abs(st_d["newton_iters"] - st_o["newton_iters"]) <= 1e-3 * st_o["newton_iters"]
+
+
+def test_step_parity_fp64_and_divb(setup, cuda):
+    g, geom, conn, aux, P, orc, dev = setup
+    Fo = [np.zeros_like(P) for _ in range(3)]
+    ndt = orc.fluxcalc(P, *Fo)
+    dt0 = 1.0 / sum(1.0 / x for x in ndt[: (3 if g.g.n3 > 1 else 2)])
+    Po = P.copy()
+    dto = dt0
+    for _ in range(3):
+        dto, _ = orc.step_ch(Po, dto)
+    Pd = dev_array(cuda, P)
+    dtd, st = dev.step_ch(Pd, dt0, nsteps=3)
+    Pdn = Pd.cpu().numpy()
+    act = (slice(None),) + g.active
+    for pl in range(8):
+        e = rel_err(Pdn[act][pl], Po[act][pl], floor_frac=1e-10)
+        assert e < 1e-10, (pl, e)
+    assert abs(dtd - dto) <= 1e-10 * dto
+    scale = np.abs(Pdn[5:8] * geom[0, 26][None, None]).max() / min(g.g.dx[1], g.g.dx[2])
+    assert divb_corner(g, geom, Pdn).max() / scale < 1e-12
+
+
+def test_utoprimgen_points_parity(cuda):
+    g, geom, conn, aux, P = make_torus(32, 32, 1)
+    dev = Harm(g, geom, conn, aux)
+    rng = np.random.default_rng(7)
+    cent = geom[0].reshape(28, -1)
+    n = 4096
+    cells = rng.integers(0, cent.shape[1], n)
+    rho = 10 ** rng.uniform(-6, 0, n)
+    prims = np.vstack([rho, rho * 10 ** rng.uniform(-4, 1, n), rng.normal(0, 1, (3, n)),
+                       rng.normal(0, 1, (3, n)) * np.sqrt(rho * 10 ** rng.uniform(-3, 2, n))])
+    recs = np.ascontiguousarray(cent[:, cells])
+    U = np.stack([O.primtoU_point(np.ascontiguousarray(recs[:, c]), prims[:, c]) for c in range(n)], axis=1)
+    guess = prims * (1 + 0.05 * rng.normal(size=prims.shape))
+    out_o = np.zeros_like(prims)
+    fl_o = np.zeros(n, dtype=np.int8)
+    it_o = np.zeros(n, dtype=np.int32)
+    for c in range(n):
+        out_o[:, c], fl_o[c], it_o[c] = O.utoprimgen_point(g, np.ascontiguousarray(recs[:, c]), U[:, c], guess[:, c])
+    Ud, Gd, Pd = (dev_array(cuda, x) for x in (U, recs, guess))
+    fl_d = cuda.zeros(n, dtype=cuda.int8, device="cuda")
+    it_d = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    dev.Utoprimgen(Ud, Gd, Pd, fl_d, it_d)
+    out_d = Pd.cpu().numpy()
+    assert np.array_equal(fl_d.cpu().numpy(), fl_o)
+    for pl in range(8):
+        assert rel_err(out_d[pl], out_o[pl], 1e-12) < 1e-9, pl
+    # iteration counts agree except where round-off moves the stop by one step
+    assert np.mean(np.abs(it_d.cpu().numpy() - it_o)) < 0.5
+
+
+def test_mixed_precision_close_to_fp64(setup, cuda):
+    g, geom, conn, aux, P, orc, dev = setup
+    Fo = [np.zeros_like(P) for _ in range(3)]
+    ndt = orc.fluxcalc(P, *Fo)
+    dt0 = 1.0 / sum(1.0 / x for x in ndt[: (3 if g.g.n3 > 1 else 2)])
+    Pa = dev_array(cuda, P)
+    Pb = dev_array(cuda, P)
+    dev.step_ch(Pa, dt0, precision=HARM_PREC_FP64, nsteps=5)
+    dev.step_ch(Pb, dt0, precision=HARM_PREC_MIXED, nsteps=5)
+    a = Pa.cpu().numpy()[(slice(None),) + g.active]
+    b = Pb.cpu().numpy()[(slice(None),) + g.active]
+    l1_rho = np.abs(a[0] - b[0]).mean() / np.abs(a[0]).mean()
+    assert np.isfinite(b).all()
+    assert l1_rho < 1e-5, l1_rho
+    scale = np.abs(Pb.cpu().numpy()[5:8] * geom[0, 26][None, None]).max() / min(g.g.dx[1], g.g.dx[2])
+    assert divb_corner(g, geom, Pb.cpu().numpy()).max() / scale < 1e-6
