@@ -5,7 +5,7 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIBDIR = os.path.join(HERE, "lib")
+LIBDIR = os.environ.get("HARM_B200_LIBDIR") or os.path.join(HERE, "lib")
 
 HARM_NPR = 8
 HARM_LIM_MC, HARM_LIM_PARA, HARM_LIM_WENO5 = 0, 1, 2

@@ -66,18 +66,30 @@ def device_sources() -> list[str]:
     return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
 
 
-def build_device(force: bool = False, extra: list[str] | None = None) -> str:
-    os.makedirs(LIB, exist_ok=True)
-    out = os.path.join(LIB, "libharm_b200.so")
+def device_flags(src: str) -> list[str]:
+    """Per-file flags: the FP64 path is compiled without FMA contraction so that its FP64
+    operations are the IEEE operations of the C restatement, in the same order."""
+    return ["-fmad=false"] if src.endswith("_fp64.cu") else []
+
+
+def build_device(force: bool = False, extra: list[str] | None = None, out_dir: str | None = None) -> str:
+    out_dir = out_dir or LIB
+    os.makedirs(out_dir, exist_ok=True)
+    objdir = os.path.join(out_dir, "obj")
+    os.makedirs(objdir, exist_ok=True)
+    out = os.path.join(out_dir, "libharm_b200.so")
     srcs = device_sources()
-    deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")] + [
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] + [
         os.path.join(INCLUDE, "harm_b200.h")]
-    if force or not _newer(out, deps):
-        cmd = [nvcc(), *NVCC_ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-               "--cudart", "static", "-I" + INCLUDE, "-I" + CSRC, "-o", out, *srcs]
-        if extra:
-            cmd[1:1] = extra
-        _run(cmd)
+    if force or not _newer(out, srcs + headers):
+        objs = []
+        for src in srcs:
+            obj = os.path.join(objdir, os.path.basename(src) + ".o")
+            cmd = [nvcc(), *NVCC_ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE,
+                   "-I" + CSRC, *device_flags(src), *(extra or []), "-c", "-o", obj, src]
+            _run(cmd)
+            objs.append(obj)
+        _run([nvcc(), *NVCC_ARCH, "-shared", "--cudart", "static", "-o", out, *objs])
     return out
 
 

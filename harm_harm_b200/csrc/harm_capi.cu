@@ -1,0 +1,272 @@
+// harm_capi.cu -- the C ABI of libharm_b200.so (include/harm_b200.h): context, uploads,
+// and the reference-shaped entry points, each a sequence of launches on the context stream.
+//
+// Substep order (advance_standard advance.c:140 + post_advance step_ch.c:288):
+//   fluxes(p_b) -> EMFs -> update+inversion(p_i, p_b -> p_f) -> bound(p_f) ->
+//   bound(pflag) + fixup_utoprim(p_f) -> bound(p_f)
+// Full step: two substeps (RK2 midpoint), then dt on the device (prepare_globaldt
+// advance.c:1558, post_stepch step_ch.c:213).
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <algorithm>
+#include "harm_common.cuh"
+#include "harm_paths.h"
+
+static __thread char g_errbuf[512];
+
+int hb_seterr(const char* what, cudaError_t e) {
+  snprintf(g_errbuf, sizeof(g_errbuf), "%s: %s", what, cudaGetErrorString(e));
+  return 1;
+}
+
+static int seterr_msg(const char* msg, int code) {
+  snprintf(g_errbuf, sizeof(g_errbuf), "%s", msg);
+  return code;
+}
+
+extern "C" const char* harm_b200_last_error(void) { return g_errbuf; }
+
+extern "C" int harm_b200_create(const harm_grid* g, const double* geom_h, const double* conn_h, const double* aux_h,
+                                int device, harm_ctx** out) {
+  if (!g || !geom_h || !conn_h || !aux_h || !out) return seterr_msg("null argument", 1);
+  if (g->lim != HARM_LIM_MC) return seterr_msg("this reconstruction is not available in the device library", 2);
+  harm_ctx* c = new harm_ctx();
+  memset((void*)c, 0, sizeof(*c));
+  c->g = *g;
+  c->device = device;
+  CK(cudaSetDevice(device));
+  CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  Dims d = dims_of(*g);
+  c->plane = d.plane;
+  c->cells = d.cells;
+  size_t gsz = (size_t)HARM_NLOC * HARM_NGF * d.plane;
+  CK(cudaMalloc(&c->d_geom, gsz * sizeof(double)));
+  CK(cudaMalloc(&c->d_geomf, gsz * sizeof(float)));
+  CK(cudaMalloc(&c->d_conn, 64 * d.plane * sizeof(double)));
+  CK(cudaMalloc(&c->d_aux, HARM_NAUX * d.plane * sizeof(double)));
+  CK(cudaMemcpy(c->d_geom, geom_h, gsz * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_conn, conn_h, 64 * d.plane * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_aux, aux_h, HARM_NAUX * d.plane * sizeof(double), cudaMemcpyHostToDevice));
+  {
+    float* tmp = (float*)malloc(gsz * sizeof(float));
+    if (!tmp) return seterr_msg("host allocation failed", 3);
+    for (size_t q = 0; q < gsz; q++) tmp[q] = (float)geom_h[q];
+    cudaError_t e = cudaMemcpy(c->d_geomf, tmp, gsz * sizeof(float), cudaMemcpyHostToDevice);
+    free(tmp);
+    if (e != cudaSuccess) return hb_seterr("upload FP32 metric", e);
+  }
+  for (int q = 0; q < 3; q++) {
+    CK(cudaMalloc(&c->d_F[q], NPR * d.cells * sizeof(double)));
+    CK(cudaMalloc(&c->d_Ff[q], NPR * d.cells * sizeof(float)));
+  }
+  CK(cudaMalloc(&c->d_emf, 3 * d.cells * sizeof(double)));
+  CK(cudaMalloc(&c->d_emff, 3 * d.cells * sizeof(float)));
+  CK(cudaMalloc(&c->d_pk, NPR * d.cells * sizeof(double)));
+  CK(cudaMalloc(&c->d_pflag, d.cells));
+  CK(cudaMemset(c->d_pflag, 0, d.cells));
+  c->fix_cap = (unsigned int)std::min<size_t>((size_t)d.n1 * d.n2 * d.n3, 0xFFFFFFF0u);
+  CK(cudaMalloc(&c->d_fixrec, (size_t)c->fix_cap * sizeof(FixRec)));
+  CK(cudaMalloc(&c->d_scal, 64 * sizeof(double)));
+  CK(cudaMemset(c->d_scal, 0, 64 * sizeof(double)));
+  c->d_dtslots = (unsigned long long*)(c->d_scal + 0);  // 6 slots
+  c->d_dt = c->d_scal + 8;
+  c->d_ndt = c->d_scal + 9;                             // 2
+  c->d_stats = c->d_scal + 16;                          // 5
+  c->d_nrec = (unsigned int*)(c->d_scal + 24);
+  CK(cudaMemset(c->d_dtslots, 0xFF, 6 * sizeof(unsigned long long)));
+  CK(cudaMallocHost(&c->h_scal, 64 * sizeof(double)));
+  *out = c;
+  return 0;
+}
+
+extern "C" int harm_b200_destroy(harm_ctx* c) {
+  if (!c) return 0;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  void* ptrs[] = {c->d_geom, c->d_geomf, c->d_conn, c->d_aux, c->d_F[0], c->d_F[1], c->d_F[2], c->d_Ff[0], c->d_Ff[1],
+                  c->d_Ff[2], c->d_emf, c->d_emff, c->d_pk, c->d_pflag, c->d_fixrec, c->d_scal, c->d_Pdev, c->d_mlp,
+                  c->d_mlp_master, c->d_mlp_adam, c->d_mlp_work};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (c->h_scal) cudaFreeHost(c->h_scal);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return 0;
+}
+
+extern "C" void* harm_b200_stream(harm_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+extern "C" unsigned long long harm_b200_launch_count(harm_ctx* c) { return c ? c->launches : 0ull; }
+
+extern "C" int harm_b200_bound(harm_ctx* c, double* d_P) { return hp_bound(c, d_P, nullptr); }
+
+extern "C" int harm_b200_fluxcalc(harm_ctx* c, int precision, const double* d_pb, double* d_F1, double* d_F2,
+                                  double* d_F3, double ndt[3]) {
+  if (precision != HARM_PREC_FP64) return seterr_msg("fluxcalc into FP64 arrays needs HARM_PREC_FP64", 2);
+  unsigned long long* slots = c->d_dtslots;
+  CK(cudaMemsetAsync(slots, 0xFF, 3 * sizeof(unsigned long long), c->stream));
+  if (hp_fluxes_fp64(c, d_pb, d_F1, d_F2, d_F3, c->d_emf, slots)) return 1;
+  if (hp_emf_to_flux_fp64(c, c->d_emf, d_F1, d_F2, d_F3)) return 1;
+  unsigned long long hb[3];
+  CK(cudaMemcpyAsync(hb, slots, sizeof(hb), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int q = 0; q < 3; q++) {
+    double v;
+    memcpy(&v, &hb[q], 8);
+    ndt[q] = (hb[q] == 0xFFFFFFFFFFFFFFFFull) ? 1.e100 : v;
+  }
+  CK(cudaMemsetAsync(slots, 0xFF, 3 * sizeof(unsigned long long), c->stream));
+  return 0;
+}
+
+// one substep on the device; dt from d_dt, dt minima of this substep into slots
+static int substep(harm_ctx* c, int precision, int guess, int timeorder, int numtimeorders, const double* d_pi,
+                   const double* d_pb, double* d_pf, int8_t* d_pflag, const double* CUf, const double* Cunew,
+                   unsigned long long* slots, bool with_stats) {
+  StepCoef sc;
+  sc.CUf0 = CUf[0]; sc.CUf2 = CUf[2];
+  sc.Cun0 = Cunew[0]; sc.Cun1 = Cunew[1]; sc.Cun2 = Cunew[2];
+  sc.finalstep = (timeorder == numtimeorders - 1);
+  sc.guess = guess;
+  double* st = with_stats ? c->d_stats : nullptr;
+  if (precision == HARM_PREC_FP64) {
+    if (hp_fluxes_fp64(c, d_pb, c->d_F[0], c->d_F[1], c->d_F[2], c->d_emf, slots)) return 1;
+    return hp_update_fp64(c, sc, d_pi, d_pb, d_pf, d_pflag, st);
+  }
+  if (hp_fluxes_mixed(c, d_pb, c->d_Ff[0], c->d_Ff[1], c->d_Ff[2], c->d_emff, slots)) return 1;
+  return hp_update_mixed(c, sc, d_pi, d_pb, d_pf, d_pflag, st);
+}
+
+static void add_stats(harm_ctx* c, harm_stats* stats, double inverted) {
+  if (!stats) return;
+  stats->newton_iters += c->h_scal[8];
+  stats->cells_inverted += inverted;
+  stats->mlp_fallbacks += c->h_scal[10];
+  stats->inversion_failures += c->h_scal[11];
+  stats->floor_hits += c->h_scal[12];
+}
+
+extern "C" int harm_b200_advance(harm_ctx* c, int precision, int guess, int timeorder, int numtimeorders,
+                                 const double* d_pi, const double* d_pb, double* d_pf, int8_t* d_pflag, double dt,
+                                 const double CUf[4], const double Cunew[4], double* ndt, harm_stats* stats) {
+  Dims d = dims_of(c->g);
+  c->h_scal[0] = dt;
+  CK(cudaMemcpyAsync(c->d_dt, c->h_scal, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->d_stats, 0, 5 * sizeof(double), c->stream));
+  if (substep(c, precision, guess, timeorder, numtimeorders, d_pi, d_pb, d_pf, d_pflag, CUf, Cunew, c->d_dtslots, true))
+    return 1;
+  if (hp_copy_ghosts(c, d_pb, d_pf)) return 1;
+  if (hp_finalize_dt(c, nullptr, c->d_ndt, 1)) return 1;
+  CK(cudaMemcpyAsync(c->h_scal + 1, c->d_ndt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(c->h_scal + 8, c->d_stats, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (ndt) *ndt = c->h_scal[1];
+  add_stats(c, stats, (double)d.n1 * d.n2 * d.n3);
+  return 0;
+}
+
+extern "C" int harm_b200_post_fixup(harm_ctx* c, double* d_pf, int8_t* d_pflag) { return hp_fixup(c, d_pf, d_pflag); }
+
+// enqueue one full RK2 step with dt in d_dt (no host synchronisation)
+static int enqueue_step(harm_ctx* c, int precision, int guess, double* d_P, bool with_stats) {
+  static const double CUf[2][4] = {{1.0, 0.0, 0.5, 0.0}, {1.0, 0.0, 1.0, 0.0}};
+  static const double Cun[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 1.0, 0.5}};
+  if (substep(c, precision, guess, 0, 2, d_P, d_P, c->d_pk, c->d_pflag, CUf[0], Cun[0], c->d_dtslots, with_stats)) return 1;
+  if (hp_bound(c, c->d_pk, nullptr)) return 1;
+  if (hp_fixup(c, c->d_pk, c->d_pflag)) return 1;
+  if (hp_bound(c, c->d_pk, nullptr)) return 1;
+  if (substep(c, precision, guess, 1, 2, d_P, c->d_pk, d_P, c->d_pflag, CUf[1], Cun[1], c->d_dtslots + 3, with_stats))
+    return 1;
+  if (hp_bound(c, d_P, nullptr)) return 1;
+  if (hp_fixup(c, d_P, c->d_pflag)) return 1;
+  if (hp_bound(c, d_P, nullptr)) return 1;
+  return hp_finalize_dt(c, c->d_dt, c->d_ndt, 2);
+}
+
+extern "C" int harm_b200_step_n(harm_ctx* c, int precision, int guess, double* d_P, int nsteps, double* dt,
+                                harm_stats* stats) {
+  Dims d = dims_of(c->g);
+  c->h_scal[0] = *dt;
+  CK(cudaMemcpyAsync(c->d_dt, c->h_scal, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (stats) CK(cudaMemsetAsync(c->d_stats, 0, 5 * sizeof(double), c->stream));
+  for (int s = 0; s < nsteps; s++)
+    if (enqueue_step(c, precision, guess, d_P, stats != nullptr)) return 1;
+  CK(cudaMemcpyAsync(c->h_scal, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (stats) CK(cudaMemcpyAsync(c->h_scal + 8, c->d_stats, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *dt = c->h_scal[0];
+  add_stats(c, stats, 2.0 * nsteps * (double)d.n1 * d.n2 * d.n3);
+  return 0;
+}
+
+extern "C" int harm_b200_step(harm_ctx* c, int precision, int guess, double* d_P, double* dt, harm_stats* stats) {
+  return harm_b200_step_n(c, precision, guess, d_P, 1, dt, stats);
+}
+
+extern "C" int harm_b200_step_host(harm_ctx* c, int precision, int guess, double* h_P, double* dt, harm_stats* stats) {
+  size_t bytes = NPR * c->cells * sizeof(double);
+  if (!c->d_Pdev) CK(cudaMalloc(&c->d_Pdev, bytes));
+  CK(cudaMemcpyAsync(c->d_Pdev, h_P, bytes, cudaMemcpyHostToDevice, c->stream));
+  if (harm_b200_step_n(c, precision, guess, c->d_Pdev, 1, dt, stats)) return 1;
+  CK(cudaMemcpyAsync(h_P, c->d_Pdev, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+extern "C" int harm_b200_utoprimgen_points(harm_ctx* c, size_t n, int guess, const double* d_U, const double* d_geom,
+                                           double* d_P, int8_t* d_pflag, int32_t* d_iters) {
+  (void)guess;
+  if (n == 0) return 0;
+  if (hp_points(c, n, d_U, d_geom, d_P, d_pflag, d_iters)) return 1;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+// Stage times of one substep (substep 0 of the RK2 step on d_P; results into scratch).
+extern "C" int harm_b200_time_stages(harm_ctx* c, int precision, int guess, const double* d_P, double dt, int reps,
+                                     double* ms) {
+  static const double CUf[4] = {1.0, 0.0, 0.5, 0.0};
+  static const double Cun[4] = {0.0, 0.0, 0.0, 0.0};
+  if (reps < 1) reps = 1;
+  cudaEvent_t ev[6];
+  for (int q = 0; q < 6; q++) CK(cudaEventCreate(&ev[q]));
+  c->h_scal[0] = dt;
+  CK(cudaMemcpyAsync(c->d_dt, c->h_scal, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  for (int q = 0; q < 5; q++) ms[q] = 0.0;
+  StepCoef sc;
+  sc.CUf0 = CUf[0]; sc.CUf2 = CUf[2]; sc.Cun0 = Cun[0]; sc.Cun1 = Cun[1]; sc.Cun2 = Cun[2];
+  sc.finalstep = 0; sc.guess = guess;
+  for (int r = 0; r < reps; r++) {
+    CK(cudaEventRecord(ev[0], c->stream));
+    if (precision == HARM_PREC_FP64) {
+      if (hp_fluxes_fp64(c, d_P, c->d_F[0], c->d_F[1], c->d_F[2], c->d_emf, c->d_dtslots)) return 1;
+    } else {
+      if (hp_fluxes_mixed(c, d_P, c->d_Ff[0], c->d_Ff[1], c->d_Ff[2], c->d_emff, c->d_dtslots)) return 1;
+    }
+    CK(cudaEventRecord(ev[1], c->stream));
+    CK(cudaEventRecord(ev[2], c->stream));
+    if (precision == HARM_PREC_FP64) {
+      if (hp_update_fp64(c, sc, d_P, d_P, c->d_pk, c->d_pflag, nullptr)) return 1;
+    } else {
+      if (hp_update_mixed(c, sc, d_P, d_P, c->d_pk, c->d_pflag, nullptr)) return 1;
+    }
+    CK(cudaEventRecord(ev[3], c->stream));
+    if (hp_bound(c, c->d_pk, nullptr)) return 1;
+    CK(cudaEventRecord(ev[4], c->stream));
+    if (hp_fixup(c, c->d_pk, c->d_pflag)) return 1;
+    CK(cudaEventRecord(ev[5], c->stream));
+    CK(cudaEventSynchronize(ev[5]));
+    float t;
+    for (int q = 0; q < 5; q++) {
+      CK(cudaEventElapsedTime(&t, ev[q], ev[q + 1]));
+      ms[q] += t / reps;
+    }
+  }
+  CK(cudaMemsetAsync(c->d_dtslots, 0xFF, 6 * sizeof(unsigned long long), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int q = 0; q < 6; q++) cudaEventDestroy(ev[q]);
+  return 0;
+}

@@ -1,0 +1,446 @@
+// harm_common.cuh -- shared structures, device helpers and kernel templates of the step.
+//
+// The kernel templates are instantiated per arithmetic path in separate translation units:
+//   harm_path_fp64.cu   FP64 path, compiled without FMA contraction (-fmad=false) so that
+//                       every FP64 operation is the IEEE operation the C restatement
+//                       performs, in the same order;
+//   harm_path_mixed.cu  mixed path (FP32 reconstruction/HLL/CT, FP64 update and
+//                       inversion), compiled with contraction.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+#include "harm_b200.h"
+#include "harm_device.cuh"
+#include "harm_invert.cuh"
+#include "harm_ctx.cuh"
+
+using namespace hb;
+
+int hb_seterr(const char* what, cudaError_t e);
+#define CK(call)                                        \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return hb_seterr(#call, e_); \
+  } while (0)
+
+// ------------------------------------------------------------------ indexing helpers
+
+struct Dims {
+  int n1, n2, n3, ng, ng3, n1e, n2e, n3e;
+  size_t plane, cells;
+};
+
+static inline Dims dims_of(const harm_grid& g) {
+  Dims d;
+  d.n1 = g.n1; d.n2 = g.n2; d.n3 = g.n3; d.ng = g.ng; d.ng3 = g.ng3;
+  d.n1e = g.n1e; d.n2e = g.n2e; d.n3e = g.n3e;
+  d.plane = (size_t)g.n1e * g.n2e;
+  d.cells = d.plane * g.n3e;
+  return d;
+}
+
+__device__ __forceinline__ size_t cidx(const Dims& d, int ii, int jj, int kk) {
+  return ((size_t)kk * d.n2e + jj) * d.n1e + ii;
+}
+
+struct Phys {
+  double gam, cour, gammamax, gammafail, defcon, safe;
+  double dx1, dx2, dx3;
+};
+
+static inline Phys phys_of(const harm_grid& g) {
+  Phys p;
+  p.gam = g.gam; p.cour = g.cour; p.gammamax = g.gammamax; p.gammafail = g.gammafail;
+  p.defcon = g.defcon; p.safe = g.safe;
+  p.dx1 = g.dx[1]; p.dx2 = g.dx[2]; p.dx3 = g.dx[3];
+  return p;
+}
+
+__device__ __forceinline__ unsigned long long dbl_bits(double x) {
+  return (unsigned long long)__double_as_longlong(x);
+}
+
+// block-wide min of a positive double, then one atomicMin on its bits
+__device__ __forceinline__ void block_min_atomic(double v, unsigned long long* slot) {
+  __shared__ double red[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    int nw = (blockDim.x + 31) >> 5;
+    v = (lane < nw) ? red[lane] : 1.e300;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (lane == 0 && v < 1.e300) atomicMin(slot, dbl_bits(v));
+  }
+}
+
+__device__ __forceinline__ void warp_add_atomic(double v, double* slot) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(slot, v);
+}
+
+struct FixRec {
+  long long id;
+  double v[5];
+};
+
+static inline unsigned int nblk(long long n, int bs = 256) { return (unsigned int)((n + bs - 1) / bs); }
+
+// ------------------------------------------------------------------ flux kernel
+
+// Face box of direction DIR (active-relative, inclusive): faces bounding active cells in
+// DIR, one transverse ghost layer on each side of every other direction with n>1.
+struct FaceBox {
+  int lo[3], hi[3], cnt[3];
+  long long n;
+};
+
+static inline FaceBox face_box(const Dims& d, int dir) {
+  FaceBox b;
+  int n[3] = {d.n1, d.n2, d.n3};
+  for (int k = 0; k < 3; k++) {
+    if (k == dir - 1) { b.lo[k] = 0; b.hi[k] = n[k]; }
+    else if (n[k] > 1) { b.lo[k] = -1; b.hi[k] = n[k]; }
+    else { b.lo[k] = 0; b.hi[k] = 0; }
+    b.cnt[k] = b.hi[k] - b.lo[k] + 1;
+  }
+  b.n = (long long)b.cnt[0] * b.cnt[1] * b.cnt[2];
+  return b;
+}
+
+template <typename T>
+__device__ __forceinline__ void recon_face_mc(const double* __restrict__ P, size_t cells, size_t c0, long long stride,
+                                              T* pl, T* pr) {
+#pragma unroll
+  for (int p = 0; p < NPR; p++) {
+    const double* base = P + (size_t)p * cells + c0;
+    T ym2 = (T)__ldg(base - 2 * stride), ym1 = (T)__ldg(base - stride), y0 = (T)__ldg(base), yp1 = (T)__ldg(base + stride);
+    T dqm = mc_slope(ym2, ym1, y0), dq0 = mc_slope(ym1, y0, yp1);
+    pl[p] = ym1 + T(0.5) * dqm;
+    pr[p] = y0 - T(0.5) * dq0;
+  }
+}
+
+template <int DIR, typename T, typename GT>
+__global__ void __launch_bounds__(256) k_flux(Dims d, Phys ph, FaceBox fb, const double* __restrict__ P,
+                                              const GT* __restrict__ geom, T* __restrict__ F,
+                                              unsigned long long* __restrict__ dtslot) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double dtij = 1.e300;
+  if (t < fb.n) {
+    int a = (int)(t % fb.cnt[0]);
+    long long r = t / fb.cnt[0];
+    int b = (int)(r % fb.cnt[1]);
+    int c = (int)(r / fb.cnt[1]);
+    int ii = a + fb.lo[0] + d.ng, jj = b + fb.lo[1] + d.ng, kk = c + fb.lo[2] + d.ng3;
+    size_t id = cidx(d, ii, jj, kk);
+    long long stride = (DIR == 1) ? 1 : (DIR == 2) ? (long long)d.n1e : (long long)d.plane;
+    T pl[NPR], pr[NPR];
+    recon_face_mc<T>(P, d.cells, id, stride, pl, pr);
+    constexpr int loc = (DIR == 1) ? HARM_LOC_FACE1 : (DIR == 2) ? HARM_LOC_FACE2 : HARM_LOC_CENT;
+    Geo<T> g;
+    load_geo<T, GT>(geom + (size_t)loc * HARM_NGF * d.plane, d.plane, (size_t)jj * d.n1e + ii, g);
+    const int bp = HARM_B1 + DIR - 1;
+    pl[bp] = pr[bp] = T(0.5) * (pl[bp] + pr[bp]);
+    const T gam = (T)ph.gam, gmax = (T)ph.gammamax;
+    limit_gamma<T>(gmax, pl, g);
+    limit_gamma<T>(gmax, pr, g);
+    State<T> ql, qr;
+    get_state<T>(pl, g, gam, ql);
+    get_state<T>(pr, g, gam, qr);
+    T Fl[NPR], Fr[NPR], Ul[NPR], Ur[NPR];
+    primtoflux<T>(pl, ql, DIR, g, g.gdet, Fl);
+    primtoflux<T>(pl, ql, 0, g, g.gdet, Ul);
+    primtoflux<T>(pr, qr, DIR, g, g.gdet, Fr);
+    primtoflux<T>(pr, qr, 0, g, g.gdet, Ur);
+    T cmaxl, cminl, cmaxr, cminr;
+    vchar<T>(pl, ql, DIR, g, gam, cmaxl, cminl);
+    vchar<T>(pr, qr, DIR, g, gam, cmaxr, cminr);
+    T lmin = fmin(cminl, cminr), lmax = fmax(cmaxl, cmaxr);
+    lmin = fabs(fmax(T(0), -lmin));
+    lmax = fabs(fmax(T(0), lmax));
+    const T cmin = lmin, cmax = lmax, ctop = fmax(lmax, lmin);
+    if (cmax + cmin != T(0)) {
+      const T inv = cmax + cmin;
+#pragma unroll
+      for (int p = 0; p < NPR; p++) F[(size_t)p * d.cells + id] = ((cmax * Fl[p] + cmin * Fr[p]) - (cmax * cmin) * (Ur[p] - Ul[p])) / inv;
+    } else {
+#pragma unroll
+      for (int p = 0; p < NPR; p++) F[(size_t)p * d.cells + id] = T(0.5) * ((Fl[p] + Fr[p]) - ctop * (Ur[p] - Ul[p]));
+    }
+    const double dxd = (DIR == 1) ? ph.dx1 : (DIR == 2) ? ph.dx2 : ph.dx3;
+    dtij = ph.cour * dxd / (double)ctop;
+    if (!(dtij > 0.0)) dtij = 1.e300;
+  }
+  block_min_atomic(dtij, dtslot);
+}
+
+// ------------------------------------------------------------------ EMF kernel
+
+template <typename T, typename GT>
+__global__ void __launch_bounds__(256) k_emf(Dims d, const T* __restrict__ F1, const T* __restrict__ F2,
+                                             const T* __restrict__ F3, const GT* __restrict__ geom, T* __restrict__ emf) {
+  const int has3 = d.n3 > 1;
+  const int c1n = d.n1 + 1, c2n = d.n2 + 1, c3n = has3 ? d.n3 + 1 : 1;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)c1n * c2n * c3n) return;
+  int i = (int)(t % c1n);
+  long long r = t / c1n;
+  int j = (int)(r % c2n), k = (int)(r / c2n);
+  int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
+  int km = has3 ? kk - 1 : kk;
+  const size_t cells = d.cells, plane = d.plane;
+  auto ig = [&](int loc, int a, int b) -> T {
+    return (T)__ldg(geom + ((size_t)loc * HARM_NGF + HARM_G_IGDET) * plane + (size_t)b * d.n1e + a);
+  };
+  auto gd = [&](int loc, int a, int b) -> T {
+    return (T)__ldg(geom + ((size_t)loc * HARM_NGF + HARM_G_GDET) * plane + (size_t)b * d.n1e + a);
+  };
+  auto FF = [&](const T* Fa, int pl, int a, int b, int c) -> T { return Fa[(size_t)pl * cells + cidx(d, a, b, c)]; };
+  T f2b3 = FF(F2, HARM_B3, ii, jj, kk) * ig(HARM_LOC_FACE2, ii, jj);
+  T f2b3m = FF(F2, HARM_B3, ii, jj, km) * ig(HARM_LOC_FACE2, ii, jj);
+  T f1b3 = FF(F1, HARM_B3, ii, jj, kk) * ig(HARM_LOC_FACE1, ii, jj);
+  T f1b3m = FF(F1, HARM_B3, ii, jj, km) * ig(HARM_LOC_FACE1, ii, jj);
+  T f1b2 = FF(F1, HARM_B2, ii, jj, kk) * ig(HARM_LOC_FACE1, ii, jj);
+  T f1b2m = FF(F1, HARM_B2, ii, jj - 1, kk) * ig(HARM_LOC_FACE1, ii, jj - 1);
+  T f2b1 = FF(F2, HARM_B1, ii, jj, kk) * ig(HARM_LOC_FACE2, ii, jj);
+  T f2b1m = FF(F2, HARM_B1, ii - 1, jj, kk) * ig(HARM_LOC_FACE2, ii - 1, jj);
+  T e1, e2, e3;
+  if (has3) {
+    T f3b2 = FF(F3, HARM_B2, ii, jj, kk) * ig(HARM_LOC_CENT, ii, jj);
+    T f3b2m = FF(F3, HARM_B2, ii, jj - 1, kk) * ig(HARM_LOC_CENT, ii, jj - 1);
+    T f3b1 = FF(F3, HARM_B1, ii, jj, kk) * ig(HARM_LOC_CENT, ii, jj);
+    T f3b1m = FF(F3, HARM_B1, ii - 1, jj, kk) * ig(HARM_LOC_CENT, ii - 1, jj);
+    e1 = T(0.25) * (+f2b3 + f2b3m - f3b2 - f3b2m);
+    e2 = T(0.25) * (+f3b1 + f3b1m - f1b3 - f1b3m);
+  } else {
+    e1 = T(0.5) * (+f2b3 + f2b3m);
+    e2 = T(0.5) * (-f1b3 - f1b3m);
+  }
+  e3 = T(0.25) * (+f1b2 + f1b2m - f2b1 - f2b1m);
+  size_t id = cidx(d, ii, jj, kk);
+  emf[id] = e1 * gd(HARM_LOC_FACE2, ii, jj);
+  emf[cells + id] = e2 * gd(HARM_LOC_FACE1, ii, jj);
+  emf[2 * cells + id] = e3 * gd(HARM_LOC_CORN3, ii, jj);
+}
+
+// ------------------------------------------------------------------ update + inversion
+
+struct StepCoef {
+  double CUf0, CUf2, Cun0, Cun1, Cun2;
+  int finalstep;
+  int guess;
+};
+
+template <typename T>
+__device__ __forceinline__ double dU_cell(const Dims& d, int ii, int jj, int kk, int p, const T* __restrict__ F1,
+                                          const T* __restrict__ F2, const T* __restrict__ F3, const T* __restrict__ emf,
+                                          double idx1, double idx2, double idx3) {
+  const size_t cells = d.cells;
+  const int has3 = d.n3 > 1;
+  const size_t id = cidx(d, ii, jj, kk);
+  const size_t ip = cidx(d, ii + 1, jj, kk), jp = cidx(d, ii, jj + 1, kk), kp = has3 ? cidx(d, ii, jj, kk + 1) : id;
+  double f1a, f1b, f2a, f2b, f3a = 0.0, f3b = 0.0;
+  if (p < HARM_B1) {
+    f1a = (double)F1[(size_t)p * cells + id]; f1b = (double)F1[(size_t)p * cells + ip];
+    f2a = (double)F2[(size_t)p * cells + id]; f2b = (double)F2[(size_t)p * cells + jp];
+    if (has3) { f3a = (double)F3[(size_t)p * cells + id]; f3b = (double)F3[(size_t)p * cells + kp]; }
+  } else {
+    const T* e1 = emf;
+    const T* e2 = emf + cells;
+    const T* e3 = emf + 2 * cells;
+    auto E = [&](const T* e, int a, int b, int c) -> T { return e[cidx(d, a, b, c)]; };
+    const int kq = has3 ? kk + 1 : kk;
+    if (p == HARM_B1) {
+      f1a = 0.0; f1b = 0.0;
+      f2a = (double)(T(-0.5) * (E(e3, ii, jj, kk) + E(e3, ii + 1, jj, kk)));
+      f2b = (double)(T(-0.5) * (E(e3, ii, jj + 1, kk) + E(e3, ii + 1, jj + 1, kk)));
+      if (has3) {
+        f3a = (double)(T(0.5) * (E(e2, ii, jj, kk) + E(e2, ii + 1, jj, kk)));
+        f3b = (double)(T(0.5) * (E(e2, ii, jj, kk + 1) + E(e2, ii + 1, jj, kk + 1)));
+      }
+    } else if (p == HARM_B2) {
+      f1a = (double)(T(0.5) * (E(e3, ii, jj, kk) + E(e3, ii, jj + 1, kk)));
+      f1b = (double)(T(0.5) * (E(e3, ii + 1, jj, kk) + E(e3, ii + 1, jj + 1, kk)));
+      f2a = 0.0; f2b = 0.0;
+      if (has3) {
+        f3a = (double)(T(-0.5) * (E(e1, ii, jj, kk) + E(e1, ii, jj + 1, kk)));
+        f3b = (double)(T(-0.5) * (E(e1, ii, jj, kk + 1) + E(e1, ii, jj + 1, kk + 1)));
+      }
+    } else {
+      f1a = (double)(T(-0.5) * (E(e2, ii, jj, kk) + E(e2, ii, jj, kq)));
+      f1b = (double)(T(-0.5) * (E(e2, ii + 1, jj, kk) + E(e2, ii + 1, jj, kq)));
+      f2a = (double)(T(0.5) * (E(e1, ii, jj, kk) + E(e1, ii, jj, kq)));
+      f2b = (double)(T(0.5) * (E(e1, ii, jj + 1, kk) + E(e1, ii, jj + 1, kq)));
+      f3a = 0.0; f3b = 0.0;
+    }
+  }
+  double d1 = -(f1b - f1a) * idx1;
+  double d2 = -(f2b - f2a) * idx2;
+  double d3 = has3 ? -(f3b - f3a) * idx3 : 0.0;
+  return d1 + d2 + d3;
+}
+
+// connection source (source_conn): dU^{UU+l} = gdet [ T^j_k Gamma^k_{l j} - rho u^j Gamma^t_{l j} ]
+__device__ __forceinline__ void source_conn(const double* pr, const State<double>& q, const Geo<double>& g,
+                                            const double* __restrict__ conn, size_t plane, size_t c2, double* dUg) {
+  double mhd[4][4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    double F[NPR];
+    primtoflux<double>(pr, q, j, g, 1.0, F);
+#pragma unroll
+    for (int k = 0; k < 4; k++) mhd[j][k] = F[HARM_UU + k];
+  }
+#pragma unroll
+  for (int l = 0; l < 4; l++) {
+    double s = 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int k = 0; k < 4; k++) s += mhd[j][k] * __ldg(conn + (size_t)((k * 4 + l) * 4 + j) * plane + c2);
+#pragma unroll
+    for (int j = 0; j < 4; j++) s += -pr[HARM_RHO] * q.ucon[j] * __ldg(conn + (size_t)((0 * 4 + l) * 4 + j) * plane + c2);
+    dUg[HARM_UU + l] = g.gdet * s;
+  }
+  dUg[HARM_RHO] = g.gdet * 0.0;
+  dUg[HARM_B1] = g.gdet * 0.0;
+  dUg[HARM_B2] = g.gdet * 0.0;
+  dUg[HARM_B3] = g.gdet * 0.0;
+}
+
+// fixup1zone with FIXUPTYPE 1; returns floor-hit indicator, updates pr/flag/iters
+__device__ __forceinline__ int fixup1zone(double* pr, const Geo<double>& g, double rhofl, double ufl, double gam,
+                                          double gammamax, double gammafail, int8_t& flag, int& iters) {
+  double prnew[NPR];
+  int did = 0;
+  rhofl = (rhofl < kSMALL) ? kSMALL : rhofl;
+  ufl = (ufl < kSMALL) ? kSMALL : ufl;
+#pragma unroll
+  for (int pl = 0; pl < NPR; pl++) prnew[pl] = pr[pl];
+  if (rhofl > pr[HARM_RHO]) { did = 1; prnew[HARM_RHO] = rhofl; }
+  if (ufl > pr[HARM_UU]) { did = 1; prnew[HARM_UU] = ufl; }
+  if (did) {
+    State<double> q, dq;
+    double U[NPR], dU[NPR], dpr[NPR];
+#pragma unroll
+    for (int pl = 0; pl < NPR; pl++) dpr[pl] = 0.0;
+    get_state<double>(pr, g, gam, q);
+    primtoflux<double>(pr, q, 0, g, 1.0, U);
+    dpr[HARM_RHO] = prnew[HARM_RHO] - pr[HARM_RHO];
+    dpr[HARM_UU] = prnew[HARM_UU] - pr[HARM_UU];
+    get_state<double>(dpr, g, gam, dq);
+    primtoflux<double>(dpr, dq, 0, g, 1.0, dU);
+#pragma unroll
+    for (int pl = 0; pl < NPR; pl++) U[pl] += dU[pl];
+    iters += utoprimgen(U, g, 1.0, pr, flag, gam, gammafail, false, 0.0, nullptr);
+    if (flag > 0) {
+#pragma unroll
+      for (int pl = 0; pl < NPR; pl++) pr[pl] = prnew[pl];
+    }
+  }
+  limit_gamma<double>(gammamax, pr, g);
+  return did;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_update(Dims d, Phys ph, StepCoef sc, const double* __restrict__ dtp,
+                                                const double* pi, const double* pb, double* pf,
+                                                int8_t* __restrict__ pflag, const T* __restrict__ F1,
+                                                const T* __restrict__ F2, const T* __restrict__ F3,
+                                                const T* __restrict__ emf, const double* __restrict__ geom,
+                                                const double* __restrict__ conn, const double* __restrict__ aux,
+                                                const float* __restrict__ mlp, double* __restrict__ stats) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long ncell = (long long)d.n1 * d.n2 * d.n3;
+  double iters_d = 0.0, fails = 0.0, floors = 0.0, fallbacks = 0.0;
+  if (t < ncell) {
+    int i = (int)(t % d.n1);
+    long long r = t / d.n1;
+    int j = (int)(r % d.n2), k = (int)(r / d.n2);
+    int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
+    const size_t id = cidx(d, ii, jj, kk), c2 = (size_t)jj * d.n1e + ii;
+    Geo<double> g;
+    load_geo<double, double>(geom, d.plane, c2, g);
+    double pri[NPR], prb[NPR];
+#pragma unroll
+    for (int p = 0; p < NPR; p++) { pri[p] = pi[(size_t)p * d.cells + id]; prb[p] = pb[(size_t)p * d.cells + id]; }
+    State<double> qi, qb;
+    get_state<double>(pri, g, ph.gam, qi);
+    double Ui[NPR];
+    primtoflux<double>(pri, qi, 0, g, g.gdet, Ui);
+    const double idx1 = 1.0 / ph.dx1, idx2 = 1.0 / ph.dx2, idx3 = 1.0 / ph.dx3;
+    get_state<double>(prb, g, ph.gam, qb);
+    double dUg[NPR];
+    source_conn(prb, qb, g, conn, d.plane, c2, dUg);
+    const double dt = *dtp;
+    double U[NPR];
+#pragma unroll
+    for (int p = 0; p < NPR; p++) {
+      double dU = dU_cell<T>(d, ii, jj, kk, p, F1, F2, F3, emf, idx1, idx2, idx3);
+      double Uf = sc.CUf0 * Ui[p] + sc.CUf2 * dt * (dU + dUg[p]);
+      double ucum = sc.Cun0 * Ui[p] + sc.Cun1 * dt * (dU + dUg[p]) + sc.Cun2 * Uf;
+      U[p] = sc.finalstep ? ucum : Uf;
+    }
+    int8_t flag = 0;
+    double pr[NPR];
+#pragma unroll
+    for (int p = 0; p < NPR; p++) pr[p] = prb[p];
+    bool gfail = false;
+    int it = utoprimgen(U, g, g.igdet, pr, flag, ph.gam, ph.gammafail, false, 0.0, &gfail);
+    if (gfail) fallbacks = 1.0;
+    if (flag > 0) fails = 1.0;
+    floors = (double)fixup1zone(pr, g, __ldg(aux + (size_t)HARM_AUX_RHOFLOOR * d.plane + c2),
+                                __ldg(aux + (size_t)HARM_AUX_UFLOOR * d.plane + c2), ph.gam, ph.gammamax, ph.gammafail,
+                                flag, it);
+    iters_d = (double)it;
+    pflag[id] = flag;
+#pragma unroll
+    for (int p = 0; p < NPR; p++) pf[(size_t)p * d.cells + id] = pr[p];
+  }
+  if (stats) {
+    warp_add_atomic(iters_d, stats + 0);
+    warp_add_atomic(fails, stats + 3);
+    warp_add_atomic(floors, stats + 4);
+    warp_add_atomic(fallbacks, stats + 2);
+  }
+}
+
+// field fluxes of the faces of active cells from the EMFs (for the standalone fluxcalc)
+template <typename T>
+__global__ void k_emf_to_flux(Dims d, const T* __restrict__ emf, T* F1, T* F2, T* F3) {
+  const int has3 = d.n3 > 1;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int c1n = d.n1 + 1, c2n = d.n2 + 1, c3n = has3 ? d.n3 + 1 : 1;
+  if (t >= (long long)c1n * c2n * c3n) return;
+  int i = (int)(t % c1n);
+  long long r = t / c1n;
+  int j = (int)(r % c2n), k = (int)(r / c2n);
+  int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
+  const size_t cells = d.cells;
+  auto E = [&](int q, int a, int b, int cc) -> T { return emf[(size_t)q * cells + cidx(d, a, b, cc)]; };
+  size_t id = cidx(d, ii, jj, kk);
+  int kp = has3 ? kk + 1 : kk;
+  if (k < d.n3 && j < d.n2) {
+    F1[(size_t)HARM_B1 * cells + id] = T(0);
+    F1[(size_t)HARM_B2 * cells + id] = T(0.5) * (E(2, ii, jj, kk) + E(2, ii, jj + 1, kk));
+    F1[(size_t)HARM_B3 * cells + id] = T(-0.5) * (E(1, ii, jj, kk) + E(1, ii, jj, kp));
+  }
+  if (k < d.n3 && i < d.n1) {
+    F2[(size_t)HARM_B1 * cells + id] = T(-0.5) * (E(2, ii, jj, kk) + E(2, ii + 1, jj, kk));
+    F2[(size_t)HARM_B2 * cells + id] = T(0);
+    F2[(size_t)HARM_B3 * cells + id] = T(0.5) * (E(0, ii, jj, kk) + E(0, ii, jj, kp));
+  }
+  if (has3 && i < d.n1 && j < d.n2) {
+    F3[(size_t)HARM_B1 * cells + id] = T(0.5) * (E(1, ii, jj, kk) + E(1, ii + 1, jj, kk));
+    F3[(size_t)HARM_B2 * cells + id] = T(-0.5) * (E(0, ii, jj, kk) + E(0, ii, jj + 1, kk));
+    F3[(size_t)HARM_B3 * cells + id] = T(0);
+  }
+}
+

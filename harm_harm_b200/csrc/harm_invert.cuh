@@ -98,7 +98,7 @@ __device__ __forceinline__ bool errcheck(double errx, double x0, const InvC& c) 
 __device__ __forceinline__ int extracheck(double x0, const InvC& c) { return ultrarel(x0, c) ? 4 : 2; }
 
 // general_newton_raphson, n=1, no line search.  Returns 0/1 (retval), updates flag.
-__device__ int newton(int8_t& flag, double& xio, const InvC& c, int& lntries, int& nstroke) {
+static __device__ int newton(int8_t& flag, double& xio, const InvC& c, int& lntries, int& nstroke) {
   double x = xio, x_old = x, x_older = x;
   double dx, dx_old = kVERYBIG, resid, jac, f = 1.0, errx = 1.0, damp = 1.0;
   int n_iter = 0, diddamp = 0, i_extra = 0, doing_extra = 0;
@@ -148,7 +148,7 @@ __device__ int newton(int8_t& flag, double& xio, const InvC& c, int& lntries, in
 
 // Setup scalars and the previous-state guess; returns retval contribution of the guess.
 // U and prim are alpha-scaled as in Utoprim_jon_nonrelcompat_inputnorestmass.
-__device__ int inv_setup(const double* U, const Geo<double>& g, const double* prim, InvC& c, double Qtcon[4],
+static __device__ int inv_setup(const double* U, const Geo<double>& g, const double* prim, InvC& c, double Qtcon[4],
                          double Bcon[4], double& Wp_last, int8_t& flag) {
   c.D = U[HARM_RHO];
   Bcon[0] = 0.;
@@ -209,7 +209,7 @@ __device__ int inv_setup(const double* U, const Geo<double>& g, const double* pr
 }
 
 // verify_Wlast and the utsq>=0 guard loop of set_guess_Wp
-__device__ int inv_verify_guess(double& Wp_last, const InvC& c, int8_t& flag) {
+static __device__ int inv_verify_guess(double& Wp_last, const InvC& c, int8_t& flag) {
   double W_last = Wp_last + c.D;
   if (W_last < -(c.D) || Wp_last < 0) { W_last = -(c.D); Wp_last = 0; }
   for (int inc = 0; vsqgtr1(W_last, c) && inc < 10; inc++) {
@@ -230,7 +230,7 @@ __device__ int inv_verify_guess(double& Wp_last, const InvC& c, int8_t& flag) {
 }
 
 // W' -> primitives (Wp2prim), including check_Wp's flags.  prim is alpha-scaled.
-__device__ int inv_finish(double Wp, const InvC& c, const double* Qtcon, const double* Bcon, double* prim, int8_t& flag) {
+static __device__ int inv_finish(double Wp, const InvC& c, const double* Qtcon, const double* Bcon, double* prim, int8_t& flag) {
   if (Wp == kBIG) flag = HARM_UTOPRIMFAILCONVRET + 1;
   else if (Wp <= -(c.D)) flag = HARM_UTOPRIMFAILCONVRET + 1;
   else if (Wp / c.w1 > c.gsq_too_big) flag = HARM_UTOPRIMFAILCONVW;
@@ -260,7 +260,7 @@ __device__ int inv_finish(double Wp, const InvC& c, const double* Qtcon, const d
 
 // Hot or cold Jon inversion on geometry-free U (Utoprim_jon_nonrelcompat_inputnorestmass).
 // `wpguess` >= 0 replaces the previous-state W' when use_guess is set.
-__device__ void utoprim_jon(bool cold, const double* Ugf, const Geo<double>& g, int8_t& flag, double* prim, double gam,
+static __device__ void utoprim_jon(bool cold, const double* Ugf, const Geo<double>& g, int8_t& flag, double* prim, double gam,
                             double gammafail, int& nstroke, bool use_guess, double wpguess) {
   int lntries = 0;
   double U[NPR], pt[NPR];
@@ -296,7 +296,7 @@ __device__ void utoprim_jon(bool cold, const double* Ugf, const Geo<double>& g, 
 }
 
 // Utoprimgen from UEVOLVE U (igdet scales to geometry-free).  Returns the Newton iterations.
-__device__ int utoprimgen(const double* U, const Geo<double>& g, double igdet, double* pr, int8_t& flag, double gam,
+static __device__ int utoprimgen(const double* U, const Geo<double>& g, double igdet, double* pr, int8_t& flag, double gam,
                           double gammafail, bool use_guess, double wpguess, bool* guess_failed) {
   double Ugf[NPR], pr0[NPR];
 #pragma unroll

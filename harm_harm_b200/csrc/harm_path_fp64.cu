@@ -1,0 +1,320 @@
+// harm_path_fp64.cu -- FP64 path of the step (compiled with -fmad=false) and the FP64
+// kernels shared by both paths: boundary conditions, fixups, dt finalisation, point
+// inversions.
+#include "harm_common.cuh"
+#include "harm_paths.h"
+
+// copy p_b into the ghost zones of p_f (advance.c:654 copies the full grid)
+__global__ void k_copy_ghosts(Dims d, const double* __restrict__ pb, double* __restrict__ pf) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)d.cells) return;
+  int ii = (int)(t % d.n1e);
+  long long r = t / d.n1e;
+  int jj = (int)(r % d.n2e), kk = (int)(r / d.n2e);
+  bool active = ii >= d.ng && ii < d.ng + d.n1 && jj >= d.ng && jj < d.ng + d.n2 && kk >= d.ng3 && kk < d.ng3 + d.n3;
+  if (active) return;
+#pragma unroll
+  for (int p = 0; p < NPR; p++) pf[(size_t)p * d.cells + t] = pb[(size_t)p * d.cells + t];
+}
+
+// ------------------------------------------------------------------ boundary conditions
+
+__global__ void k_bound_x1(Dims d, Phys ph, double* P, int8_t* flag, const double* __restrict__ geom) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)2 * d.ng * d.n2e * d.n3e;
+  if (t >= n) return;
+  int gq = (int)(t % (2 * d.ng));
+  long long r = t / (2 * d.ng);
+  int jj = (int)(r % d.n2e), kk = (int)(r / d.n2e);
+  if (gq < d.ng) {
+    int ii = gq;
+    size_t dst = cidx(d, ii, jj, kk), src = cidx(d, d.ng, jj, kk);
+    if (P)
+      for (int p = 0; p < NPR; p++) P[(size_t)p * d.cells + dst] = P[(size_t)p * d.cells + src];
+    if (flag) flag[dst] = flag[src];
+  } else {
+    int ii = d.ng + d.n1 + (gq - d.ng);
+    size_t dst = cidx(d, ii, jj, kk), src = cidx(d, d.ng + d.n1 - 1, jj, kk);
+    if (flag) flag[dst] = flag[src];
+    if (!P) return;
+    double pr[NPR];
+    for (int p = 0; p < NPR; p++) pr[p] = P[(size_t)p * d.cells + src];
+    Geo<double> g;
+    load_geo<double, double>(geom, d.plane, (size_t)jj * d.n1e + ii, g);
+    // inflow_check_rel4vel (fixup.c:3255) for the outer radial boundary
+    double ucon[4], gamma, qsq;
+    ucon_of<double>(pr, g, ucon, gamma, qsq);
+    if (ucon[1] < 0.) {
+      pr[HARM_U1] /= gamma; pr[HARM_U2] /= gamma; pr[HARM_U3] /= gamma;
+      double alpha = 1. / sqrt(-g.gcon[0]);
+      double betacon = g.gcon[1] * alpha * alpha;
+      pr[HARM_U1] = betacon / alpha;
+      double vsq = 0.;
+      for (int a = 1; a < 4; a++)
+        for (int b = 1; b < 4; b++) vsq += g.gcov[sym(a, b)] * pr[HARM_U1 + a - 1] * pr[HARM_U1 + b - 1];
+      if (vsq < 0.0 && vsq > -2.220446049250313e-16 * 100.0) vsq = 0.0;
+      if (vsq >= 1.0) vsq = 1.0 - 1.0 / (ph.gammamax * ph.gammamax);
+      gamma = 1. / sqrt(1. - vsq);
+      pr[HARM_U1] *= gamma; pr[HARM_U2] *= gamma; pr[HARM_U3] *= gamma;
+    }
+    limit_gamma<double>(ph.gammamax, pr, g);
+    for (int p = 0; p < NPR; p++) P[(size_t)p * d.cells + dst] = pr[p];
+  }
+}
+
+__global__ void k_bound_x2(Dims d, double* P, int8_t* flag) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)2 * d.ng * d.n1e * d.n3e;
+  if (t >= n) return;
+  int ii = (int)(t % d.n1e);
+  long long r = t / d.n1e;
+  int gq = (int)(r % (2 * d.ng)), kk = (int)(r / (2 * d.ng));
+  int k = kk - d.ng3;
+  int ks = (d.n3 > 1) ? ((k + d.n3 / 2) % d.n3 + d.n3) % d.n3 + d.ng3 : kk;
+  int jj, js;
+  if (gq < d.ng) { jj = gq; js = 2 * d.ng - 1 - jj; }
+  else { jj = d.ng + d.n2 + (gq - d.ng); js = 2 * (d.ng + d.n2) - 1 - jj; }
+  size_t dst = cidx(d, ii, jj, kk), src = cidx(d, ii, js, ks);
+  if (flag) flag[dst] = flag[src];
+  if (!P) return;
+  for (int p = 0; p < NPR; p++) {
+    double v = P[(size_t)p * d.cells + src];
+    if (p == HARM_U2 || p == HARM_B2) v = -v;
+    P[(size_t)p * d.cells + dst] = v;
+  }
+}
+
+__global__ void k_bound_x3(Dims d, double* P, int8_t* flag) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)2 * d.ng3 * d.plane;
+  if (t >= n) return;
+  int ii = (int)(t % d.n1e);
+  long long r = t / d.n1e;
+  int jj = (int)(r % d.n2e), gq = (int)(r / d.n2e);
+  int kk, ks;
+  if (gq < d.ng3) { kk = gq; ks = kk + d.n3; }
+  else { kk = d.ng3 + d.n3 + (gq - d.ng3); ks = kk - d.n3; }
+  size_t dst = cidx(d, ii, jj, kk), src = cidx(d, ii, jj, ks);
+  if (flag) flag[dst] = flag[src];
+  if (P)
+    for (int p = 0; p < NPR; p++) P[(size_t)p * d.cells + dst] = P[(size_t)p * d.cells + src];
+}
+
+// ------------------------------------------------------------------ post_fixup
+
+
+__global__ void __launch_bounds__(256) k_fixup_compute(Dims d, Phys ph, const double* __restrict__ P,
+                                                       const int8_t* __restrict__ flag, const double* __restrict__ geom,
+                                                       FixRec* __restrict__ recs, unsigned int* __restrict__ nrec,
+                                                       unsigned int cap) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)d.n1 * d.n2 * d.n3) return;
+  int i = (int)(t % d.n1);
+  long long r = t / d.n1;
+  int j = (int)(r % d.n2), k = (int)(r / d.n2);
+  int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
+  size_t id = cidx(d, ii, jj, kk);
+  int8_t f = flag[id];
+  if (f <= 0) return;
+  int startpl, endpl;
+  const bool u2 = (f == HARM_UTOPRIMFAILU2AVG1 || f == HARM_UTOPRIMFAILU2AVG2);
+  if (u2 || f == 13) { startpl = endpl = HARM_UU; }
+  else { startpl = HARM_RHO; endpl = HARM_U3; }
+  const int s1 = d.n1 > 1, s2 = d.n2 > 1, s3 = d.n3 > 1;
+  const int rnx = s1 ? 3 : 1, rny = s2 ? 3 : 1;
+  const int npairs = ((s1 + s2 + s3) == 3 ? 27 : (s1 + s2 + s3) == 2 ? 9 : 3) / 2;
+  double sum0[5] = {0, 0, 0, 0, 0}, sum1[5] = {0, 0, 0, 0, 0}, lastmin[5];
+  for (int p = 0; p < 5; p++) lastmin[p] = 1E50;
+  int numavg0 = 0, numavg1 = 0;
+  const double ref = P[(size_t)HARM_UU * d.cells + id];
+  for (int qq = 0; qq < npairs; qq++) {
+    int di = (qq % rnx) - s1, dj = ((qq % (rnx * rny)) / rnx) - s2, dk = (qq / (rnx * rny)) - s3;
+    size_t a = cidx(d, ii + di, jj + dj, kk + dk), b = cidx(d, ii - di, jj - dj, kk - dk);
+    int thisok = flag[a] <= 0, thatok = flag[b] <= 0;
+    numavg0 += thisok + thatok;
+    for (int p = startpl; p <= endpl; p++) {
+      double fa = P[(size_t)p * d.cells + a], fb = P[(size_t)p * d.cells + b];
+      if (!u2) {
+        double add = fa * thisok + fb * thatok;
+        if (qq % 2 == 0) sum0[p] += add; else sum1[p] += add;
+      } else if (fa >= ref && fb >= ref) {
+        lastmin[p] = fmin(fmin(lastmin[p], fa), fb);
+        numavg1++;
+      }
+    }
+  }
+  double out[5];
+  for (int p = 0; p < 5; p++) out[p] = P[(size_t)p * d.cells + id];
+  if (!u2) {
+    if (numavg0 != 0)
+      for (int p = startpl; p <= endpl; p++) out[p] = (sum0[p] + sum1[p]) / (double)numavg0;
+  } else {
+    if (numavg1 != 0)
+      for (int p = startpl; p <= endpl; p++) out[p] = lastmin[p];
+  }
+  if (startpl <= HARM_U1 && endpl >= HARM_U3) {
+    Geo<double> g;
+    load_geo<double, double>(geom, d.plane, (size_t)jj * d.n1e + ii, g);
+    double pa[NPR], pv[NPR];
+    for (int p = 0; p < NPR; p++) pa[p] = P[(size_t)p * d.cells + id];
+    for (int p = 0; p < NPR; p++) pv[p] = (p < 5) ? out[p] : pa[p];
+    double ucon[4], gamma, qsq;
+    ucon_of<double>(pa, g, ucon, gamma, qsq);
+    if (gamma > ph.gammamax) gamma = ph.gammamax;
+    limit_gamma<double>(gamma, pv, g);
+    for (int p = 0; p < 5; p++) out[p] = pv[p];
+  }
+  unsigned int slot = atomicAdd(nrec, 1u);
+  if (slot < cap) {
+    recs[slot].id = (long long)id;
+    for (int p = 0; p < 5; p++) recs[slot].v[p] = out[p];
+  }
+}
+
+__global__ void k_fixup_apply(Dims d, double* __restrict__ P, const FixRec* __restrict__ recs,
+                              const unsigned int* __restrict__ nrec, unsigned int cap) {
+  unsigned int n = *nrec;
+  if (n > cap) n = cap;
+  for (unsigned int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    size_t id = (size_t)recs[s].id;
+    for (int p = 0; p < 5; p++) P[(size_t)p * d.cells + id] = recs[s].v[p];
+  }
+}
+
+// ------------------------------------------------------------------ dt
+
+// slots[6]: per substep s (0,1) and direction d the atomic min of cour dx/ctop.
+__global__ void k_finalize_dt(Phys ph, unsigned long long* slots, double* dt, double* ndt_out, int nsub) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double last = 1.e100;
+  for (int s = 0; s < nsub; s++) {
+    double nd[3];
+    for (int q = 0; q < 3; q++) {
+      unsigned long long b = slots[s * 3 + q];
+      nd[q] = (b == 0xFFFFFFFFFFFFFFFFull) ? 1.e100 : __longlong_as_double((long long)b);
+    }
+    double wavedt = 1. / (1. / nd[0] + 1. / nd[1] + 1. / nd[2]);
+    double ndt = ph.defcon * fmin(wavedt, 1.e100);
+    if (ndt_out) ndt_out[s] = ndt;
+    if (ndt < last) last = ndt;
+  }
+  if (dt) {
+    double cur = *dt;
+    if (last > ph.safe * cur) last = ph.safe * cur;
+    *dt = last;
+  }
+  for (int q = 0; q < 3 * nsub; q++) slots[q] = 0xFFFFFFFFFFFFFFFFull;
+}
+
+// ------------------------------------------------------------------ points inversion
+
+__global__ void k_utoprim_points(size_t n, Phys ph, const double* __restrict__ U, const double* __restrict__ geom,
+                                 double* __restrict__ P, int8_t* __restrict__ pflag, int32_t* __restrict__ iters) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  Geo<double> g;
+  load_geo<double, double>(geom, n, t, g);
+  double u[NPR], pr[NPR];
+  for (int p = 0; p < NPR; p++) { u[p] = U[(size_t)p * n + t]; pr[p] = P[(size_t)p * n + t]; }
+  int8_t flag = 0;
+  int it = utoprimgen(u, g, g.igdet, pr, flag, ph.gam, ph.gammafail, false, 0.0, nullptr);
+  for (int p = 0; p < NPR; p++) P[(size_t)p * n + t] = pr[p];
+  pflag[t] = flag;
+  if (iters) iters[t] = it;
+}
+
+
+// ------------------------------------------------------------------ launchers
+
+int hp_fluxes_fp64(harm_ctx* c, const double* pb, double* F1, double* F2, double* F3, double* emf,
+                   unsigned long long* slots) {
+  Dims d = dims_of(c->g);
+  Phys ph = phys_of(c->g);
+  FaceBox b1 = face_box(d, 1), b2 = face_box(d, 2), b3 = face_box(d, 3);
+  k_flux<1, double, double><<<nblk(b1.n), 256, 0, c->stream>>>(d, ph, b1, pb, c->d_geom, F1, slots + 0);
+  k_flux<2, double, double><<<nblk(b2.n), 256, 0, c->stream>>>(d, ph, b2, pb, c->d_geom, F2, slots + 1);
+  c->launches += 2;
+  if (d.n3 > 1) {
+    k_flux<3, double, double><<<nblk(b3.n), 256, 0, c->stream>>>(d, ph, b3, pb, c->d_geom, F3, slots + 2);
+    c->launches++;
+  }
+  long long nc = (long long)(d.n1 + 1) * (d.n2 + 1) * (d.n3 > 1 ? d.n3 + 1 : 1);
+  k_emf<double, double><<<nblk(nc), 256, 0, c->stream>>>(d, F1, F2, F3, c->d_geom, emf);
+  c->launches++;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int hp_update_fp64(harm_ctx* c, const StepCoef& sc, const double* pi, const double* pb, double* pf, int8_t* pflag,
+                   double* stats) {
+  Dims d = dims_of(c->g);
+  Phys ph = phys_of(c->g);
+  long long ncell = (long long)d.n1 * d.n2 * d.n3;
+  k_update<double><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, sc, c->d_dt, pi, pb, pf, pflag, c->d_F[0], c->d_F[1],
+                                                       c->d_F[2], c->d_emf, c->d_geom, c->d_conn, c->d_aux, c->d_mlp,
+                                                       stats);
+  c->launches++;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int hp_emf_to_flux_fp64(harm_ctx* c, const double* emf, double* F1, double* F2, double* F3) {
+  Dims d = dims_of(c->g);
+  long long nc = (long long)(d.n1 + 1) * (d.n2 + 1) * (d.n3 > 1 ? d.n3 + 1 : 1);
+  k_emf_to_flux<double><<<nblk(nc), 256, 0, c->stream>>>(d, emf, F1, F2, F3);
+  c->launches++;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int hp_bound(harm_ctx* c, double* P, int8_t* flag) {
+  Dims d = dims_of(c->g);
+  Phys ph = phys_of(c->g);
+  k_bound_x1<<<nblk(2LL * d.ng * d.n2e * d.n3e), 256, 0, c->stream>>>(d, ph, P, flag, c->d_geom);
+  k_bound_x2<<<nblk(2LL * d.ng * d.n1e * d.n3e), 256, 0, c->stream>>>(d, P, flag);
+  c->launches += 2;
+  if (d.n3 > 1) {
+    k_bound_x3<<<nblk(2LL * d.ng3 * (long long)d.plane), 256, 0, c->stream>>>(d, P, flag);
+    c->launches++;
+  }
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int hp_copy_ghosts(harm_ctx* c, const double* pb, double* pf) {
+  Dims d = dims_of(c->g);
+  k_copy_ghosts<<<nblk((long long)d.cells), 256, 0, c->stream>>>(d, pb, pf);
+  c->launches++;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int hp_fixup(harm_ctx* c, double* pf, int8_t* pflag) {
+  Dims d = dims_of(c->g);
+  Phys ph = phys_of(c->g);
+  if (hp_bound(c, nullptr, pflag)) return 1;
+  CK(cudaMemsetAsync(c->d_nrec, 0, sizeof(unsigned int), c->stream));
+  long long ncell = (long long)d.n1 * d.n2 * d.n3;
+  k_fixup_compute<<<nblk(ncell), 256, 0, c->stream>>>(d, ph, pf, pflag, c->d_geom, (FixRec*)c->d_fixrec, c->d_nrec,
+                                                       c->fix_cap);
+  k_fixup_apply<<<4 * 148, 256, 0, c->stream>>>(d, pf, (const FixRec*)c->d_fixrec, c->d_nrec, c->fix_cap);
+  c->launches += 2;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int hp_finalize_dt(harm_ctx* c, double* dt, double* ndt_out, int nsub) {
+  Phys ph = phys_of(c->g);
+  k_finalize_dt<<<1, 32, 0, c->stream>>>(ph, c->d_dtslots, dt, ndt_out, nsub);
+  c->launches++;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int hp_points(harm_ctx* c, size_t n, const double* U, const double* geom, double* P, int8_t* pflag, int32_t* iters) {
+  Phys ph = phys_of(c->g);
+  k_utoprim_points<<<nblk((long long)n), 256, 0, c->stream>>>(n, ph, U, geom, P, pflag, iters);
+  c->launches++;
+  CK(cudaGetLastError());
+  return 0;
+}

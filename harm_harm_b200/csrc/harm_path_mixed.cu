@@ -1,0 +1,36 @@
+// harm_path_mixed.cu -- mixed-precision path of the step: FP32 reconstruction, HLL and
+// flux-CT; FP64 conserved update, sources and inversion (compiled with FMA contraction).
+#include "harm_common.cuh"
+#include "harm_paths.h"
+
+int hp_fluxes_mixed(harm_ctx* c, const double* pb, float* F1, float* F2, float* F3, float* emf,
+                    unsigned long long* slots) {
+  Dims d = dims_of(c->g);
+  Phys ph = phys_of(c->g);
+  FaceBox b1 = face_box(d, 1), b2 = face_box(d, 2), b3 = face_box(d, 3);
+  k_flux<1, float, float><<<nblk(b1.n), 256, 0, c->stream>>>(d, ph, b1, pb, c->d_geomf, F1, slots + 0);
+  k_flux<2, float, float><<<nblk(b2.n), 256, 0, c->stream>>>(d, ph, b2, pb, c->d_geomf, F2, slots + 1);
+  c->launches += 2;
+  if (d.n3 > 1) {
+    k_flux<3, float, float><<<nblk(b3.n), 256, 0, c->stream>>>(d, ph, b3, pb, c->d_geomf, F3, slots + 2);
+    c->launches++;
+  }
+  long long nc = (long long)(d.n1 + 1) * (d.n2 + 1) * (d.n3 > 1 ? d.n3 + 1 : 1);
+  k_emf<float, float><<<nblk(nc), 256, 0, c->stream>>>(d, F1, F2, F3, c->d_geomf, emf);
+  c->launches++;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int hp_update_mixed(harm_ctx* c, const StepCoef& sc, const double* pi, const double* pb, double* pf, int8_t* pflag,
+                    double* stats) {
+  Dims d = dims_of(c->g);
+  Phys ph = phys_of(c->g);
+  long long ncell = (long long)d.n1 * d.n2 * d.n3;
+  k_update<float><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, sc, c->d_dt, pi, pb, pf, pflag, c->d_Ff[0], c->d_Ff[1],
+                                                      c->d_Ff[2], c->d_emff, c->d_geom, c->d_conn, c->d_aux, c->d_mlp,
+                                                      stats);
+  c->launches++;
+  CK(cudaGetLastError());
+  return 0;
+}

@@ -1,0 +1,21 @@
+// harm_paths.h -- launch entry points of the two arithmetic paths (host side).
+#pragma once
+#include <stdint.h>
+#include "harm_ctx.cuh"
+
+struct StepCoef;
+
+int hp_fluxes_fp64(harm_ctx* c, const double* pb, double* F1, double* F2, double* F3, double* emf,
+                   unsigned long long* slots);
+int hp_fluxes_mixed(harm_ctx* c, const double* pb, float* F1, float* F2, float* F3, float* emf,
+                    unsigned long long* slots);
+int hp_update_fp64(harm_ctx* c, const StepCoef& sc, const double* pi, const double* pb, double* pf, int8_t* pflag,
+                   double* stats);
+int hp_update_mixed(harm_ctx* c, const StepCoef& sc, const double* pi, const double* pb, double* pf, int8_t* pflag,
+                    double* stats);
+int hp_emf_to_flux_fp64(harm_ctx* c, const double* emf, double* F1, double* F2, double* F3);
+int hp_bound(harm_ctx* c, double* P, int8_t* flag);
+int hp_copy_ghosts(harm_ctx* c, const double* pb, double* pf);
+int hp_fixup(harm_ctx* c, double* pf, int8_t* pflag);
+int hp_finalize_dt(harm_ctx* c, double* dt, double* ndt_out, int nsub);
+int hp_points(harm_ctx* c, size_t n, const double* U, const double* geom, double* P, int8_t* pflag, int32_t* iters);

@@ -210,8 +210,9 @@ int harm_b200_utoprimgen_points(harm_ctx *ctx, size_t n, int guess, const double
                                 int32_t *d_iters);
 
 /* Stage times of one RK substep on d_P (unchanged), averaged over `reps` runs, measured
-   with CUDA events on the context stream: ms[0] flux kernels (all directions), ms[1] EMF
-   kernel, ms[2] update+inversion kernel, ms[3] one bound_prim, ms[4] post_fixup. */
+   with CUDA events on the context stream: ms[0] flux kernels of all directions and the
+   EMF kernel, ms[1] (reserved, 0), ms[2] update+inversion, ms[3] one bound_prim,
+   ms[4] post_fixup. */
 int harm_b200_time_stages(harm_ctx *ctx, int precision, int guess, const double *d_P,
                           double dt, int reps, double ms[5]);
 
