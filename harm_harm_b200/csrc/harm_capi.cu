@@ -65,6 +65,8 @@ extern "C" int harm_b200_create(const harm_grid* g, const double* geom_h, const 
   CK(cudaMalloc(&c->d_emf, 3 * d.cells * sizeof(double)));
   CK(cudaMalloc(&c->d_emff, 3 * d.cells * sizeof(float)));
   CK(cudaMalloc(&c->d_pk, NPR * d.cells * sizeof(double)));
+  CK(cudaMalloc(&c->d_U, NPR * d.cells * sizeof(double)));
+  CK(cudaMalloc(&c->d_rare, (size_t)d.n1 * d.n2 * d.n3 * sizeof(unsigned int)));
   CK(cudaMalloc(&c->d_pflag, d.cells));
   CK(cudaMemset(c->d_pflag, 0, d.cells));
   c->fix_cap = (unsigned int)std::min<size_t>((size_t)d.n1 * d.n2 * d.n3, 0xFFFFFFF0u);
@@ -76,6 +78,7 @@ extern "C" int harm_b200_create(const harm_grid* g, const double* geom_h, const 
   c->d_ndt = c->d_scal + 9;                             // 2
   c->d_stats = c->d_scal + 16;                          // 5
   c->d_nrec = (unsigned int*)(c->d_scal + 24);
+  c->d_nrare = (unsigned int*)(c->d_scal + 25);
   CK(cudaMemset(c->d_dtslots, 0xFF, 6 * sizeof(unsigned long long)));
   CK(cudaMallocHost(&c->h_scal, 64 * sizeof(double)));
   *out = c;
@@ -87,7 +90,7 @@ extern "C" int harm_b200_destroy(harm_ctx* c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   void* ptrs[] = {c->d_geom, c->d_geomf, c->d_conn, c->d_aux, c->d_F[0], c->d_F[1], c->d_F[2], c->d_Ff[0], c->d_Ff[1],
-                  c->d_Ff[2], c->d_emf, c->d_emff, c->d_pk, c->d_pflag, c->d_fixrec, c->d_scal, c->d_Pdev, c->d_mlp,
+                  c->d_Ff[2], c->d_emf, c->d_emff, c->d_pk, c->d_U, c->d_rare, c->d_pflag, c->d_fixrec, c->d_scal, c->d_Pdev, c->d_mlp,
                   c->d_mlp_master, c->d_mlp_adam, c->d_mlp_work};
   for (void* p : ptrs)
     if (p) cudaFree(p);

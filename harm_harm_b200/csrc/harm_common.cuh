@@ -349,17 +349,63 @@ __device__ __forceinline__ int fixup1zone(double* pr, const Geo<double>& g, doub
   return did;
 }
 
+// Conserved update of one substep: U_i = primtoU(p_i), flux divergence (field fluxes from
+// the EMFs), connection source of p_b, RK combination; U (UEVOLVE) to global memory.
 template <typename T>
-__global__ void __launch_bounds__(256) k_update(Dims d, Phys ph, StepCoef sc, const double* __restrict__ dtp,
-                                                const double* pi, const double* pb, double* pf,
-                                                int8_t* __restrict__ pflag, const T* __restrict__ F1,
-                                                const T* __restrict__ F2, const T* __restrict__ F3,
-                                                const T* __restrict__ emf, const double* __restrict__ geom,
-                                                const double* __restrict__ conn, const double* __restrict__ aux,
-                                                const float* __restrict__ mlp, double* __restrict__ stats) {
+__global__ void __launch_bounds__(256, 2) k_conserved(Dims d, Phys ph, StepCoef sc, const double* __restrict__ dtp,
+                                                      const double* __restrict__ pi, const double* __restrict__ pb,
+                                                      const T* __restrict__ F1, const T* __restrict__ F2,
+                                                      const T* __restrict__ F3, const T* __restrict__ emf,
+                                                      const double* __restrict__ geom, const double* __restrict__ conn,
+                                                      double* __restrict__ Uout) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   long long ncell = (long long)d.n1 * d.n2 * d.n3;
-  double iters_d = 0.0, fails = 0.0, floors = 0.0, fallbacks = 0.0;
+  if (t >= ncell) return;
+  int i = (int)(t % d.n1);
+  long long r = t / d.n1;
+  int j = (int)(r % d.n2), k = (int)(r / d.n2);
+  int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
+  const size_t id = cidx(d, ii, jj, kk), c2 = (size_t)jj * d.n1e + ii;
+  Geo<double> g;
+  load_geo<double, double>(geom, d.plane, c2, g);
+  double pr[NPR];
+#pragma unroll
+  for (int p = 0; p < NPR; p++) pr[p] = pi[(size_t)p * d.cells + id];
+  State<double> q;
+  get_state<double>(pr, g, ph.gam, q);
+  double Ui[NPR];
+  primtoflux<double>(pr, q, 0, g, g.gdet, Ui);
+#pragma unroll
+  for (int p = 0; p < NPR; p++) pr[p] = pb[(size_t)p * d.cells + id];
+  get_state<double>(pr, g, ph.gam, q);
+  double dUg[NPR];
+  source_conn(pr, q, g, conn, d.plane, c2, dUg);
+  const double idx1 = 1.0 / ph.dx1, idx2 = 1.0 / ph.dx2, idx3 = 1.0 / ph.dx3;
+  const double dt = *dtp;
+#pragma unroll
+  for (int p = 0; p < NPR; p++) {
+    double dU = dU_cell<T>(d, ii, jj, kk, p, F1, F2, F3, emf, idx1, idx2, idx3);
+    double Uf = sc.CUf0 * Ui[p] + sc.CUf2 * dt * (dU + dUg[p]);
+    double ucum = sc.Cun0 * Ui[p] + sc.Cun1 * dt * (dU + dUg[p]) + sc.Cun2 * Uf;
+    Uout[(size_t)p * d.cells + id] = sc.finalstep ? ucum : Uf;
+  }
+}
+
+// Inversion of one substep, common path: the hot Newton inversion of U with p_b as guess,
+// then, when no floor acts, limit_gamma (the end of fixup1zone).  Cells whose hot inversion
+// failed, or whose density or internal energy falls below a floor, are appended to a list
+// and finished by k_invert_rare, so that the rarely taken branches (cold inversion, the
+// floor re-inversion) neither diverge warps nor enlarge the register footprint here.
+// PATH distinguishes the instantiation of each arithmetic path's translation unit.
+template <int PATH>
+__global__ void __launch_bounds__(256, 2) k_invert(Dims d, Phys ph, const double* __restrict__ U,
+                                                   const double* __restrict__ pb, double* __restrict__ pf,
+                                                   int8_t* __restrict__ pflag, const double* __restrict__ geom,
+                                                   const double* __restrict__ aux, unsigned int* __restrict__ rare,
+                                                   unsigned int* __restrict__ nrare, double* __restrict__ stats) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long ncell = (long long)d.n1 * d.n2 * d.n3;
+  double iters_d = 0.0;
   if (t < ncell) {
     int i = (int)(t % d.n1);
     long long r = t / d.n1;
@@ -368,47 +414,84 @@ __global__ void __launch_bounds__(256) k_update(Dims d, Phys ph, StepCoef sc, co
     const size_t id = cidx(d, ii, jj, kk), c2 = (size_t)jj * d.n1e + ii;
     Geo<double> g;
     load_geo<double, double>(geom, d.plane, c2, g);
-    double pri[NPR], prb[NPR];
+    double Ugf[NPR], pr[NPR];
 #pragma unroll
-    for (int p = 0; p < NPR; p++) { pri[p] = pi[(size_t)p * d.cells + id]; prb[p] = pb[(size_t)p * d.cells + id]; }
-    State<double> qi, qb;
-    get_state<double>(pri, g, ph.gam, qi);
-    double Ui[NPR];
-    primtoflux<double>(pri, qi, 0, g, g.gdet, Ui);
-    const double idx1 = 1.0 / ph.dx1, idx2 = 1.0 / ph.dx2, idx3 = 1.0 / ph.dx3;
-    get_state<double>(prb, g, ph.gam, qb);
-    double dUg[NPR];
-    source_conn(prb, qb, g, conn, d.plane, c2, dUg);
-    const double dt = *dtp;
-    double U[NPR];
-#pragma unroll
-    for (int p = 0; p < NPR; p++) {
-      double dU = dU_cell<T>(d, ii, jj, kk, p, F1, F2, F3, emf, idx1, idx2, idx3);
-      double Uf = sc.CUf0 * Ui[p] + sc.CUf2 * dt * (dU + dUg[p]);
-      double ucum = sc.Cun0 * Ui[p] + sc.Cun1 * dt * (dU + dUg[p]) + sc.Cun2 * Uf;
-      U[p] = sc.finalstep ? ucum : Uf;
-    }
+    for (int p = 0; p < NPR; p++) { Ugf[p] = U[(size_t)p * d.cells + id] * g.igdet; pr[p] = pb[(size_t)p * d.cells + id]; }
     int8_t flag = 0;
-    double pr[NPR];
-#pragma unroll
-    for (int p = 0; p < NPR; p++) pr[p] = prb[p];
-    bool gfail = false;
-    int it = utoprimgen(U, g, g.igdet, pr, flag, ph.gam, ph.gammafail, false, 0.0, &gfail);
-    if (gfail) fallbacks = 1.0;
-    if (flag > 0) fails = 1.0;
-    floors = (double)fixup1zone(pr, g, __ldg(aux + (size_t)HARM_AUX_RHOFLOOR * d.plane + c2),
-                                __ldg(aux + (size_t)HARM_AUX_UFLOOR * d.plane + c2), ph.gam, ph.gammamax, ph.gammafail,
-                                flag, it);
+    int it = 0;
+    utoprim_jon(false, Ugf, g, flag, pr, ph.gam, ph.gammafail, it, false, 0.0);
     iters_d = (double)it;
+    bool defer = (flag != 0);
+    if (!defer) {
+      double rhofl = __ldg(aux + (size_t)HARM_AUX_RHOFLOOR * d.plane + c2);
+      double ufl = __ldg(aux + (size_t)HARM_AUX_UFLOOR * d.plane + c2);
+      rhofl = (rhofl < kSMALL) ? kSMALL : rhofl;
+      ufl = (ufl < kSMALL) ? kSMALL : ufl;
+      defer = (rhofl > pr[HARM_RHO]) || (ufl > pr[HARM_UU]);
+      if (!defer) limit_gamma<double>(ph.gammamax, pr, g);
+    }
+    if (defer) {
+      unsigned int slot = atomicAdd(nrare, 1u);
+      rare[slot] = (unsigned int)t;
+    }
     pflag[id] = flag;
 #pragma unroll
     for (int p = 0; p < NPR; p++) pf[(size_t)p * d.cells + id] = pr[p];
   }
-  if (stats) {
-    warp_add_atomic(iters_d, stats + 0);
-    warp_add_atomic(fails, stats + 3);
-    warp_add_atomic(floors, stats + 4);
-    warp_add_atomic(fallbacks, stats + 2);
+  if (stats) warp_add_atomic(iters_d, stats + 0);
+}
+
+// Inversion, rare path over the listed cells: the cold fallback of a failed hot inversion
+// (trycoldinversion utoprimgen.c:594), then fixup1zone (fixup.c:561) with its floor
+// re-inversion.  p_f holds the hot result, p_b the guess the hot inversion started from.
+template <int PATH>
+__global__ void __launch_bounds__(128) k_invert_rare(Dims d, Phys ph, const double* __restrict__ U,
+                                                     const double* __restrict__ pb, double* __restrict__ pf,
+                                                     int8_t* __restrict__ pflag, const double* __restrict__ geom,
+                                                     const double* __restrict__ aux, const unsigned int* __restrict__ rare,
+                                                     const unsigned int* __restrict__ nrare, double* __restrict__ stats) {
+  const unsigned int n = *nrare;
+  for (unsigned int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    long long t = rare[s];
+    int i = (int)(t % d.n1);
+    long long r = t / d.n1;
+    int j = (int)(r % d.n2), k = (int)(r / d.n2);
+    int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
+    const size_t id = cidx(d, ii, jj, kk), c2 = (size_t)jj * d.n1e + ii;
+    Geo<double> g;
+    load_geo<double, double>(geom, d.plane, c2, g);
+    double pr[NPR];
+#pragma unroll
+    for (int p = 0; p < NPR; p++) pr[p] = pf[(size_t)p * d.cells + id];
+    int8_t flag = pflag[id];
+    int it = 0;
+    double fails = 0.0;
+    if (flag) {
+      fails = 1.0;
+      double Ugf[NPR], prcold[NPR];
+#pragma unroll
+      for (int p = 0; p < NPR; p++) { Ugf[p] = U[(size_t)p * d.cells + id] * g.igdet; prcold[p] = pb[(size_t)p * d.cells + id]; }
+      double pr0uu = prcold[HARM_UU];
+      int8_t cflag = 0;
+      utoprim_jon(true, Ugf, g, cflag, prcold, ph.gam, ph.gammafail, it, false, 0.0);
+      if (cflag <= 0) {
+#pragma unroll
+        for (int p = 0; p < NPR; p++) pr[p] = prcold[p];
+        pr[HARM_UU] = pr0uu;
+        flag = HARM_UTOPRIMFAILU2AVG1;
+      }
+    }
+    double floors = (double)fixup1zone(pr, g, __ldg(aux + (size_t)HARM_AUX_RHOFLOOR * d.plane + c2),
+                                       __ldg(aux + (size_t)HARM_AUX_UFLOOR * d.plane + c2), ph.gam, ph.gammamax,
+                                       ph.gammafail, flag, it);
+    pflag[id] = flag;
+#pragma unroll
+    for (int p = 0; p < NPR; p++) pf[(size_t)p * d.cells + id] = pr[p];
+    if (stats) {
+      atomicAdd(stats + 0, (double)it);
+      if (fails != 0.0) atomicAdd(stats + 3, fails);
+      if (floors != 0.0) atomicAdd(stats + 4, floors);
+    }
   }
 }
 

@@ -20,6 +20,9 @@ struct harm_ctx {
   double* d_emf;
   float* d_emff;
   double* d_pk;     // midpoint primitives of the RK2 step
+  double* d_U;      // conserved variables to invert (UEVOLVE)
+  unsigned int* d_rare;   // cells finished by the rare inversion path
+  unsigned int* d_nrare;  // their count
   int8_t* d_pflag;  // inversion flags
   void* d_fixrec;   // fixup records
   unsigned int fix_cap;

@@ -260,7 +260,7 @@ static __device__ int inv_finish(double Wp, const InvC& c, const double* Qtcon, 
 
 // Hot or cold Jon inversion on geometry-free U (Utoprim_jon_nonrelcompat_inputnorestmass).
 // `wpguess` >= 0 replaces the previous-state W' when use_guess is set.
-static __device__ void utoprim_jon(bool cold, const double* Ugf, const Geo<double>& g, int8_t& flag, double* prim, double gam,
+static __device__ __forceinline__ void utoprim_jon(bool cold, const double* Ugf, const Geo<double>& g, int8_t& flag, double* prim, double gam,
                             double gammafail, int& nstroke, bool use_guess, double wpguess) {
   int lntries = 0;
   double U[NPR], pt[NPR];
@@ -296,7 +296,7 @@ static __device__ void utoprim_jon(bool cold, const double* Ugf, const Geo<doubl
 }
 
 // Utoprimgen from UEVOLVE U (igdet scales to geometry-free).  Returns the Newton iterations.
-static __device__ int utoprimgen(const double* U, const Geo<double>& g, double igdet, double* pr, int8_t& flag, double gam,
+static __device__ __forceinline__ int utoprimgen(const double* U, const Geo<double>& g, double igdet, double* pr, int8_t& flag, double gam,
                           double gammafail, bool use_guess, double wpguess, bool* guess_failed) {
   double Ugf[NPR], pr0[NPR];
 #pragma unroll

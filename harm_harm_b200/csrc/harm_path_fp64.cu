@@ -250,10 +250,14 @@ int hp_update_fp64(harm_ctx* c, const StepCoef& sc, const double* pi, const doub
   Dims d = dims_of(c->g);
   Phys ph = phys_of(c->g);
   long long ncell = (long long)d.n1 * d.n2 * d.n3;
-  k_update<double><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, sc, c->d_dt, pi, pb, pf, pflag, c->d_F[0], c->d_F[1],
-                                                       c->d_F[2], c->d_emf, c->d_geom, c->d_conn, c->d_aux, c->d_mlp,
-                                                       stats);
-  c->launches++;
+  k_conserved<double><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, sc, c->d_dt, pi, pb, c->d_F[0], c->d_F[1],
+                                                          c->d_F[2], c->d_emf, c->d_geom, c->d_conn, c->d_U);
+  CK(cudaMemsetAsync(c->d_nrare, 0, sizeof(unsigned int), c->stream));
+  k_invert<0><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare, c->d_nrare,
+                                                  stats);
+  k_invert_rare<0><<<2 * 148, 128, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
+                                                     c->d_nrare, stats);
+  c->launches += 3;
   CK(cudaGetLastError());
   return 0;
 }
