@@ -18,6 +18,7 @@ HARM_NAUX = 3
 HARM_G_GCOV, HARM_G_GCON, HARM_G_GCOVPERT_TT, HARM_G_ALPHA = 0, 10, 20, 21
 HARM_G_BETASQOALPHASQ, HARM_G_BETA, HARM_G_GDET, HARM_G_IGDET = 22, 23, 26, 27
 HARM_AUX_R, HARM_AUX_RHOFLOOR, HARM_AUX_UFLOOR = 0, 1, 2
+HARM_NOALLOC_MAX_CELLS = 2097152
 
 
 class harm_grid(C.Structure):
@@ -61,6 +62,7 @@ _DEVICE_SIGS = {
     "harm_b200_step_host": (Ip, [P, Ip, Ip, P, C.POINTER(D), C.POINTER(harm_stats)]),
     "harm_b200_utoprimgen_points": (Ip, [P, C.c_size_t, Ip, P, P, P, P, P]),
     "harm_b200_time_stages": (Ip, [P, Ip, Ip, P, D, Ip, C.POINTER(D)]),
+    "harm_b200_fluxcalc_noalloc": (Ip, [C.POINTER(harm_grid), P, P, P, P, P, C.POINTER(D), P]),
     "harm_b200_last_error": (C.c_char_p, []),
 }
 

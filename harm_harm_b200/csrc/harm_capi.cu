@@ -27,6 +27,8 @@ static int seterr_msg(const char* msg, int code) {
   return code;
 }
 
+int hb_setmsg(const char* msg, int code) { return seterr_msg(msg, code); }
+
 extern "C" const char* harm_b200_last_error(void) { return g_errbuf; }
 
 extern "C" int harm_b200_create(const harm_grid* g, const double* geom_h, const double* conn_h, const double* aux_h,

@@ -216,6 +216,23 @@ int harm_b200_utoprimgen_points(harm_ctx *ctx, size_t n, int guess, const double
 int harm_b200_time_stages(harm_ctx *ctx, int precision, int guess, const double *d_P,
                           double dt, int reps, double ms[5]);
 
+/* Largest grid (extended cells n1e*n2e*n3e) harm_b200_fluxcalc_noalloc accepts: its EMF
+   scratch is 3 doubles per cell, 48 MiB at this size. */
+#define HARM_NOALLOC_MAX_CELLS 2097152
+
+/* No counterpart in the reference.  fluxcalc for callers that cannot allocate device
+   memory (a caller working inside a memory pool it does not own, or a host that forbids
+   allocation once its time loop runs): same FP64 fluxes and ndt[3] as harm_b200_fluxcalc,
+   from caller-provided d_geom (the device copy of the geom table), d_pb and d_F1..d_F3, on
+   `stream` (cudaStream_t, NULL for the default stream).  It allocates nothing: the EMF and
+   CFL scratch is a file-scope device array that every GPU loading the library holds until
+   exit.  Grids above HARM_NOALLOC_MAX_CELLS are rejected (return 2).  All calls share the
+   scratch, so calls that overlap on the GPU race; the first call on a device looks up the
+   scratch address and should come before any stream capture on that device. */
+int harm_b200_fluxcalc_noalloc(const harm_grid *g, const double *d_geom, const double *d_pb,
+                               double *d_F1, double *d_F2, double *d_F3, double ndt[3],
+                               void *stream);
+
 /* Last CUDA error text of this thread's most recent failing call. */
 const char *harm_b200_last_error(void);
 
