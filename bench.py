@@ -28,13 +28,15 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 CONFIGS = {
-    # name: (n1, n2, n3, lim)
-    "torus3d_384x192x128": (384, 192, 128, 0),
-    "torus3d_256x128x64": (256, 128, 64, 0),
-    "torus3d_192x96x64": (192, 96, 64, 0),
+    # name: (n1, n2, n3, lim) -- the reconstruction of each torus configuration: WENO5 in 3-D,
+    # MC for the 2-D CPU-runnable case
+    "torus3d_384x192x128": (384, 192, 128, 2),
+    "torus3d_256x128x64": (256, 128, 64, 2),
+    "torus3d_192x96x64": (192, 96, 64, 2),
     "torus2d_128x128": (128, 128, 1, 0),
 }
 LIMNAME = {0: "mc", 1: "ppm", 2: "weno5"}
+LIMS = {"mc": 0, "ppm": 1, "weno5": 2}
 METRIC = "zone-updates/s on 3D torus: learned+mixed vs plain FP64 GPU at L1 err≤1e-6"
 
 
@@ -145,6 +147,7 @@ def run_reference(args, ws, rank):
     from harm_harm_b200 import Grid
     from oracle import oracle as O
     n1, n2, n3, lim = CONFIGS[args.config]
+    lim = LIMS.get(args.lim, lim)
     sn3 = min(n3, args.cpu_sample_n3)
     g = Grid.torus(n1, n2, sn3, lim=lim)
     geom, conn, aux = g.geometry()
@@ -181,7 +184,7 @@ def cpu_baseline_sample(args, lim) -> dict:
     from harm_harm_b200 import Grid
     from oracle import oracle as O
     n1, n2, n3, _ = CONFIGS[args.config]
-    sn3 = min(n3, 4)
+    sn3 = min(n3, args.cpu_sample_n3)
     g = Grid.torus(n1, n2, sn3, lim=lim)
     geom, conn, aux = g.geometry()
     P = g.torus_init(geom, aux, seed=args.seed)
@@ -208,6 +211,7 @@ def run_ours(args, ws, rank, local):
     from harm_harm_b200 import HARM_PREC_FP64, HARM_PREC_MIXED, Grid, Harm
     torch.cuda.set_device(local)
     n1, n2, n3, lim = CONFIGS[args.config]
+    lim = LIMS.get(args.lim, lim)
     g = Grid.torus(n1, n2, n3, lim=lim)
     geom, conn, aux = g.geometry()
     P0 = g.torus_init(geom, aux, seed=args.seed + rank)
@@ -332,11 +336,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="torus3d_384x192x128", choices=list(CONFIGS))
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--lim", default="config", choices=["config", "mc", "ppm", "weno5"])
     ap.add_argument("--guess", default="prev", choices=["prev", "mlp"])
     ap.add_argument("--seed", type=int, default=12345)
     ap.add_argument("--err-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--cpu-sample-n3", type=int, default=4)
+    ap.add_argument("--cpu-sample-n3", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

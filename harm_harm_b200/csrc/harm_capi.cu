@@ -34,7 +34,9 @@ extern "C" const char* harm_b200_last_error(void) { return g_errbuf; }
 extern "C" int harm_b200_create(const harm_grid* g, const double* geom_h, const double* conn_h, const double* aux_h,
                                 int device, harm_ctx** out) {
   if (!g || !geom_h || !conn_h || !aux_h || !out) return seterr_msg("null argument", 1);
-  if (g->lim != HARM_LIM_MC) return seterr_msg("this reconstruction is not available in the device library", 2);
+  if (g->lim != HARM_LIM_MC && g->lim != HARM_LIM_PARA && g->lim != HARM_LIM_WENO5)
+    return seterr_msg("unknown reconstruction", 2);
+  if (g->lim == HARM_LIM_WENO5 && g->ng < 6) return seterr_msg("WENO5 needs ng >= 6", 2);
   harm_ctx* c = new harm_ctx();
   memset((void*)c, 0, sizeof(*c));
   c->g = *g;

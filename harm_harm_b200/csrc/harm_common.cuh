@@ -127,7 +127,46 @@ __device__ __forceinline__ void recon_face_mc(const double* __restrict__ P, size
   }
 }
 
-template <int DIR, typename T, typename GT>
+// PPM: cells i-3..i+2 around the face below cell i (para4 of cells i-1 and i)
+template <typename T>
+__device__ __forceinline__ void recon_face_para(const double* __restrict__ P, size_t cells, size_t c0, long long stride,
+                                                T* pl, T* pr) {
+#pragma unroll 1
+  for (int p = 0; p < NPR; p++) {
+    const double* base = P + (size_t)p * cells + c0;
+    T y[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) y[q] = (T)__ldg(base + (long long)(q - 3) * stride);
+    T la, ra, lb, rb;
+    para4_cell<T>(y + 2, la, ra);
+    para4_cell<T>(y + 3, lb, rb);
+    pl[p] = ra;
+    pr[p] = lb;
+  }
+}
+
+// WENO5: cells i-5..i+4; unoptimised weights of cells i-3..i+2, edges of cells i-1 and i
+template <typename T>
+__device__ __forceinline__ void recon_face_weno5(const double* __restrict__ P, size_t cells, size_t c0,
+                                                 long long stride, T* pl, T* pr) {
+#pragma unroll 1
+  for (int p = 0; p < NPR; p++) {
+    const double* base = P + (size_t)p * cells + c0;
+    T y[10];
+#pragma unroll
+    for (int q = 0; q < 10; q++) y[q] = (T)__ldg(base + (long long)(q - 5) * stride);
+    T w[6][3];
+#pragma unroll
+    for (int q = 0; q < 6; q++) weno5_unopt<T>(y + 2 + q, w[q]);
+    T la, ra, lb, rb;
+    weno5_edges<T>(y + 4, w[2], w[0], w[4], la, ra);
+    weno5_edges<T>(y + 5, w[3], w[1], w[5], lb, rb);
+    pl[p] = ra;
+    pr[p] = lb;
+  }
+}
+
+template <int DIR, typename T, typename GT, int LIM = HARM_LIM_MC>
 __global__ void __launch_bounds__(256) k_flux(Dims d, Phys ph, FaceBox fb, const double* __restrict__ P,
                                               const GT* __restrict__ geom, T* __restrict__ F,
                                               unsigned long long* __restrict__ dtslot) {
@@ -142,7 +181,9 @@ __global__ void __launch_bounds__(256) k_flux(Dims d, Phys ph, FaceBox fb, const
     size_t id = cidx(d, ii, jj, kk);
     long long stride = (DIR == 1) ? 1 : (DIR == 2) ? (long long)d.n1e : (long long)d.plane;
     T pl[NPR], pr[NPR];
-    recon_face_mc<T>(P, d.cells, id, stride, pl, pr);
+    if (LIM == HARM_LIM_WENO5) recon_face_weno5<T>(P, d.cells, id, stride, pl, pr);
+    else if (LIM == HARM_LIM_PARA) recon_face_para<T>(P, d.cells, id, stride, pl, pr);
+    else recon_face_mc<T>(P, d.cells, id, stride, pl, pr);
     constexpr int loc = (DIR == 1) ? HARM_LOC_FACE1 : (DIR == 2) ? HARM_LOC_FACE2 : HARM_LOC_CENT;
     Geo<T> g;
     load_geo<T, GT>(geom + (size_t)loc * HARM_NGF * d.plane, d.plane, (size_t)jj * d.n1e + ii, g);

@@ -218,4 +218,223 @@ __device__ __forceinline__ T mc_slope(T yl, T yc, T yr) {
   return (Dqc * m1 <= T(0)) ? T(0) : ((fabs(Dqc) < fabs(m1)) ? Dqc : m1);
 }
 
+
+// ---------------------------------------------------------------- PPM (para4)
+// interppoint.para.c:568-760 with PARA2LIM=MC and the defaults of para_and_paraenohybrid.h;
+// checkparamonotonicity :1069.  y points at the cell, uses y[-2..2].
+template <typename T>
+__device__ __forceinline__ T minmod2(T a, T b) {
+  return (a * b <= T(0)) ? T(0) : ((fabs(a) < fabs(b)) ? a : b);
+}
+
+template <typename T>
+__device__ __forceinline__ void para4_cell(const T* y, T& lout, T& rout) {
+  T dq[3];
+#pragma unroll
+  for (int mm = -1; mm <= 1; mm++) {
+    T dq1m = y[mm] - y[mm - 1], dq1p = y[mm + 1] - y[mm];
+    T Dqc = T(0.5) * (y[mm + 1] - y[mm - 1]);
+    dq[mm + 1] = minmod2(Dqc, minmod2(T(2) * dq1m, T(2) * dq1p));
+  }
+  T ddql = dq[1] - dq[0], ddqr = dq[2] - dq[1];
+  T l = T(0.5) * (y[0] + y[-1]) - ddql * T(1.0 / 8.0);
+  T r = T(0.5) * (y[1] + y[0]) - ddqr * T(1.0 / 8.0);
+  const T a6 = T(4);
+  T qa = (r - y[0]) * (y[0] - l), qd = (r - l), qe = a6 * (y[0] - T(0.5) * (l + r));
+  if (qa <= T(0)) {
+    l = y[0];
+    r = y[0];
+  } else {
+    if (qd * (qd - qe) < T(0)) l = (-(T(2) + a6) * r + T(2) * a6 * y[0]) / (a6 - T(2));
+    else if (qd * (qd + qe) < T(0)) r = (-(T(2) + a6) * l + T(2) * a6 * y[0]) / (a6 - T(2));
+  }
+  lout = l;
+  rout = r;
+}
+
+// ---------------------------------------------------------------- WENO5 (WENO5BND core)
+// eno_line_reconstruct reconstructeno.c:333 for CVT_C2E: smoothness indicators
+// (compute_cf_stencil_weights :1693), desensitising and normalisation (:2001, :2292),
+// 1/(beta+eps)^2 weights (:2211), limit_weight (:3015), optimal face weights (:1905),
+// WENO3 lower-order weights, weight-ratio stencil reduction (compute_weights_ratios :2316,
+// choose_weno_order :2442), edge values (eno_cvt :884).  Sums use the symmetric pairwise
+// order of get_sum_of_elements.  The SMONO indicator is taken as 0 (pure WENO output).
+template <typename T>
+struct WenoEps;
+template <>
+struct WenoEps<double> {
+  static constexpr double eps = (500.0 * 2.220446049250313e-16) * (500.0 * 2.220446049250313e-16);
+  static constexpr double tiny = 2.2250738585072014e-308;  // DBL_MIN
+};
+template <>
+struct WenoEps<float> {
+  static constexpr float eps = (500.0f * 1.1920929e-07f) * (500.0f * 1.1920929e-07f);
+  static constexpr float tiny = 1.17549435e-38f;  // FLT_MIN
+};
+
+template <typename T>
+__device__ __forceinline__ T symsum3(T a0, T a1, T a2) {
+  T s = T(0);
+  s += a0 + a2;
+  s += a1 * T(1);
+  return s;
+}
+template <typename T>
+__device__ __forceinline__ T symsum2(T a0, T a1) {
+  T s = T(0);
+  s += a0 + a1;
+  s += a1 * T(0);  // the loop's next element, multiplied by (count odd) = 0
+  return s;
+}
+
+template <typename T>
+__device__ __forceinline__ T limit_weight(int order, T w) {
+  const T avg = T(1) / T(order), w1 = T(0.2) * avg, w2 = (T(1) - T(0.2)) * avg, w3 = (T(1) + T(0.2)) * avg, w4 = T(1);
+  if (w < w1) return T(0);
+  if (w < w2) return avg * (w - w1) / (w2 - w1);
+  if (w < w3) return avg;
+  return (w - w3) * (w4 - avg) / (w4 - w3) + avg;
+}
+
+// unoptimised (limited, normalised) weights of the three 3-point stencils of the cell at u
+template <typename T>
+__device__ __forceinline__ void weno5_unopt(const T* u, T* w) {
+  T fd0 = -(T(3) * u[0] + u[2]) + T(4) * u[1];
+  T fd1 = u[1] - u[-1];
+  T fd2 = (T(3) * u[0] + u[-2]) - T(4) * u[-1];
+  T sd0 = (u[0] + u[2]) - T(2) * u[1];
+  T sd1 = (u[-1] + u[1]) - T(2) * u[0];
+  T sd2 = (u[0] + u[-2]) - T(2) * u[-1];
+  T b[3];
+  b[0] = T(13. / 12.) * sd0 * sd0 + T(1. / 4.) * fd0 * fd0;
+  b[1] = T(13. / 12.) * sd1 * sd1 + T(1. / 4.) * fd1 * fd1;
+  b[2] = T(13. / 12.) * sd2 * sd2 + T(1. / 4.) * fd2 * fd2;
+  // desensitise: sum of u^2 over the 5 cells in the symmetric order
+  T normu = T(0);
+  normu += u[-2] * u[-2] + u[2] * u[2];
+  normu += u[-1] * u[-1] + u[1] * u[1];
+  normu += u[0] * u[0] * T(1);
+  const T ee = normu * WenoEps<T>::eps;
+#pragma unroll
+  for (int s = 0; s < 3; s++) b[s] += ee;
+  T sb = symsum3(b[0], b[1], b[2]);
+#pragma unroll
+  for (int s = 0; s < 3; s++) b[s] /= (sb + WenoEps<T>::tiny);
+#pragma unroll
+  for (int s = 0; s < 3; s++) {
+    T t = b[s] + WenoEps<T>::eps;
+    t *= t;
+    w[s] = T(1) / t;
+  }
+  T sw = symsum3(w[0], w[1], w[2]);
+#pragma unroll
+  for (int s = 0; s < 3; s++) w[s] /= (sw + T(0));
+#pragma unroll
+  for (int s = 0; s < 3; s++) w[s] = limit_weight<T>(3, w[s]);
+  sw = symsum3(w[0], w[1], w[2]);
+#pragma unroll
+  for (int s = 0; s < 3; s++) w[s] /= (sw + T(0));
+}
+
+// the same for the two 2-point stencils (WENO3)
+template <typename T>
+__device__ __forceinline__ void weno3_unopt(const T* u, T* w) {
+  T fd0 = u[1] - u[0], fd1 = u[0] - u[-1];
+  T b[2] = {fd0 * fd0, fd1 * fd1};
+  T normu = T(0);
+  normu += u[-1] * u[-1] + u[1] * u[1];
+  normu += u[0] * u[0] * T(1);
+  const T ee = normu * WenoEps<T>::eps;
+  b[0] += ee;
+  b[1] += ee;
+  T sb = symsum2(b[0], b[1]);
+  b[0] /= (sb + WenoEps<T>::tiny);
+  b[1] /= (sb + WenoEps<T>::tiny);
+#pragma unroll
+  for (int s = 0; s < 2; s++) {
+    T t = b[s] + WenoEps<T>::eps;
+    t *= t;
+    w[s] = T(1) / t;
+  }
+  T sw = symsum2(w[0], w[1]);
+  w[0] /= (sw + T(0));
+  w[1] /= (sw + T(0));
+  w[0] = limit_weight<T>(2, w[0]);
+  w[1] = limit_weight<T>(2, w[1]);
+  sw = symsum2(w[0], w[1]);
+  w[0] /= (sw + T(0));
+  w[1] /= (sw + T(0));
+}
+
+// left and right edge values of the cell at u, given its neighbours' unoptimised weights
+// (wm at u-2, wp at u+2) for the stencil-reduction ratio
+template <typename T>
+__device__ __forceinline__ void weno5_edges(const T* u, const T* w, const T* wm, const T* wp, T& yl, T& yr) {
+  const T E = WenoEps<T>::eps;
+  T rl = (w[2] + E) / (wm[0] + E);
+  T rr = (w[0] + E) / (wp[2] + E);
+  T ratio = fmin(rl, rr);
+  T f = (ratio - T(1.3)) / (T(1.6) - T(1.3));
+  f = fmax(T(0), fmin(f, T(1)));
+  // optimal face weights (order 3)
+  T wl[3] = {w[0] * T(1. / 16.), w[1] * T(5. / 8.), w[2] * T(5. / 16.)};
+  T wr[3] = {w[0] * T(5. / 16.), w[1] * T(5. / 8.), w[2] * T(1. / 16.)};
+  T sl = symsum3(wl[0], wl[1], wl[2]), sr = symsum3(wr[0], wr[1], wr[2]);
+#pragma unroll
+  for (int s = 0; s < 3; s++) {
+    wl[s] /= (sl + WenoEps<T>::tiny);
+    wr[s] /= (sr + WenoEps<T>::tiny);
+  }
+  const bool two = (T(0) < f);
+  if (two) {
+#pragma unroll
+    for (int s = 0; s < 3; s++) {
+      wl[s] *= (T(1) - f);
+      wr[s] *= (T(1) - f);
+    }
+  }
+  // stencil polynomials (c2l/c2r_array3)
+  T recl0 = symsum3(T(15. / 8.) * u[0], T(-5. / 4.) * u[1], T(3. / 8.) * u[2]);
+  T recl1 = symsum3(T(3. / 8.) * u[-1], T(3. / 4.) * u[0], T(-1. / 8.) * u[1]);
+  T recl2 = symsum3(T(-1. / 8.) * u[-2], T(3. / 4.) * u[-1], T(3. / 8.) * u[0]);
+  T recr0 = symsum3(T(3. / 8.) * u[0], T(3. / 4.) * u[1], T(-1. / 8.) * u[2]);
+  T recr1 = symsum3(T(-1. / 8.) * u[-1], T(3. / 4.) * u[0], T(3. / 8.) * u[1]);
+  T recr2 = symsum3(T(3. / 8.) * u[-2], T(-5. / 4.) * u[-1], T(15. / 8.) * u[0]);
+  T ul0 = (wl[0] != T(0)) ? wl[0] * recl0 : T(0);
+  T ul1 = (wl[1] != T(0)) ? wl[1] * recl1 : T(0);
+  T ul2 = (wl[2] != T(0)) ? wl[2] * recl2 : T(0);
+  T ur0 = (wr[0] != T(0)) ? wr[0] * recr0 : T(0);
+  T ur1 = (wr[1] != T(0)) ? wr[1] * recr1 : T(0);
+  T ur2 = (wr[2] != T(0)) ? wr[2] * recr2 : T(0);
+  T outl = T(0), outr = T(0);
+  outl += symsum3(ul0, ul1, ul2);
+  outr += symsum3(ur0, ur1, ur2);
+  if (two) {
+    T w3[2];
+    weno3_unopt<T>(u, w3);
+    T l3[2] = {w3[0] * T(1. / 4.), w3[1] * T(3. / 4.)};
+    T r3[2] = {w3[0] * T(3. / 4.), w3[1] * T(1. / 4.)};
+    T sl3 = symsum2(l3[0], l3[1]), sr3 = symsum2(r3[0], r3[1]);
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      l3[s] /= (sl3 + WenoEps<T>::tiny);
+      r3[s] /= (sr3 + WenoEps<T>::tiny);
+      l3[s] *= f;
+      r3[s] *= f;
+    }
+    T rl0 = symsum2(T(3. / 2.) * u[0], T(-1. / 2.) * u[1]);
+    T rl1 = symsum2(T(1. / 2.) * u[-1], T(1. / 2.) * u[0]);
+    T rr0 = symsum2(T(1. / 2.) * u[0], T(1. / 2.) * u[1]);
+    T rr1 = symsum2(T(-1. / 2.) * u[-1], T(3. / 2.) * u[0]);
+    T a0 = (l3[0] != T(0)) ? l3[0] * rl0 : T(0);
+    T a1 = (l3[1] != T(0)) ? l3[1] * rl1 : T(0);
+    T b0 = (r3[0] != T(0)) ? r3[0] * rr0 : T(0);
+    T b1 = (r3[1] != T(0)) ? r3[1] * rr1 : T(0);
+    outl += symsum2(a0, a1);
+    outr += symsum2(b0, b1);
+  }
+  yl = (T(1) - T(0)) * outl + T(0) * u[0];
+  yr = (T(1) - T(0)) * outr + T(0) * u[0];
+}
+
 }  // namespace hb

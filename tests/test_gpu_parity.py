@@ -13,12 +13,14 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-CASES = {"2d": (64, 64, 1), "3d": (32, 24, 8)}
+CASES = {"2d_mc": (64, 64, 1, 0), "3d_mc": (32, 24, 8, 0), "3d_ppm": (32, 24, 8, 1),
+         "3d_weno5": (32, 24, 8, 2), "2d_weno5": (48, 48, 1, 2)}
 
 
 @pytest.fixture(scope="module", params=list(CASES))
 def setup(request, cuda):
-    g, geom, conn, aux, P = make_torus(*CASES[request.param])
+    n1, n2, n3, lim = CASES[request.param]
+    g, geom, conn, aux, P = make_torus(n1, n2, n3, lim=lim)
     orc = O.Oracle(g, geom, conn, aux)
     orc.bound_prim(P)
     dev = Harm(g, geom, conn, aux)

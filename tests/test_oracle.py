@@ -112,3 +112,36 @@ def test_oracle_3d_runs():
         dt, st = orc.step_ch(P, dt)
     assert np.isfinite(P).all()
     assert divb_corner(g, geom, P).max() / scale < 1e-12
+
+
+@pytest.mark.parametrize("lim,order", [(2, 4.5), (1, 1.8)])
+def test_high_order_reconstruction_convergence_and_no_overshoot(lim, order):
+    errs = []
+    for n in (32, 64, 128):
+        x = (np.arange(n) + 0.5) / n
+        y = np.sin(2 * np.pi * x) + 2.0
+        yl, yr = O.reconstruct_line(lim, y)
+        exact_l = np.sin(2 * np.pi * np.arange(n) / n) + 2.0
+        exact_r = np.sin(2 * np.pi * (np.arange(n) + 1) / n) + 2.0
+        errs.append(max(np.abs(yl[6:-6] - exact_l[6:-6]).max(), np.abs(yr[6:-6] - exact_r[6:-6]).max()))
+    rates = [np.log2(errs[i] / errs[i + 1]) for i in range(2)]
+    assert min(rates) > order, rates
+    y = np.where(np.arange(40) < 20, 1.0, 0.1)
+    yl, yr = O.reconstruct_line(lim, y)
+    assert yl[5:-5].min() >= 0.1 - 1e-12 and yl[5:-5].max() <= 1.0 + 1e-12
+    assert yr[5:-5].min() >= 0.1 - 1e-12 and yr[5:-5].max() <= 1.0 + 1e-12
+
+
+@pytest.mark.parametrize("lim", [1, 2])
+def test_oracle_torus_with_ppm_and_weno5(lim):
+    g, geom, conn, aux, P = make_torus(48, 48, 1, lim=lim)
+    orc = O.Oracle(g, geom, conn, aux)
+    orc.bound_prim(P)
+    F = [np.zeros_like(P) for _ in range(3)]
+    ndt = orc.fluxcalc(P, *F)
+    dt = 1.0 / (1 / ndt[0] + 1 / ndt[1])
+    scale = np.abs(P[5:8] * geom[0, 26][None, None]).max() / min(g.g.dx[1], g.g.dx[2])
+    for _ in range(4):
+        dt, st = orc.step_ch(P, dt)
+    assert np.isfinite(P).all()
+    assert divb_corner(g, geom, P).max() / scale < 1e-13
