@@ -222,6 +222,251 @@ __global__ void __launch_bounds__(256) k_flux(Dims d, Phys ph, FaceBox fb, const
   block_min_atomic(dtij, dtslot);
 }
 
+// ------------------------------------------------------------------ tiled flux kernel
+//
+// One block of 256 threads = a tile of A = 32 faces of direction DIR times NT = 8 transverse
+// lines, consecutive threads along i so that every global load is coalesced.  VB primitives
+// at a time (all 8 in FP32, 4 in FP64) are staged in shared memory with the stencil halo along
+// DIR; the block then computes every cell's reconstruction once (MC slope, para4, or the WENO5
+// weights and then the edge values), three barriers per group instead of three per primitive.
+// Each thread keeps the two states of its own face and evaluates states, fluxes, wave speeds
+// and the HLL flux of that face.
+template <int LIM>
+struct ReconGeom;
+template <>
+struct ReconGeom<HARM_LIM_MC> {
+  static constexpr int H = 2, X = 1;  // staged cells below / above the tile's faces
+};
+template <>
+struct ReconGeom<HARM_LIM_PARA> {
+  static constexpr int H = 3, X = 2;
+};
+template <>
+struct ReconGeom<HARM_LIM_WENO5> {
+  static constexpr int H = 5, X = 4;
+};
+
+template <int LIM, typename T>
+struct FluxTile {
+  static constexpr int A = 32;                                 // faces along DIR
+  static constexpr int NT = 8;                                 // transverse lines
+  static constexpr int H = ReconGeom<LIM>::H;
+  static constexpr int NL = A + H + ReconGeom<LIM>::X;         // staged cells along DIR
+  static constexpr int VB = (sizeof(T) == 4) ? 8 : 4;          // primitives per stage
+  static constexpr int NW = (LIM == HARM_LIM_WENO5) ? 3 : 0;   // weights per cell
+  static constexpr int PLANE = NL * NT;
+  static constexpr size_t smem = (size_t)VB * PLANE * (3 + NW) * sizeof(T);
+};
+
+template <int DIR, int LIM, typename T, typename GT>
+__global__ void __launch_bounds__(256) k_fluxt(Dims d, Phys ph, FaceBox fb, const double* __restrict__ P,
+                                               const GT* __restrict__ geom, T* __restrict__ F,
+                                               unsigned long long* __restrict__ dtslot) {
+  using TL = FluxTile<LIM, T>;
+  constexpr int A = TL::A, NT = TL::NT, H = TL::H, NL = TL::NL, VB = TL::VB, PL = TL::PLANE;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s_y = reinterpret_cast<T*>(smem_raw);   // [VB][plane]
+  T* s_el = s_y + VB * PL;                    // left edge of each cell
+  T* s_er = s_el + VB * PL;                   // right edge of each cell
+  T* s_w = s_er + VB * PL;                    // WENO5 unoptimised weights, [VB][plane][3]
+  // a plane is [NT][NL] for DIR 1 and [NL][NT] otherwise: the index along i is contiguous
+  auto sx = [](int c, int t) -> int { return (DIR == 1) ? t * NL + c : c * NT + t; };
+  // item idx over VB x nc cells (from c0) x NT lines, fastest along i
+  auto split = [](int idx, int c0, int nc, int& v, int& c, int& t) {
+    if (DIR == 1) {
+      c = c0 + idx % nc;
+      int r = idx / nc;
+      t = r % NT;
+      v = r / NT;
+    } else {
+      t = idx % NT;
+      int r = idx / NT;
+      c = c0 + r % nc;
+      v = r / nc;
+    }
+  };
+  const int tid = threadIdx.x;
+  // tile origin in active-relative face coordinates, and this thread's face
+  int l0, t0, o, lme, tme;
+  if (DIR == 1) {
+    l0 = blockIdx.x * A + fb.lo[0]; t0 = blockIdx.y * NT + fb.lo[1]; o = blockIdx.z + fb.lo[2];
+    lme = tid % A; tme = tid / A;
+  } else if (DIR == 2) {
+    t0 = blockIdx.x * NT + fb.lo[0]; l0 = blockIdx.y * A + fb.lo[1]; o = blockIdx.z + fb.lo[2];
+    lme = tid / NT; tme = tid % NT;
+  } else {
+    t0 = blockIdx.x * NT + fb.lo[0]; l0 = blockIdx.y * A + fb.lo[2]; o = blockIdx.z + fb.lo[1];
+    lme = tid / NT; tme = tid % NT;
+  }
+  const int lhi = fb.hi[DIR - 1];
+  const int thi = (DIR == 1) ? fb.hi[1] : fb.hi[0];
+  const bool valid = (l0 + lme <= lhi) && (t0 + tme <= thi);
+  // extended-grid extents along DIR and along the transverse tile axis
+  const int ngL = (DIR == 3) ? d.ng3 : d.ng;
+  const int nLe = (DIR == 1) ? d.n1e : (DIR == 2) ? d.n2e : d.n3e;
+  const int nTe = (DIR == 1) ? d.n2e : d.n1e;
+  auto cell_index = [&](int lext, int text) -> size_t {
+    if (DIR == 1) return cidx(d, lext, text, o + d.ng3);
+    if (DIR == 2) return cidx(d, text, lext, o + d.ng3);
+    return cidx(d, text, o + d.ng, lext);
+  };
+  T pl[NPR], pr[NPR];
+#pragma unroll
+  for (int p0 = 0; p0 < NPR; p0 += VB) {
+    if (p0 > 0) __syncthreads();
+    // stage VB primitives (the tile's cells and the halo along DIR; cells past the grid's
+    // edge are clamped: they only feed faces outside the face box)
+#pragma unroll 4
+    for (int idx = tid; idx < VB * PL; idx += 256) {
+      int v, cl, ct;
+      split(idx, 0, NL, v, cl, ct);
+      int lext = min(max(l0 - H + cl + ngL, 0), nLe - 1);
+      int text = min(max(t0 + ct + d.ng, 0), nTe - 1);
+      s_y[v * PL + sx(cl, ct)] = (T)__ldg(P + (size_t)(p0 + v) * d.cells + cell_index(lext, text));
+    }
+    __syncthreads();
+    if (LIM == HARM_LIM_WENO5) {
+      // unoptimised weights of cells 2 .. NL-3
+      for (int idx = tid; idx < VB * (NL - 4) * NT; idx += 256) {
+        int v, c, t;
+        split(idx, 2, NL - 4, v, c, t);
+        const T* y = s_y + v * PL;
+        T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
+        T w[3];
+        weno5_unopt<T>(u5 + 2, w);
+        T* ws = s_w + (v * PL + sx(c, t)) * 3;
+        ws[0] = w[0]; ws[1] = w[1]; ws[2] = w[2];
+      }
+      __syncthreads();
+      // edges of cells H-1 .. H+A-1
+      for (int idx = tid; idx < VB * (A + 1) * NT; idx += 256) {
+        int v, c, t;
+        split(idx, H - 1, A + 1, v, c, t);
+        const T* y = s_y + v * PL;
+        T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
+        const T* ws = s_w + v * PL * 3;
+        T w[3], wm[3], wp[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          w[k] = ws[sx(c, t) * 3 + k];
+          wm[k] = ws[sx(c - 2, t) * 3 + k];
+          wp[k] = ws[sx(c + 2, t) * 3 + k];
+        }
+        T yl, yr;
+        weno5_edges<T>(u5 + 2, w, wm, wp, yl, yr);
+        s_el[v * PL + sx(c, t)] = yl;
+        s_er[v * PL + sx(c, t)] = yr;
+      }
+    } else if (LIM == HARM_LIM_PARA) {
+      for (int idx = tid; idx < VB * (A + 1) * NT; idx += 256) {
+        int v, c, t;
+        split(idx, H - 1, A + 1, v, c, t);
+        const T* y = s_y + v * PL;
+        T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
+        T yl, yr;
+        para4_cell<T>(u5 + 2, yl, yr);
+        s_el[v * PL + sx(c, t)] = yl;
+        s_er[v * PL + sx(c, t)] = yr;
+      }
+    } else {
+      for (int idx = tid; idx < VB * (A + 1) * NT; idx += 256) {
+        int v, c, t;
+        split(idx, H - 1, A + 1, v, c, t);
+        const T* y = s_y + v * PL;
+        const T y0 = y[sx(c, t)];
+        T dq = mc_slope(y[sx(c - 1, t)], y0, y[sx(c + 1, t)]);
+        s_el[v * PL + sx(c, t)] = y0 - T(0.5) * dq;
+        s_er[v * PL + sx(c, t)] = y0 + T(0.5) * dq;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < VB; v++) {
+      pl[p0 + v] = s_er[v * PL + sx(H + lme - 1, tme)];
+      pr[p0 + v] = s_el[v * PL + sx(H + lme, tme)];
+    }
+  }
+  double dtij = 1.e300;
+  if (valid) {
+    const int lext = l0 + lme + ngL, text = t0 + tme + d.ng;
+    const size_t id = cell_index(lext, text);
+    int ii, jj;
+    if (DIR == 1) { ii = lext; jj = text; }
+    else if (DIR == 2) { ii = text; jj = lext; }
+    else { ii = text; jj = o + d.ng; }
+    constexpr int loc = (DIR == 1) ? HARM_LOC_FACE1 : (DIR == 2) ? HARM_LOC_FACE2 : HARM_LOC_CENT;
+    Geo<T> g;
+    load_geo<T, GT>(geom + (size_t)loc * HARM_NGF * d.plane, d.plane, (size_t)jj * d.n1e + ii, g);
+    const int bp = HARM_B1 + DIR - 1;
+    pl[bp] = pr[bp] = T(0.5) * (pl[bp] + pr[bp]);
+    const T gam = (T)ph.gam, gmax = (T)ph.gammamax;
+    limit_gamma<T>(gmax, pl, g);
+    limit_gamma<T>(gmax, pr, g);
+    State<T> ql, qr;
+    get_state<T>(pl, g, gam, ql);
+    get_state<T>(pr, g, gam, qr);
+    T Fl[NPR], Fr[NPR], Ul[NPR], Ur[NPR];
+    primtoflux<T>(pl, ql, DIR, g, g.gdet, Fl);
+    primtoflux<T>(pl, ql, 0, g, g.gdet, Ul);
+    primtoflux<T>(pr, qr, DIR, g, g.gdet, Fr);
+    primtoflux<T>(pr, qr, 0, g, g.gdet, Ur);
+    T cmaxl, cminl, cmaxr, cminr;
+    vchar<T>(pl, ql, DIR, g, gam, cmaxl, cminl);
+    vchar<T>(pr, qr, DIR, g, gam, cmaxr, cminr);
+    T lmin = fmin(cminl, cminr), lmax = fmax(cmaxl, cmaxr);
+    lmin = fabs(fmax(T(0), -lmin));
+    lmax = fabs(fmax(T(0), lmax));
+    const T cmin = lmin, cmax = lmax, ctop = fmax(lmax, lmin);
+    if (cmax + cmin != T(0)) {
+      const T inv = cmax + cmin;
+#pragma unroll
+      for (int p = 0; p < NPR; p++) F[(size_t)p * d.cells + id] = ((cmax * Fl[p] + cmin * Fr[p]) - (cmax * cmin) * (Ur[p] - Ul[p])) / inv;
+    } else {
+#pragma unroll
+      for (int p = 0; p < NPR; p++) F[(size_t)p * d.cells + id] = T(0.5) * ((Fl[p] + Fr[p]) - ctop * (Ur[p] - Ul[p]));
+    }
+    const double dxd = (DIR == 1) ? ph.dx1 : (DIR == 2) ? ph.dx2 : ph.dx3;
+    dtij = ph.cour * dxd / (double)ctop;
+    if (!(dtij > 0.0)) dtij = 1.e300;
+  }
+  // block minimum and one atomic per block
+  __shared__ double red[8];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) dtij = fmin(dtij, __shfl_xor_sync(0xffffffffu, dtij, off));
+  if ((tid & 31) == 0) red[tid >> 5] = dtij;
+  __syncthreads();
+  if (tid < 32) {
+    double v = (tid < 8) ? red[tid] : 1.e300;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, off));
+    if (tid == 0 && v < 1.e300) atomicMin(dtslot, dbl_bits(v));
+  }
+}
+
+template <int DIR, int LIM>
+static inline dim3 fluxt_grid(const FaceBox& fb) {
+  constexpr int A = 32, NT = 8;
+  if (DIR == 1) return dim3((fb.cnt[0] + A - 1) / A, (fb.cnt[1] + NT - 1) / NT, fb.cnt[2]);
+  if (DIR == 2) return dim3((fb.cnt[0] + NT - 1) / NT, (fb.cnt[1] + A - 1) / A, fb.cnt[2]);
+  return dim3((fb.cnt[0] + NT - 1) / NT, (fb.cnt[2] + A - 1) / A, fb.cnt[1]);
+}
+
+// launch k_fluxt<DIR, LIM, T, GT>; the first launch of each instantiation raises its dynamic
+// shared-memory limit (the FP32 WENO5 tile needs 63 KB)
+template <int DIR, int LIM, typename T, typename GT>
+static inline cudaError_t launch_fluxt(const Dims& d, const Phys& ph, const FaceBox& fb, const double* P,
+                                       const GT* geom, T* F, unsigned long long* dtslot, cudaStream_t st) {
+  constexpr size_t smem = FluxTile<LIM, T>::smem;
+  static bool attr_set = false;  // per instantiation; setting it twice is harmless
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(k_fluxt<DIR, LIM, T, GT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  k_fluxt<DIR, LIM, T, GT><<<fluxt_grid<DIR, LIM>(fb), 256, smem, st>>>(d, ph, fb, P, geom, F, dtslot);
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ EMF kernel
 
 template <typename T, typename GT>

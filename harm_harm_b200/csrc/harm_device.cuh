@@ -287,13 +287,25 @@ __device__ __forceinline__ T symsum2(T a0, T a1) {
   return s;
 }
 
+// Division inside the WENO weights.  FP64: IEEE division (the oracle's operations).  FP32
+// (mixed path): the fast reciprocal-multiply form, error of 2 ulp; the weights only steer the
+// stencil combination, so this stays far inside the FP32 reconstruction's own rounding.
+template <typename T>
+__device__ __forceinline__ T wdiv(T a, T b) {
+  return a / b;
+}
+template <>
+__device__ __forceinline__ float wdiv<float>(float a, float b) {
+  return __fdividef(a, b);
+}
+
 template <typename T>
 __device__ __forceinline__ T limit_weight(int order, T w) {
   const T avg = T(1) / T(order), w1 = T(0.2) * avg, w2 = (T(1) - T(0.2)) * avg, w3 = (T(1) + T(0.2)) * avg, w4 = T(1);
   if (w < w1) return T(0);
-  if (w < w2) return avg * (w - w1) / (w2 - w1);
+  if (w < w2) return wdiv<T>(avg * (w - w1), w2 - w1);
   if (w < w3) return avg;
-  return (w - w3) * (w4 - avg) / (w4 - w3) + avg;
+  return wdiv<T>((w - w3) * (w4 - avg), w4 - w3) + avg;
 }
 
 // unoptimised (limited, normalised) weights of the three 3-point stencils of the cell at u
@@ -319,21 +331,21 @@ __device__ __forceinline__ void weno5_unopt(const T* u, T* w) {
   for (int s = 0; s < 3; s++) b[s] += ee;
   T sb = symsum3(b[0], b[1], b[2]);
 #pragma unroll
-  for (int s = 0; s < 3; s++) b[s] /= (sb + WenoEps<T>::tiny);
+  for (int s = 0; s < 3; s++) b[s] = wdiv<T>(b[s], sb + WenoEps<T>::tiny);
 #pragma unroll
   for (int s = 0; s < 3; s++) {
     T t = b[s] + WenoEps<T>::eps;
     t *= t;
-    w[s] = T(1) / t;
+    w[s] = wdiv<T>(T(1), t);
   }
   T sw = symsum3(w[0], w[1], w[2]);
 #pragma unroll
-  for (int s = 0; s < 3; s++) w[s] /= (sw + T(0));
+  for (int s = 0; s < 3; s++) w[s] = wdiv<T>(w[s], sw + T(0));
 #pragma unroll
   for (int s = 0; s < 3; s++) w[s] = limit_weight<T>(3, w[s]);
   sw = symsum3(w[0], w[1], w[2]);
 #pragma unroll
-  for (int s = 0; s < 3; s++) w[s] /= (sw + T(0));
+  for (int s = 0; s < 3; s++) w[s] = wdiv<T>(w[s], sw + T(0));
 }
 
 // the same for the two 2-point stencils (WENO3)
@@ -348,22 +360,22 @@ __device__ __forceinline__ void weno3_unopt(const T* u, T* w) {
   b[0] += ee;
   b[1] += ee;
   T sb = symsum2(b[0], b[1]);
-  b[0] /= (sb + WenoEps<T>::tiny);
-  b[1] /= (sb + WenoEps<T>::tiny);
+  b[0] = wdiv<T>(b[0], sb + WenoEps<T>::tiny);
+  b[1] = wdiv<T>(b[1], sb + WenoEps<T>::tiny);
 #pragma unroll
   for (int s = 0; s < 2; s++) {
     T t = b[s] + WenoEps<T>::eps;
     t *= t;
-    w[s] = T(1) / t;
+    w[s] = wdiv<T>(T(1), t);
   }
   T sw = symsum2(w[0], w[1]);
-  w[0] /= (sw + T(0));
-  w[1] /= (sw + T(0));
+  w[0] = wdiv<T>(w[0], sw + T(0));
+  w[1] = wdiv<T>(w[1], sw + T(0));
   w[0] = limit_weight<T>(2, w[0]);
   w[1] = limit_weight<T>(2, w[1]);
   sw = symsum2(w[0], w[1]);
-  w[0] /= (sw + T(0));
-  w[1] /= (sw + T(0));
+  w[0] = wdiv<T>(w[0], sw + T(0));
+  w[1] = wdiv<T>(w[1], sw + T(0));
 }
 
 // left and right edge values of the cell at u, given its neighbours' unoptimised weights
@@ -371,10 +383,10 @@ __device__ __forceinline__ void weno3_unopt(const T* u, T* w) {
 template <typename T>
 __device__ __forceinline__ void weno5_edges(const T* u, const T* w, const T* wm, const T* wp, T& yl, T& yr) {
   const T E = WenoEps<T>::eps;
-  T rl = (w[2] + E) / (wm[0] + E);
-  T rr = (w[0] + E) / (wp[2] + E);
+  T rl = wdiv<T>(w[2] + E, wm[0] + E);
+  T rr = wdiv<T>(w[0] + E, wp[2] + E);
   T ratio = fmin(rl, rr);
-  T f = (ratio - T(1.3)) / (T(1.6) - T(1.3));
+  T f = wdiv<T>(ratio - T(1.3), T(1.6) - T(1.3));
   f = fmax(T(0), fmin(f, T(1)));
   // optimal face weights (order 3)
   T wl[3] = {w[0] * T(1. / 16.), w[1] * T(5. / 8.), w[2] * T(5. / 16.)};
@@ -382,8 +394,8 @@ __device__ __forceinline__ void weno5_edges(const T* u, const T* w, const T* wm,
   T sl = symsum3(wl[0], wl[1], wl[2]), sr = symsum3(wr[0], wr[1], wr[2]);
 #pragma unroll
   for (int s = 0; s < 3; s++) {
-    wl[s] /= (sl + WenoEps<T>::tiny);
-    wr[s] /= (sr + WenoEps<T>::tiny);
+    wl[s] = wdiv<T>(wl[s], sl + WenoEps<T>::tiny);
+    wr[s] = wdiv<T>(wr[s], sr + WenoEps<T>::tiny);
   }
   const bool two = (T(0) < f);
   if (two) {
@@ -417,8 +429,8 @@ __device__ __forceinline__ void weno5_edges(const T* u, const T* w, const T* wm,
     T sl3 = symsum2(l3[0], l3[1]), sr3 = symsum2(r3[0], r3[1]);
 #pragma unroll
     for (int s = 0; s < 2; s++) {
-      l3[s] /= (sl3 + WenoEps<T>::tiny);
-      r3[s] /= (sr3 + WenoEps<T>::tiny);
+      l3[s] = wdiv<T>(l3[s], sl3 + WenoEps<T>::tiny);
+      r3[s] = wdiv<T>(r3[s], sr3 + WenoEps<T>::tiny);
       l3[s] *= f;
       r3[s] *= f;
     }

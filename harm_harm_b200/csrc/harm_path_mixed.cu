@@ -4,25 +4,26 @@
 #include "harm_paths.h"
 
 template <int LIM>
-static void flux_dirs_float(harm_ctx* c, const Dims& d, const Phys& ph, const double* pb, float* F1, float* F2, float* F3,
+static int flux_dirs_float(harm_ctx* c, const Dims& d, const Phys& ph, const double* pb, float* F1, float* F2, float* F3,
                          unsigned long long* slots) {
   FaceBox b1 = face_box(d, 1), b2 = face_box(d, 2), b3 = face_box(d, 3);
-  k_flux<1, float, float, LIM><<<nblk(b1.n), 256, 0, c->stream>>>(d, ph, b1, pb, c->d_geomf, F1, slots + 0);
-  k_flux<2, float, float, LIM><<<nblk(b2.n), 256, 0, c->stream>>>(d, ph, b2, pb, c->d_geomf, F2, slots + 1);
+  CK((launch_fluxt<1, LIM, float, float>(d, ph, b1, pb, c->d_geomf, F1, slots + 0, c->stream)));
+  CK((launch_fluxt<2, LIM, float, float>(d, ph, b2, pb, c->d_geomf, F2, slots + 1, c->stream)));
   c->launches += 2;
   if (d.n3 > 1) {
-    k_flux<3, float, float, LIM><<<nblk(b3.n), 256, 0, c->stream>>>(d, ph, b3, pb, c->d_geomf, F3, slots + 2);
+    CK((launch_fluxt<3, LIM, float, float>(d, ph, b3, pb, c->d_geomf, F3, slots + 2, c->stream)));
     c->launches++;
   }
+  return 0;
 }
 
 int hp_fluxes_mixed(harm_ctx* c, const double* pb, float* F1, float* F2, float* F3, float* emf,
                    unsigned long long* slots) {
   Dims d = dims_of(c->g);
   Phys ph = phys_of(c->g);
-  if (c->g.lim == HARM_LIM_WENO5) flux_dirs_float<HARM_LIM_WENO5>(c, d, ph, pb, F1, F2, F3, slots);
-  else if (c->g.lim == HARM_LIM_PARA) flux_dirs_float<HARM_LIM_PARA>(c, d, ph, pb, F1, F2, F3, slots);
-  else flux_dirs_float<HARM_LIM_MC>(c, d, ph, pb, F1, F2, F3, slots);
+  if (c->g.lim == HARM_LIM_WENO5) { int rc = flux_dirs_float<HARM_LIM_WENO5>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
+  else if (c->g.lim == HARM_LIM_PARA) { int rc = flux_dirs_float<HARM_LIM_PARA>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
+  else { int rc = flux_dirs_float<HARM_LIM_MC>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
   long long nc = (long long)(d.n1 + 1) * (d.n2 + 1) * (d.n3 > 1 ? d.n3 + 1 : 1);
   k_emf<float, float><<<nblk(nc), 256, 0, c->stream>>>(d, F1, F2, F3, c->d_geomf, emf);
   c->launches++;
