@@ -19,6 +19,7 @@ HARM_G_GCOV, HARM_G_GCON, HARM_G_GCOVPERT_TT, HARM_G_ALPHA = 0, 10, 20, 21
 HARM_G_BETASQOALPHASQ, HARM_G_BETA, HARM_G_GDET, HARM_G_IGDET = 22, 23, 26, 27
 HARM_AUX_R, HARM_AUX_RHOFLOOR, HARM_AUX_UFLOOR = 0, 1, 2
 HARM_NOALLOC_MAX_CELLS = 2097152
+HARM_MLP_NIN, HARM_MLP_NOUT, HARM_MLP_NPARAMS, HARM_MLP_NNORM = 10, 2, 9154, 24
 
 
 class harm_grid(C.Structure):
@@ -63,6 +64,14 @@ _DEVICE_SIGS = {
     "harm_b200_utoprimgen_points": (Ip, [P, C.c_size_t, Ip, P, P, P, P, P]),
     "harm_b200_time_stages": (Ip, [P, Ip, Ip, P, D, Ip, C.POINTER(D)]),
     "harm_b200_fluxcalc_noalloc": (Ip, [C.POINTER(harm_grid), P, P, P, P, P, C.POINTER(D), P]),
+    "harm_b200_mlp_dump": (Ip, [P, P, Ip, Ip, C.c_size_t, P, P, P, C.POINTER(C.c_size_t)]),
+    "harm_b200_mlp_synth": (Ip, [P, C.c_size_t, C.c_uint64, P, P, P, P, P]),
+    "harm_b200_mlp_norm": (Ip, [P, C.c_size_t, P, P, P]),
+    "harm_b200_mlp_init": (Ip, [P, C.c_uint64, P]),
+    "harm_b200_mlp_loss_grad": (Ip, [P, C.c_size_t, P, P, P, P, C.POINTER(D), P]),
+    "harm_b200_mlp_train": (Ip, [P, C.c_size_t, P, P, P, P, Ip, Ip, C.c_float, C.c_uint64, P]),
+    "harm_b200_mlp_set": (Ip, [P, P, P, D]),
+    "harm_b200_mlp_predict": (Ip, [P, C.c_size_t, P, P]),
     "harm_b200_last_error": (C.c_char_p, []),
 }
 

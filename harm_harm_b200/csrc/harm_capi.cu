@@ -129,10 +129,19 @@ extern "C" int harm_b200_fluxcalc(harm_ctx* c, int precision, const double* d_pb
   return 0;
 }
 
+// the learned guess needs a network set by harm_b200_mlp_set
+static int check_guess(harm_ctx* c, int guess) {
+  if (guess != HARM_GUESS_PREV && guess != HARM_GUESS_MLP) return seterr_msg("unknown guess", 2);
+  if (guess == HARM_GUESS_MLP && (!c->d_mlp || !c->mlp_step))
+    return seterr_msg("HARM_GUESS_MLP without a network (harm_b200_mlp_set)", 3);
+  return 0;
+}
+
 // one substep on the device; dt from d_dt, dt minima of this substep into slots
 static int substep(harm_ctx* c, int precision, int guess, int timeorder, int numtimeorders, const double* d_pi,
                    const double* d_pb, double* d_pf, int8_t* d_pflag, const double* CUf, const double* Cunew,
                    unsigned long long* slots, bool with_stats) {
+  if (int rc = check_guess(c, guess)) return rc;
   StepCoef sc;
   sc.CUf0 = CUf[0]; sc.CUf2 = CUf[2];
   sc.Cun0 = Cunew[0]; sc.Cun1 = Cunew[1]; sc.Cun2 = Cunew[2];
@@ -225,9 +234,9 @@ extern "C" int harm_b200_step_host(harm_ctx* c, int precision, int guess, double
 
 extern "C" int harm_b200_utoprimgen_points(harm_ctx* c, size_t n, int guess, const double* d_U, const double* d_geom,
                                            double* d_P, int8_t* d_pflag, int32_t* d_iters) {
-  (void)guess;
+  if (int rc = check_guess(c, guess)) return rc;
   if (n == 0) return 0;
-  if (hp_points(c, n, d_U, d_geom, d_P, d_pflag, d_iters)) return 1;
+  if (hp_points(c, n, guess, d_U, d_geom, d_P, d_pflag, d_iters)) return 1;
   CK(cudaStreamSynchronize(c->stream));
   return 0;
 }
@@ -237,6 +246,7 @@ extern "C" int harm_b200_time_stages(harm_ctx* c, int precision, int guess, cons
                                      double* ms) {
   static const double CUf[4] = {1.0, 0.0, 0.5, 0.0};
   static const double Cun[4] = {0.0, 0.0, 0.0, 0.0};
+  if (int rc = check_guess(c, guess)) return rc;
   if (reps < 1) reps = 1;
   cudaEvent_t ev[6];
   for (int q = 0; q < 6; q++) CK(cudaEventCreate(&ev[q]));

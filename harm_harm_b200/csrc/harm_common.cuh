@@ -14,6 +14,7 @@
 #include "harm_b200.h"
 #include "harm_device.cuh"
 #include "harm_invert.cuh"
+#include "harm_mlp.cuh"
 #include "harm_ctx.cuh"
 
 using namespace hb;
@@ -451,17 +452,23 @@ static inline dim3 fluxt_grid(const FaceBox& fb) {
   return dim3((fb.cnt[0] + NT - 1) / NT, (fb.cnt[2] + A - 1) / A, fb.cnt[1]);
 }
 
-// launch k_fluxt<DIR, LIM, T, GT>; the first launch of each instantiation raises its dynamic
-// shared-memory limit (the FP32 WENO5 tile needs 63 KB)
+// launch k_fluxt<DIR, LIM, T, GT>; the first launch of an instantiation on a device raises
+// its dynamic shared-memory limit where the tile needs more than 48 KB (FP32 WENO5: 63 KB)
 template <int DIR, int LIM, typename T, typename GT>
 static inline cudaError_t launch_fluxt(const Dims& d, const Phys& ph, const FaceBox& fb, const double* P,
                                        const GT* geom, T* F, unsigned long long* dtslot, cudaStream_t st) {
   constexpr size_t smem = FluxTile<LIM, T>::smem;
-  static bool attr_set = false;  // per instantiation; setting it twice is harmless
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(k_fluxt<DIR, LIM, T, GT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (smem > 48 * 1024) {
+    static unsigned long long attr_devices = 0;  // per instantiation: devices already raised
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    attr_set = true;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(attr_devices & bit)) {
+      e = cudaFuncSetAttribute(k_fluxt<DIR, LIM, T, GT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      attr_devices |= bit;
+    }
   }
   k_fluxt<DIR, LIM, T, GT><<<fluxt_grid<DIR, LIM>(fb), 256, smem, st>>>(d, ph, fb, P, geom, F, dtslot);
   return cudaGetLastError();
@@ -725,6 +732,86 @@ __global__ void __launch_bounds__(256, 2) k_invert(Dims d, Phys ph, const double
     for (int p = 0; p < NPR; p++) pf[(size_t)p * d.cells + id] = pr[p];
   }
   if (stats) warp_add_atomic(iters_d, stats + 0);
+}
+
+// Inversion with the learned guess: the same work as k_invert, except that the Newton
+// iteration starts from the network's W' (evaluated per warp on the tensor cores between
+// the setup and the solve) and, when that start does not converge, starts again from the
+// previous-state W' exactly as k_invert does (counted in stats[2]).  A persistent grid
+// (two blocks per SM) walks the cells in tiles of 256, so the packed network is copied to
+// shared memory once per block.
+template <int PATH>
+__global__ void __launch_bounds__(256, 2) k_invert_mlp(Dims d, Phys ph, const double* __restrict__ U,
+                                                       const double* __restrict__ pb, double* __restrict__ pf,
+                                                       int8_t* __restrict__ pflag, const double* __restrict__ geom,
+                                                       const double* __restrict__ aux, unsigned int* __restrict__ rare,
+                                                       unsigned int* __restrict__ nrare, double* __restrict__ stats,
+                                                       const MlpPacked* __restrict__ mlp) {
+  __shared__ MlpPacked sm;
+  __shared__ MlpWarpScratch wsc[8];
+  mlp_load_packed(sm, mlp);
+  __syncthreads();
+  const long long ncell = (long long)d.n1 * d.n2 * d.n3;
+  double iters_d = 0.0, fb_d = 0.0;
+  for (long long base = (long long)blockIdx.x * 256; base < ncell; base += (long long)gridDim.x * 256) {
+    const long long t = base + threadIdx.x;
+    const bool valid = t < ncell;
+    size_t id = 0, c2 = 0;
+    JonSetup s;
+    double pr[NPR];
+    float f[MLP_IN];
+    if (valid) {
+      int i = (int)(t % d.n1);
+      long long r = t / d.n1;
+      int j = (int)(r % d.n2), k = (int)(r / d.n2);
+      int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
+      id = cidx(d, ii, jj, kk);
+      c2 = (size_t)jj * d.n1e + ii;
+      Geo<double> g;
+      load_geo<double, double>(geom, d.plane, c2, g);
+      double Ugf[NPR];
+#pragma unroll
+      for (int p = 0; p < NPR; p++) { Ugf[p] = U[(size_t)p * d.cells + id] * g.igdet; pr[p] = pb[(size_t)p * d.cells + id]; }
+      jon_prepare(false, Ugf, g, pr, ph.gam, ph.gammafail, s);
+      mlp_features(s.c, g, f);
+    }
+    float y[MLP_OUT];
+    mlp_warp_eval(sm, wsc[threadIdx.x >> 5], f, valid, y);
+    if (valid) {
+      int8_t flag = 0;
+      int it = 0;
+      jon_solve(s, mlp_wp_guess(y[0], sm.start_bias, s), pr, flag, it);
+      if (flag != 0) {  // the learned start did not converge: the plain start
+        fb_d += 1.0;
+        jon_solve(s, s.Wp_prev, pr, flag, it);
+      }
+      iters_d += (double)it;
+      bool defer = (flag != 0);
+      if (!defer) {
+        double rhofl = __ldg(aux + (size_t)HARM_AUX_RHOFLOOR * d.plane + c2);
+        double ufl = __ldg(aux + (size_t)HARM_AUX_UFLOOR * d.plane + c2);
+        rhofl = (rhofl < kSMALL) ? kSMALL : rhofl;
+        ufl = (ufl < kSMALL) ? kSMALL : ufl;
+        defer = (rhofl > pr[HARM_RHO]) || (ufl > pr[HARM_UU]);
+        if (!defer) {
+          Geo<double> g;
+          load_geo<double, double>(geom, d.plane, c2, g);
+          limit_gamma<double>(ph.gammamax, pr, g);
+        }
+      }
+      if (defer) {
+        unsigned int slot = atomicAdd(nrare, 1u);
+        rare[slot] = (unsigned int)t;
+      }
+      pflag[id] = flag;
+#pragma unroll
+      for (int p = 0; p < NPR; p++) pf[(size_t)p * d.cells + id] = pr[p];
+    }
+  }
+  if (stats) {
+    warp_add_atomic(iters_d, stats + 0);
+    warp_add_atomic(fb_d, stats + 2);
+  }
 }
 
 // Inversion, rare path over the listed cells: the cold fallback of a failed hot inversion

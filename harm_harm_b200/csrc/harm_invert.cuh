@@ -258,11 +258,21 @@ static __device__ int inv_finish(double Wp, const InvC& c, const double* Qtcon, 
   return 0;
 }
 
-// Hot or cold Jon inversion on geometry-free U (Utoprim_jon_nonrelcompat_inputnorestmass).
-// `wpguess` >= 0 replaces the previous-state W' when use_guess is set.
-static __device__ __forceinline__ void utoprim_jon(bool cold, const double* Ugf, const Geo<double>& g, int8_t& flag, double* prim, double gam,
-                            double gammafail, int& nstroke, bool use_guess, double wpguess) {
-  int lntries = 0;
+// The inversion split in two: jon_prepare computes everything that does not depend on the
+// starting W' (the alpha-scaled setup quantities and the previous-state guess with its
+// convergence scales wglobal), jon_solve runs verify_Wlast, the Newton iteration and Wp2prim
+// from a given starting W'.  The learned guess runs between the two.
+struct JonSetup {
+  InvC c;
+  double Qtcon[4], Bcon[4];
+  double Wp_prev;  // set_guess_Wp's W' from the previous primitive state
+  int8_t flag0;    // flag raised by the setup (cold-HD guess without a root)
+};
+
+// Utoprim_jon_nonrelcompat_inputnorestmass up to set_guess_Wp, on geometry-free U.
+// prim's field components are replaced by U's (as the reference does on entry).
+static __device__ __forceinline__ void jon_prepare(bool cold, const double* Ugf, const Geo<double>& g, double* prim,
+                                                   double gam, double gammafail, JonSetup& s) {
   double U[NPR], pt[NPR];
   const double alpha = g.alpha;
 #pragma unroll
@@ -275,24 +285,40 @@ static __device__ __forceinline__ void utoprim_jon(bool cold, const double* Ugf,
   prim[HARM_B1] = Ugf[HARM_B1];
   prim[HARM_B2] = Ugf[HARM_B2];
   prim[HARM_B3] = Ugf[HARM_B3];
-  InvC c;
-  c.cold = cold;
-  c.gam = gam;
-  c.gsq_too_big = gammafail * gammafail;
-  c.utsq_too_big = (gammafail - 1.0) * (gammafail - 1.0);
-  flag = HARM_UTOPRIMNOFAIL;
-  double Qtcon[4], Bcon[4], Wp;
-  int retval = inv_setup(U, g, pt, c, Qtcon, Bcon, Wp, flag);
-  if (use_guess) Wp = wpguess;
-  retval += inv_verify_guess(Wp, c, flag);
-  retval += newton(flag, Wp, c, lntries, nstroke);
-  if (retval == 0) retval = inv_finish(Wp, c, Qtcon, Bcon, pt, flag);
+  s.c.cold = cold;
+  s.c.gam = gam;
+  s.c.gsq_too_big = gammafail * gammafail;
+  s.c.utsq_too_big = (gammafail - 1.0) * (gammafail - 1.0);
+  s.flag0 = HARM_UTOPRIMNOFAIL;
+  inv_setup(U, g, pt, s.c, s.Qtcon, s.Bcon, s.Wp_prev, s.flag0);
+}
+
+// The rest of the inversion from the starting W' `Wp`: prim[RHO..U3] receive the
+// primitives on success; flag the outcome; wp_out (optional) the final W'.
+static __device__ __forceinline__ void jon_solve(const JonSetup& s, double Wp, double* prim, int8_t& flag, int& nstroke,
+                                                 double* wp_out = nullptr) {
+  int lntries = 0;
+  flag = s.flag0;
+  int retval = inv_verify_guess(Wp, s.c, flag);
+  retval += newton(flag, Wp, s.c, lntries, nstroke);
+  if (wp_out) *wp_out = Wp;
+  double pt[5];
+  if (retval == 0) retval = inv_finish(Wp, s.c, s.Qtcon, s.Bcon, pt, flag);
   if (retval == 0) {
 #pragma unroll
     for (int i = 0; i <= HARM_U3; i++) prim[i] = pt[i];
   } else {
     if (flag <= 0) flag = (int8_t)(retval + HARM_UTOPRIMFAILCONVRET + 1);
   }
+}
+
+// Hot or cold Jon inversion on geometry-free U (Utoprim_jon_nonrelcompat_inputnorestmass).
+// `wpguess` replaces the previous-state W' when use_guess is set.
+static __device__ __forceinline__ void utoprim_jon(bool cold, const double* Ugf, const Geo<double>& g, int8_t& flag, double* prim, double gam,
+                            double gammafail, int& nstroke, bool use_guess, double wpguess) {
+  JonSetup s;
+  jon_prepare(cold, Ugf, g, prim, gam, gammafail, s);
+  jon_solve(s, use_guess ? wpguess : s.Wp_prev, prim, flag, nstroke);
 }
 
 // Utoprimgen from UEVOLVE U (igdet scales to geometry-free).  Returns the Newton iterations.

@@ -1,6 +1,7 @@
 // harm_path_fp64.cu -- FP64 path of the step (compiled with -fmad=false) and the FP64
 // kernels shared by both paths: boundary conditions, fixups, dt finalisation, point
 // inversions.
+#include <algorithm>
 #include "harm_common.cuh"
 #include "harm_paths.h"
 
@@ -223,6 +224,51 @@ __global__ void k_utoprim_points(size_t n, Phys ph, const double* __restrict__ U
   if (iters) iters[t] = it;
 }
 
+// the same with the learned start of the hot inversion (fallback to the plain start inside
+// utoprimgen); stats[2] counts the fallbacks
+__global__ void __launch_bounds__(256, 2) k_utoprim_points_mlp(size_t n, Phys ph, const double* __restrict__ U,
+                                                               const double* __restrict__ geom, double* __restrict__ P,
+                                                               int8_t* __restrict__ pflag, int32_t* __restrict__ iters,
+                                                               const MlpPacked* __restrict__ mlp, double* stats) {
+  __shared__ MlpPacked sm;
+  __shared__ MlpWarpScratch wsc[8];
+  mlp_load_packed(sm, mlp);
+  __syncthreads();
+  double fb_d = 0.0;
+  for (size_t base = (size_t)blockIdx.x * 256; base < n; base += (size_t)gridDim.x * 256) {
+    const size_t t = base + threadIdx.x;
+    const bool valid = t < n;
+    Geo<double> g;
+    double u[NPR], pr[NPR];
+    float f[MLP_IN];
+    JonSetup s;
+    if (valid) {
+      load_geo<double, double>(geom, n, t, g);
+      double Ugf[NPR], prc[NPR];
+      for (int p = 0; p < NPR; p++) {
+        u[p] = U[(size_t)p * n + t];
+        pr[p] = P[(size_t)p * n + t];
+        Ugf[p] = u[p] * g.igdet;
+        prc[p] = pr[p];
+      }
+      jon_prepare(false, Ugf, g, prc, ph.gam, ph.gammafail, s);
+      mlp_features(s.c, g, f);
+    }
+    float y[MLP_OUT];
+    mlp_warp_eval(sm, wsc[threadIdx.x >> 5], f, valid, y);
+    if (valid) {
+      int8_t flag = 0;
+      bool failed = false;
+      int it = utoprimgen(u, g, g.igdet, pr, flag, ph.gam, ph.gammafail, true, mlp_wp_guess(y[0], sm.start_bias, s),
+                          &failed);
+      fb_d += failed ? 1.0 : 0.0;
+      for (int p = 0; p < NPR; p++) P[(size_t)p * n + t] = pr[p];
+      pflag[t] = flag;
+      if (iters) iters[t] = it;
+    }
+  }
+  if (stats) warp_add_atomic(fb_d, stats + 2);
+}
 
 // ------------------------------------------------------------------ launchers
 
@@ -262,8 +308,13 @@ int hp_update_fp64(harm_ctx* c, const StepCoef& sc, const double* pi, const doub
   k_conserved<double><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, sc, c->d_dt, pi, pb, c->d_F[0], c->d_F[1],
                                                           c->d_F[2], c->d_emf, c->d_geom, c->d_conn, c->d_U);
   CK(cudaMemsetAsync(c->d_nrare, 0, sizeof(unsigned int), c->stream));
-  k_invert<0><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare, c->d_nrare,
-                                                  stats);
+  if (sc.guess == HARM_GUESS_MLP) {
+    k_invert_mlp<0><<<2 * 148, 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
+                                                     c->d_nrare, stats, reinterpret_cast<const MlpPacked*>(c->d_mlp));
+  } else {
+    k_invert<0><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
+                                                    c->d_nrare, stats);
+  }
   k_invert_rare<0><<<2 * 148, 128, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
                                                      c->d_nrare, stats);
   c->launches += 3;
@@ -324,9 +375,16 @@ int hp_finalize_dt(harm_ctx* c, double* dt, double* ndt_out, int nsub) {
   return 0;
 }
 
-int hp_points(harm_ctx* c, size_t n, const double* U, const double* geom, double* P, int8_t* pflag, int32_t* iters) {
+int hp_points(harm_ctx* c, size_t n, int guess, const double* U, const double* geom, double* P, int8_t* pflag,
+              int32_t* iters) {
   Phys ph = phys_of(c->g);
-  k_utoprim_points<<<nblk((long long)n), 256, 0, c->stream>>>(n, ph, U, geom, P, pflag, iters);
+  if (guess == HARM_GUESS_MLP) {
+    const unsigned int nb = (unsigned int)std::min<size_t>((n + 255) / 256, (size_t)2 * 148);
+    k_utoprim_points_mlp<<<nb, 256, 0, c->stream>>>(n, ph, U, geom, P, pflag, iters,
+                                                   reinterpret_cast<const MlpPacked*>(c->d_mlp), c->d_stats);
+  } else {
+    k_utoprim_points<<<nblk((long long)n), 256, 0, c->stream>>>(n, ph, U, geom, P, pflag, iters);
+  }
   c->launches++;
   CK(cudaGetLastError());
   return 0;

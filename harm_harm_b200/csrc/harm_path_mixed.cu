@@ -39,8 +39,13 @@ int hp_update_mixed(harm_ctx* c, const StepCoef& sc, const double* pi, const dou
   k_conserved<float><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, sc, c->d_dt, pi, pb, c->d_Ff[0], c->d_Ff[1],
                                                          c->d_Ff[2], c->d_emff, c->d_geom, c->d_conn, c->d_U);
   CK(cudaMemsetAsync(c->d_nrare, 0, sizeof(unsigned int), c->stream));
-  k_invert<1><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare, c->d_nrare,
-                                                  stats);
+  if (sc.guess == HARM_GUESS_MLP) {
+    k_invert_mlp<1><<<2 * 148, 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
+                                                     c->d_nrare, stats, reinterpret_cast<const MlpPacked*>(c->d_mlp));
+  } else {
+    k_invert<1><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
+                                                    c->d_nrare, stats);
+  }
   k_invert_rare<1><<<2 * 148, 128, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
                                                      c->d_nrare, stats);
   c->launches += 3;

@@ -18,4 +18,4 @@ int hp_bound(harm_ctx* c, double* P, int8_t* flag);
 int hp_copy_ghosts(harm_ctx* c, const double* pb, double* pf);
 int hp_fixup(harm_ctx* c, double* pf, int8_t* pflag);
 int hp_finalize_dt(harm_ctx* c, double* dt, double* ndt_out, int nsub);
-int hp_points(harm_ctx* c, size_t n, const double* U, const double* geom, double* P, int8_t* pflag, int32_t* iters);
+int hp_points(harm_ctx* c, size_t n, int guess, const double* U, const double* geom, double* P, int8_t* pflag, int32_t* iters);

@@ -11,6 +11,9 @@ the same operations:
     Harm.post_fixup                post_fixup (fixup.c:53)
     Harm.Utoprimgen                Utoprimgen (utoprimgen.c:32), over a batch of points
     Harm.step_ch                   step_ch_full (step_ch.c:35): one full RK2 step
+    Harm.mlp_*                     the learned starting point of the inversion (replaces
+                                   set_guess_Wp utoprim_jon.c:890 under HARM_GUESS_MLP):
+                                   training pairs, training, packing, inference
 
 Device arrays are torch CUDA tensors (torch is only the allocator and stream owner here);
 every numeric routine runs in libharm_b200.so.  Errors are raised as RuntimeError with the
@@ -173,3 +176,45 @@ class Harm:
         ms = (C.c_double * 5)()
         self._check(self.lib.harm_b200_time_stages(self._ctx, precision, guess, _ptr(P), dt, reps, ms), "time_stages")
         return dict(zip(("flux", "emf", "update_invert", "bound", "post_fixup"), list(ms)))
+
+    # ---------------------------------------------------------------- learned guess
+    def mlp_dump(self, P, feat, targ, cell=None, stride: int = 1, phase: int = 0) -> int:
+        """Training pairs from the most recent inversion of this context (its U and the
+        primitives P it produced); returns the number written (at most len(feat))."""
+        n = C.c_size_t()
+        self._check(self.lib.harm_b200_mlp_dump(self._ctx, _ptr(P), stride, phase, feat.shape[0], _ptr(feat),
+                                                _ptr(targ), _ptr(cell), C.byref(n)), "mlp_dump")
+        return int(n.value)
+
+    def mlp_synth(self, feat, targ, seed: int, U=None, P=None, cell=None) -> None:
+        self._check(self.lib.harm_b200_mlp_synth(self._ctx, feat.shape[0], seed, _ptr(feat), _ptr(targ), _ptr(U),
+                                                 _ptr(P), _ptr(cell)), "mlp_synth")
+
+    def mlp_norm(self, feat, targ, norm, n: int | None = None) -> None:
+        n = feat.shape[0] if n is None else n
+        self._check(self.lib.harm_b200_mlp_norm(self._ctx, n, _ptr(feat), _ptr(targ), _ptr(norm)), "mlp_norm")
+
+    def mlp_init(self, params, seed: int = 1) -> None:
+        self._check(self.lib.harm_b200_mlp_init(self._ctx, seed, _ptr(params)), "mlp_init")
+
+    def mlp_loss_grad(self, feat, targ, params, norm, grad, n: int | None = None) -> float:
+        n = feat.shape[0] if n is None else n
+        loss = C.c_double()
+        self._check(self.lib.harm_b200_mlp_loss_grad(self._ctx, n, _ptr(feat), _ptr(targ), _ptr(params), _ptr(norm),
+                                                     C.byref(loss), _ptr(grad)), "mlp_loss_grad")
+        return loss.value
+
+    def mlp_train(self, feat, targ, norm, params, steps: int, batch: int = 8192, lr: float = 3e-3, seed: int = 7,
+                  n: int | None = None) -> np.ndarray:
+        n = feat.shape[0] if n is None else n
+        hist = np.zeros(steps, dtype=np.float32)
+        self._check(self.lib.harm_b200_mlp_train(self._ctx, n, _ptr(feat), _ptr(targ), _ptr(norm), _ptr(params), steps,
+                                                 batch, lr, seed, _ptr(hist)), "mlp_train")
+        return hist
+
+    def mlp_set(self, params, norm, start_bias: float = 0.0) -> None:
+        self._check(self.lib.harm_b200_mlp_set(self._ctx, _ptr(params), _ptr(norm), start_bias), "mlp_set")
+
+    def mlp_predict(self, feat, out, n: int | None = None) -> None:
+        n = feat.shape[0] if n is None else n
+        self._check(self.lib.harm_b200_mlp_predict(self._ctx, n, _ptr(feat), _ptr(out)), "mlp_predict")

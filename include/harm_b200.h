@@ -216,6 +216,78 @@ int harm_b200_utoprimgen_points(harm_ctx *ctx, size_t n, int guess, const double
 int harm_b200_time_stages(harm_ctx *ctx, int precision, int guess, const double *d_P,
                           double dt, int reps, double ms[5]);
 
+/* ------------------------------------------------------------------------------------
+ * Learned initial guess of the inversion.  No counterpart function in the reference: the
+ * network replaces the starting point set_guess_Wp (utoprim_jon.c:890) computes from the
+ * previous primitive state; the Newton iteration (general_newton_raphson utoprim_jon.c:3853)
+ * and its tolerances are unchanged, and a cell whose learned start does not converge is
+ * solved again from the previous-state start.
+ *
+ * Network: 10 features -> 64 -> 64 -> 64 -> 2 outputs, SiLU.  Features of a cell, from the
+ * alpha-scaled setup quantities of U/sqrt(-g) (compute_setup_quantities utoprim_jon.c:716)
+ * and the metric, slog(x) = sign(x) log(1+|x|):
+ *   log D, slog(B^2/D), slog(Qt^2/D^2), slog((Q.B)^2/D^3), slog(-Q.n'/D),
+ *   slog(Qt^2/((Q.n')^2+D^2)), alpha, log sqrt(-g), beta^2/alpha^2, g_tt+1.
+ * Outputs: log(W'/D) (the start of the iteration) and log(1+utsq) (v^2 = utsq/(1+utsq)).
+ * Parameters: HARM_MLP_NPARAMS floats W1[10][64] b1 W2[64][64] b2 W3[64][64] b3 W4[64][2] b4.
+ * Normalisation record: HARM_MLP_NNORM floats: feature means[10], standard deviations[10],
+ * target means[2], target standard deviations[2].
+ * Arrays of pairs: d_feat[n][10], d_targ[n][2] (FP32, sample-major).
+ * ------------------------------------------------------------------------------------ */
+#define HARM_MLP_NIN 10
+#define HARM_MLP_NOUT 2
+#define HARM_MLP_NPARAMS 9154
+#define HARM_MLP_NNORM 24
+
+/* Training pairs dumped from the context's most recent inversion: the U that inversion
+   inverted and the primitives d_P it produced (active cells t = phase + stride*k, in
+   i-fastest order over active cells).  Targets are the converged W' of a plain re-solve;
+   cells whose hot inversion fails are skipped.  Writes at most `max` pairs (order not
+   fixed; d_cell, if not NULL, receives each pair's active-cell index) and their number. */
+int harm_b200_mlp_dump(harm_ctx *ctx, const double *d_P, int stride, int phase, size_t max,
+                       float *d_feat, float *d_targ, int32_t *d_cell, size_t *n_out);
+
+/* n synthetic pairs from wide primitive distributions on this context's metric (rho
+   log-uniform [1e-6,1], u/rho log-uniform [1e-4,1e2], gamma uniform [1,50], b^2/rho
+   log-uniform [1e-3,1e3], isotropic directions, Boyer-Lindquist r uniform [1.2,40]).
+   Optional outputs: d_U[8][n] (UEVOLVE), d_P[8][n] and d_cell[n] = the (i,j) offset
+   jj*n1e+ii of the metric record used. */
+int harm_b200_mlp_synth(harm_ctx *ctx, size_t n, uint64_t seed, float *d_feat, float *d_targ,
+                        double *d_U, double *d_P, int32_t *d_cell);
+
+/* Normalisation record of a training set (means and standard deviations, FP64 sums). */
+int harm_b200_mlp_norm(harm_ctx *ctx, size_t n, const float *d_feat, const float *d_targ,
+                       float *d_norm);
+
+/* Glorot-uniform weights and zero biases from `seed`. */
+int harm_b200_mlp_init(harm_ctx *ctx, uint64_t seed, float *d_params);
+
+/* Loss L = 1/(2n) sum (y - t~)^2 over the standardised targets t~ of the n pairs, and its
+   gradient d_grad[HARM_MLP_NPARAMS] (FP32 forward and backward kernels). */
+int harm_b200_mlp_loss_grad(harm_ctx *ctx, size_t n, const float *d_feat, const float *d_targ,
+                            const float *d_params, const float *d_norm, double *loss,
+                            float *d_grad);
+
+/* `steps` Adam steps (beta 0.9/0.999, learning rate lr with cosine decay to lr/100) on
+   minibatches of `batch` pairs drawn from the n pairs by a hash of `seed`; d_params is
+   updated in place.  loss_hist (host, `steps` floats, may be NULL) receives each step's
+   minibatch loss. */
+int harm_b200_mlp_train(harm_ctx *ctx, size_t n, const float *d_feat, const float *d_targ,
+                        const float *d_norm, float *d_params, int steps, int batch, float lr,
+                        uint64_t seed, float *loss_hist);
+
+/* Pack the network for inference (BF16 weights, FP32 biases and normalisation) into the
+   context; HARM_GUESS_MLP then uses it.  The Newton iteration starts from
+   W' = D exp(log(W'/D)_predicted + start_bias): a small positive bias (a few times the
+   network's typical error in log(W'/D)) starts it above the root, the side from which it
+   converges without verify_Wlast's tenfold raises of W' (utoprim_jon.c:1120). */
+int harm_b200_mlp_set(harm_ctx *ctx, const float *d_params, const float *d_norm,
+                      double start_bias);
+
+/* Outputs d_out[n][2] (de-standardised) of the packed network for features d_feat[n][10],
+   on the tensor cores as inside the inversion. */
+int harm_b200_mlp_predict(harm_ctx *ctx, size_t n, const float *d_feat, float *d_out);
+
 /* Largest grid (extended cells n1e*n2e*n3e) harm_b200_fluxcalc_noalloc accepts: its EMF
    scratch is 3 doubles per cell, 48 MiB at this size. */
 #define HARM_NOALLOC_MAX_CELLS 2097152

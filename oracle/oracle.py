@@ -60,6 +60,9 @@ def lib() -> C.CDLL:
             "orc_post_fixup": (I, [C.POINTER(orc), P, P]),
             "orc_step": (I, [C.POINTER(orc), P, C.POINTER(D), C.POINTER(N.harm_stats)]),
             "orc_reconstruct_line": (None, [I, I, P, P, P]),
+            "orc_mlp_nparams": (I, []),
+            "orc_mlp_features": (None, [C.POINTER(N.harm_grid), P, P, P, P, P]),
+            "orc_mlp_loss_grad": (D, [I, P, P, P, P, P, P]),
         }
         for fn, (res, args) in sigs.items():
             f = getattr(L, fn)
@@ -112,31 +115,61 @@ class Oracle:
         return d.value, st.as_dict()
 
 
+def _c(a, dtype=np.float64):
+    """C-contiguous array of `dtype` (the caller keeps it alive across the C call)"""
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
 def utoprimgen_point(grid, geomrec, U, pr):
-    pr = np.ascontiguousarray(pr, dtype=np.float64).copy()
+    pr = _c(pr).copy()
+    rec, Uc = _c(geomrec), _c(U)
     flag = np.zeros(1, dtype=np.int8)
     it = np.zeros(1, dtype=np.int32)
-    lib().orc_utoprimgen_point(C.byref(grid.g), _p(np.ascontiguousarray(geomrec)), _p(np.ascontiguousarray(U)),
-                               _p(pr), _p(flag), _p(it))
+    lib().orc_utoprimgen_point(C.byref(grid.g), _p(rec), _p(Uc), _p(pr), _p(flag), _p(it))
     return pr, int(flag[0]), int(it[0])
 
 
 def primtoU_point(geomrec, pr):
     U = np.zeros(8)
-    lib().orc_primtoU_point(_p(np.ascontiguousarray(geomrec)), _p(np.ascontiguousarray(pr, dtype=np.float64)), _p(U))
+    rec, prc = _c(geomrec), _c(pr)
+    lib().orc_primtoU_point(_p(rec), _p(prc), _p(U))
     return U
 
 
 def primtoflux_point(geomrec, pr, d):
     F = np.zeros(8)
-    lib().orc_primtoflux_point(_p(np.ascontiguousarray(geomrec)), _p(np.ascontiguousarray(pr, dtype=np.float64)), d,
-                               _p(F))
+    rec, prc = _c(geomrec), _c(pr)
+    lib().orc_primtoflux_point(_p(rec), _p(prc), d, _p(F))
     return F
 
 
 def reconstruct_line(lim, y):
-    y = np.ascontiguousarray(y, dtype=np.float64)
+    y = _c(y)
     yl = np.zeros_like(y)
     yr = np.zeros_like(y)
     lib().orc_reconstruct_line(lim, len(y), _p(y), _p(yl), _p(yr))
     return yl, yr
+
+
+def mlp_features(grid, geomrec, U, P=None):
+    """features (10) and, with P, targets (2) of one point"""
+    f = np.zeros(10, dtype=np.float32)
+    t = np.zeros(2, dtype=np.float32)
+    rec, Uc = _c(geomrec), _c(U)
+    Pc = None if P is None else _c(P)
+    lib().orc_mlp_features(C.byref(grid.g), _p(rec), _p(Uc), None if Pc is None else _p(Pc), _p(f), _p(t))
+    return f, t
+
+
+def mlp_loss_grad(feat, targ, params, norm):
+    """double-precision loss, gradient and de-standardised outputs of the network"""
+    feat = _c(feat, np.float32)
+    n = feat.shape[0]
+    params = _c(params, np.float32)
+    norm = _c(norm, np.float32)
+    targ = None if targ is None else _c(targ, np.float32)
+    pred = np.zeros((n, 2))
+    grad = np.zeros(lib().orc_mlp_nparams())
+    loss = lib().orc_mlp_loss_grad(n, _p(feat), None if targ is None else _p(targ), _p(params), _p(norm), _p(pred),
+                                   _p(grad))
+    return loss, grad, pred

@@ -25,6 +25,7 @@ void o_primtoflux(const double *pr, const ostate *q, int dir, const ogeom *g, do
 int o_vchar(const double *pr, const ostate *q, int dir, const ogeom *g, double gam, double *vmax, double *vmin);
 void o_source(const double *pr, const ostate *q, const ogeom *g, const double *conn, double *dU);
 int o_utoprimgen(const double *U, const ogeom *g, double *pr, int8_t *pflag, double gam, double gammafail, int *nstroke);
+void o_inv_invariants(const double *Ugf, const ogeom *g, double *out);
 int o_limit_gamma(double gammamax, double *pr, const ogeom *g);
 void o_inflow_check_x1up(double *pr, const ogeom *g, double gammamax);
 int o_fixup1zone(double *pr, const ogeom *g, double rhofl, double ufl, double gam, double gammamax,

@@ -378,6 +378,36 @@ static int newton(int8_t *lpflag, double *xio, const inv_consts *c, int *lntries
 /* Utoprim_new_body (utoprim_jon.c:406) for the hot (E'(W')) or cold (P^2(W')) equation.
    U and prim here are already alpha-scaled (Utoprim_jon_nonrelcompat_inputnorestmass
    :136).  Returns retval of the reference. */
+/* compute_setup_quantities (utoprim_jon.c:716) on alpha-scaled U */
+static void setup_quantities(const double *U, const ogeom *g, inv_consts *c, double *Bcon, double *Qtcon) {
+  double Bcov[4], ncov[4], ncon[4], Qcovp[4], Qconp[4], Qtcov[4], Qcov[4], Qcon[4];
+  c->D = U[HARM_RHO];
+  Bcon[0] = 0.;
+  for (int i = 1; i < 4; i++) Bcon[i] = U[HARM_B1 + i - 1];
+  o_lower(Bcon, g, Bcov);
+  c->Bsq = 0.;
+  for (int i = 1; i < 4; i++) c->Bsq += Bcon[i] * Bcov[i];
+  ncov[0] = -g->alpha; ncov[1] = ncov[2] = ncov[3] = 0.;
+  o_raise(ncov, g, ncon);
+  for (int i = 0; i < 4; i++) Qcovp[i] = U[HARM_UU + i];
+  o_raise(Qcovp, g, Qconp);
+  for (int j = 0; j < 4; j++) Qtcon[j] = 0.0;
+  for (int j = 1; j < 4; j++)
+    for (int i = 1; i < 4; i++) Qtcon[j] += U[HARM_UU + i] * (g->gcon[i][j] + ncon[i] * ncon[j]);
+  o_lower(Qtcon, g, Qtcov);
+  c->Qtsq = 0.;
+  for (int i = 0; i < 4; i++) c->Qtsq += Qtcov[i] * Qtcon[i];
+  for (int i = 0; i < 4; i++) Qcov[i] = (i == 0) ? Qcovp[i] - c->D : Qcovp[i];
+  o_raise(Qcov, g, Qcon);
+  c->QdotB = 0.;
+  for (int i = 1; i < 4; i++) c->QdotB += Qcov[i] * Bcon[i];
+  c->QdotBsq = c->QdotB * c->QdotB;
+  double alpha = g->alpha, alphasq = alpha * alpha;
+  double Dfactor = (-g->gcovpert_tt + alphasq * g->betasqoalphasq) / (alphasq + alpha);
+  c->Qdotnp = Qconp[0] * ncov[0] + c->D * Dfactor;
+  c->Qdotn = Qcon[0] * ncov[0];
+}
+
 static int new_body(int eomtype, int8_t *lpflag, const double *U, const ogeom *g, double *prim,
                     double gam, double gammafail, int *lntries, int *nstroke, double *Wp_guess_io,
                     int use_guess) {
@@ -389,34 +419,9 @@ static int new_body(int eomtype, int8_t *lpflag, const double *U, const ogeom *g
   c.utsq_too_big = (gammafail - 1.0) * (gammafail - 1.0);
   *lpflag = HARM_UTOPRIMNOFAIL;
   int retval = 0;
-  /* compute_setup_quantities (utoprim_jon.c:716) */
-  double Bcon[4], Bcov[4], ncov[4], ncon[4], Qcovp[4], Qconp[4], Qtcon[4], Qtcov[4], Qcov[4], Qcon[4];
-  c.D = U[HARM_RHO];
+  double Bcon[4], Qtcon[4];
   for (int i = HARM_B1; i <= HARM_B3; i++) prim[i] = U[i];
-  Bcon[0] = 0.;
-  for (int i = 1; i < 4; i++) Bcon[i] = U[HARM_B1 + i - 1];
-  o_lower(Bcon, g, Bcov);
-  c.Bsq = 0.;
-  for (int i = 1; i < 4; i++) c.Bsq += Bcon[i] * Bcov[i];
-  ncov[0] = -g->alpha; ncov[1] = ncov[2] = ncov[3] = 0.;
-  o_raise(ncov, g, ncon);
-  for (int i = 0; i < 4; i++) Qcovp[i] = U[HARM_UU + i];
-  o_raise(Qcovp, g, Qconp);
-  for (int j = 0; j < 4; j++) Qtcon[j] = 0.0;
-  for (int j = 1; j < 4; j++)
-    for (int i = 1; i < 4; i++) Qtcon[j] += U[HARM_UU + i] * (g->gcon[i][j] + ncon[i] * ncon[j]);
-  o_lower(Qtcon, g, Qtcov);
-  c.Qtsq = 0.;
-  for (int i = 0; i < 4; i++) c.Qtsq += Qtcov[i] * Qtcon[i];
-  for (int i = 0; i < 4; i++) Qcov[i] = (i == 0) ? Qcovp[i] - c.D : Qcovp[i];
-  o_raise(Qcov, g, Qcon);
-  c.QdotB = 0.;
-  for (int i = 1; i < 4; i++) c.QdotB += Qcov[i] * Bcon[i];
-  c.QdotBsq = c.QdotB * c.QdotB;
-  double alpha = g->alpha, alphasq = alpha * alpha;
-  double Dfactor = (-g->gcovpert_tt + alphasq * g->betasqoalphasq) / (alphasq + alpha);
-  c.Qdotnp = Qconp[0] * ncov[0] + c.D * Dfactor;
-  c.Qdotn = Qcon[0] * ncov[0];
+  setup_quantities(U, g, &c, Bcon, Qtcon);
 
   /* set_guess_Wp (utoprim_jon.c:890) */
   double Wp_last, W_last;
@@ -635,4 +640,18 @@ int o_fixup1zone(double *pr, const ogeom *g, double rhofl, double ufl, double ga
   }
   o_limit_gamma(gammamax, pr, g);
   return did;
+}
+
+/* the alpha-scaled setup invariants {D, B^2, Qt^2, (Q.B)^2, Q.n'} of geometry-free U */
+void o_inv_invariants(const double *Ugf, const ogeom *g, double *out) {
+  double U[HARM_NPR], Bcon[4], Qtcon[4];
+  inv_consts c;
+  memset(&c, 0, sizeof(c));
+  for (int i = 0; i < HARM_NPR; i++) U[i] = g->alpha * Ugf[i];
+  setup_quantities(U, g, &c, Bcon, Qtcon);
+  out[0] = c.D;
+  out[1] = c.Bsq;
+  out[2] = c.Qtsq;
+  out[3] = c.QdotBsq;
+  out[4] = c.Qdotnp;
 }
