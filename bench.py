@@ -2,9 +2,11 @@
 
 A "step" is one full RK2 timestep (two advance() substeps with bounds and fixups) of the
 Fishbone-Moncrief torus on one grid.  Default workload: 384 x 192 x 128 zones (r, theta,
-phi), HLL, Toth flux-CT, mixed precision (FP32 reconstruction/HLL/CT, FP64 update and
-inversion), initial state built on the host (synthetic, seeded).  The plain FP64 device path
-is timed on the same grid beside it.
+phi), WENO5, HLL, Toth flux-CT, mixed precision (FP32 reconstruction/HLL/CT, FP64 update and
+inversion) with the learned starting point of the inversion, initial state built on the
+host (synthetic, seeded).  Before the timed region the plain method runs a few steps and
+dumps its (U, P) pairs, and the network is trained on them on the GPU.  The plain FP64
+device path and the mixed path with the plain guess are timed on the same grid beside it.
 
 Multi-GPU: the torus update does not shard in this build (one GPU per grid), so
 `--gpus N` runs N independent replicas, one per rank, and reports their aggregate.
@@ -55,6 +57,19 @@ def update_kernel_bytes_per_cell(n3: int, precision: int) -> float:
     (94 doubles per (i,j), reused along phi)."""
     w = 8 if precision == 0 else 4
     return 64 + 64 + 15 * w + 3 * w + 64 + 1 + 94 * 8 / n3
+
+
+def flux_bytes_per_cell(n3: int, precision: int) -> float:
+    """Algorithmic bytes of the three flux kernels per active cell: each direction reads the
+    8 FP64 primitives once (64 B) and writes 8 fluxes (FP32 in the mixed path: 32 B, FP64:
+    64 B), plus the face metric record (28 values per (i,j), reused along phi)."""
+    w = 4 if precision == 1 else 8
+    return 3 * (64 + 8 * w + 28 * w / n3)
+
+
+# DRAM traffic per flux launch (bytes read + written, ncu dram__bytes_*.sum) per active
+# cell, from the captures summarised in profiles/, scaled to the workload's cell count
+FLUX_TRAFFIC = {}
 
 
 def clock_sampler(stop: threading.Event, out: list, dev: int):
@@ -206,9 +221,42 @@ def cpu_baseline_sample(args, lim) -> dict:
             "sample": f"{nst} RK2 steps of a {n1}x{n2}x{sn3} slab of the torus, FP64, OpenMP ({el:.1f} s)"}
 
 
+def train_guess(dev, Pd, dt0, prec, args):
+    """The plain method runs `train_steps` steps from the initial state; after each, its
+    (U, P) pairs are dumped (every `stride`-th cell); the network is trained on them."""
+    import torch
+    from harm_harm_b200 import HARM_GUESS_PREV
+    g = dev.grid.g
+    ncell = g.n1 * g.n2 * g.n3
+    stride = max(1, (ncell * args.train_steps) // args.train_pairs)
+    cap = ncell // stride + 1
+    feat = torch.zeros((cap * args.train_steps, 10), device="cuda", dtype=torch.float32)
+    targ = torch.zeros((cap * args.train_steps, 2), device="cuda", dtype=torch.float32)
+    P = Pd.clone()
+    dt, n = dt0, 0
+    t0 = time.perf_counter()
+    for s in range(args.train_steps):
+        dt, _ = dev.step_ch(P, dt, precision=prec, guess=HARM_GUESS_PREV, stats=False)
+        n += dev.mlp_dump(P, feat[n:n + cap], targ[n:n + cap], stride=stride, phase=s % stride)
+    del P
+    feat, targ = feat[:n].contiguous(), targ[:n].contiguous()
+    norm = torch.zeros(24, device="cuda", dtype=torch.float32)
+    params = torch.zeros(9154, device="cuda", dtype=torch.float32)
+    dev.mlp_norm(feat, targ, norm)
+    dev.mlp_init(params, seed=args.seed)
+    t1 = time.perf_counter()
+    hist = dev.mlp_train(feat, targ, norm, params, steps=args.train_iters, batch=8192, lr=3e-3, seed=args.seed)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    dev.mlp_set(params, norm, args.start_bias)
+    return {"pairs": n, "dump_steps": args.train_steps, "dump_stride": stride, "adam_steps": args.train_iters,
+            "batch": 8192, "dump_s": round(t1 - t0, 3), "train_s": round(t2 - t1, 3),
+            "loss_first": float(hist[0]), "loss_last100": float(hist[-100:].mean()), "start_bias": args.start_bias}
+
+
 def run_ours(args, ws, rank, local):
     import torch
-    from harm_harm_b200 import HARM_PREC_FP64, HARM_PREC_MIXED, Grid, Harm
+    from harm_harm_b200 import HARM_GUESS_MLP, HARM_GUESS_PREV, HARM_PREC_FP64, HARM_PREC_MIXED, Grid, Harm
     torch.cuda.set_device(local)
     n1, n2, n3, lim = CONFIGS[args.config]
     lim = LIMS.get(args.lim, lim)
@@ -217,6 +265,7 @@ def run_ours(args, ws, rank, local):
     P0 = g.torus_init(geom, aux, seed=args.seed + rank)
     dev = Harm(g, geom, conn, aux, device=local)
     prec = HARM_PREC_MIXED if args.precision == "mixed" else HARM_PREC_FP64
+    guess = HARM_GUESS_MLP if args.guess == "mlp" else HARM_GUESS_PREV
     Pd = torch.from_numpy(P0).cuda()
     dev.bound_prim(Pd)
     torch.cuda.synchronize()
@@ -227,16 +276,17 @@ def run_ours(args, ws, rank, local):
     dt0 = 1.0 / sum(1.0 / x for x in ndt if x < 1e99)
     stream = torch.cuda.ExternalStream(dev.stream_ptr)
     zones = n1 * n2 * n3
+    mlp_info = train_guess(dev, Pd, dt0, prec, args) if guess == HARM_GUESS_MLP else None
 
-    def timed(precision, P, K, W):
+    def timed(precision, gs, P, K, W):
         dt = dt0
-        dt, _ = dev.step_ch(P, dt, precision=precision, nsteps=W, stats=False)
+        dt, _ = dev.step_ch(P, dt, precision=precision, guess=gs, nsteps=W, stats=False)
         barrier(ws)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         l0 = dev.launches
         e0.record(stream)
-        dt, st = dev.step_ch(P, dt, precision=precision, nsteps=K, stats=True)
+        dt, st = dev.step_ch(P, dt, precision=precision, guess=gs, nsteps=K, stats=True)
         e1.record(stream)
         torch.cuda.synchronize()
         barrier(ws)
@@ -245,37 +295,50 @@ def run_ours(args, ws, rank, local):
 
     # plain FP64 path on the same grid
     Pf = Pd.clone()
-    ms64, st64, _ = timed(HARM_PREC_FP64, Pf, max(1, args.steps // 2), args.warmup)
+    k64 = max(1, args.steps // 2)
+    ms64, st64, _ = timed(HARM_PREC_FP64, HARM_GUESS_PREV, Pf, k64, args.warmup)
     del Pf
+    # the headline precision with the plain guess
+    if guess == HARM_GUESS_MLP:
+        Pp = Pd.clone()
+        msp, stp, _ = timed(prec, HARM_GUESS_PREV, Pp, args.steps, args.warmup)
+        del Pp
     # headline path, with clocks sampled during the timed region
     stop, clines = threading.Event(), []
     th = threading.Thread(target=clock_sampler, args=(stop, clines, local), daemon=True)
     th.start()
     Pm = Pd.clone()
-    ms, st, launches = timed(prec, Pm, args.steps, args.warmup)
+    ms, st, launches = timed(prec, guess, Pm, args.steps, args.warmup)
     stop.set()
     th.join(timeout=5)
     ms = max_over_ranks(ms, ws)
     ms64 = max_over_ranks(ms64, ws)
     value = ws * zones * args.steps / (ms * 1e-3)
-    value64 = ws * zones * max(1, args.steps // 2) / (ms64 * 1e-3)
+    value64 = ws * zones * k64 / (ms64 * 1e-3)
+    if guess == HARM_GUESS_MLP:
+        msp = max_over_ranks(msp, ws)
+        value_prev = ws * zones * args.steps / (msp * 1e-3)
     # accuracy of the headline path against the FP64 path after the same steps
     Pa, Pb = Pd.clone(), Pd.clone()
     dev.step_ch(Pa, dt0, precision=HARM_PREC_FP64, nsteps=args.err_steps, stats=False)
-    dev.step_ch(Pb, dt0, precision=prec, nsteps=args.err_steps, stats=False)
+    dev.step_ch(Pb, dt0, precision=prec, guess=guess, nsteps=args.err_steps, stats=False)
     act = (slice(None),) + g.active
     a, b = Pa.cpu().numpy()[act], Pb.cpu().numpy()[act]
     l1 = {nm: float(np.abs(a[pl] - b[pl]).mean() / max(np.abs(a[pl]).mean(), 1e-300))
           for nm, pl in (("rho", 0), ("u", 1), ("B1", 5), ("B2", 6), ("B3", 7))}
+    linf = {nm: float(np.abs(a[pl] - b[pl]).max() / max(np.abs(a[pl]).max(), 1e-300))
+            for nm, pl in (("rho", 0), ("u", 1), ("B1", 5), ("B2", 6), ("B3", 7))}
     del Pa, Pb
-    # stage times and roofline of the dominant kernel (update + inversion)
-    stages = dev.time_stages(Pm, dt0, precision=prec, reps=3)
+    # stage times and roofline of the dominant kernels
+    stages = dev.time_stages(Pm, dt0, precision=prec, guess=guess, reps=3)
     peaks = measured_peaks()
+    flux_bytes = flux_bytes_per_cell(n3, prec) * zones
+    ach_flux = flux_bytes / (stages["flux"] * 1e-3) / 1e9
     upd_bytes = update_kernel_bytes_per_cell(n3, prec) * zones
     ach = upd_bytes / (stages["update_invert"] * 1e-3) / 1e9
     # end to end through the host-buffer entry point: H2D of P, step, D2H of P every step
     Ph = torch.from_numpy(P0.copy()).pin_memory()
-    dev.step_ch_host(Ph.numpy(), dt0, precision=prec)
+    dev.step_ch_host(Ph.numpy(), dt0, precision=prec, guess=guess)
     torch.cuda.synchronize()
     ke = max(2, args.steps // 4)
     t0 = time.perf_counter()
@@ -283,7 +346,7 @@ def run_ours(args, ws, rank, local):
     e0.record(stream)
     dte = dt0
     for _ in range(ke):
-        dte, _ = dev.step_ch_host(Ph.numpy(), dte, precision=prec)
+        dte, _ = dev.step_ch_host(Ph.numpy(), dte, precision=prec, guess=guess)
     e1.record(stream)
     torch.cuda.synchronize()
     wall_e2e = time.perf_counter() - t0
@@ -295,26 +358,36 @@ def run_ours(args, ws, rank, local):
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(args, lim)
     if rank == 0:
+        ninv = max(st["cells_inverted"], 1.0)
         line = {
             "metric": METRIC, "value": value, "unit": "zone-updates/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 flux / f64 update+inversion" if prec == HARM_PREC_MIXED else "f64",
             "data": "synthetic (seeded Fishbone-Moncrief torus, host-built)",
-            "config": {"workload": f"{args.config}_{LIMNAME[lim]}_hll_fluxct_{args.precision}",
+            "config": {"workload": f"{args.config}_{LIMNAME[lim]}_hll_fluxct_{args.precision}_{args.guess}",
                        "grid": [n1, n2, n3], "reconstruction": LIMNAME[lim], "riemann": "hll", "ct": "toth",
                        "precision": args.precision, "guess": args.guess,
                        "l2": "inputs larger than L2 (P is %.0f MB)" % (pbytes / 1e6),
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
             "fp64_value": value64, "speedup_vs_fp64": value / value64,
-            "l1_rel_err_vs_fp64": l1, "l1_steps": args.err_steps,
-            "newton_iters_per_cell": st["newton_iters"] / max(st["cells_inverted"], 1.0),
+            "plain_guess_value": value_prev if guess == HARM_GUESS_MLP else value,
+            "l1_rel_err_vs_fp64": l1, "linf_rel_err_vs_fp64": linf, "err_steps": args.err_steps,
+            "newton_iters_per_cell": st["newton_iters"] / ninv,
+            "newton_iters_per_cell_plain_guess": (stp if guess == HARM_GUESS_MLP else st)["newton_iters"]
+            / max((stp if guess == HARM_GUESS_MLP else st)["cells_inverted"], 1.0),
             "newton_iters_per_cell_fp64": st64["newton_iters"] / max(st64["cells_inverted"], 1.0),
-            "inversion_failures": st["inversion_failures"], "mlp_fallbacks": st["mlp_fallbacks"],
+            "mlp_fallback_rate": st["mlp_fallbacks"] / ninv, "inversion_failures": st["inversion_failures"],
+            "learned_guess": mlp_info,
             "stage_ms": stages,
-            "roofline": {"bound": "hbm", "kernel": "k_update (update + FP64 inversion)",
-                         "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": ach / peaks["hbm_gbs"],
-                         "peak_src": peaks["src"], "traffic": None,
-                         "algorithmic_bytes_per_cell": update_kernel_bytes_per_cell(n3, prec)},
+            "roofline": {"bound": "hbm", "kernel": "k_fluxt (WENO5/PPM/MC reconstruction + HLL, 3 directions)",
+                         "achieved": ach_flux, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": ach_flux / peaks["hbm_gbs"], "peak_src": peaks["src"],
+                         "traffic": FLUX_TRAFFIC.get((args.config, lim, args.precision)),
+                         "algorithmic_bytes_per_cell": flux_bytes_per_cell(n3, prec)},
+            "roofline_update_invert": {"bound": "hbm", "kernel": "k_conserved + k_invert(_mlp) + k_invert_rare",
+                                       "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                                       "frac": ach / peaks["hbm_gbs"],
+                                       "algorithmic_bytes_per_cell": update_kernel_bytes_per_cell(n3, prec)},
             "step_roofline": {"bytes_per_zone_update": bytes_per_zone_update(n3),
                               "achieved_gbs": value / ws * bytes_per_zone_update(n3) / 1e9,
                               "frac": value / ws * bytes_per_zone_update(n3) / 1e9 / peaks["hbm_gbs"]},
@@ -337,7 +410,11 @@ def main():
     ap.add_argument("--config", default="torus3d_384x192x128", choices=list(CONFIGS))
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--lim", default="config", choices=["config", "mc", "ppm", "weno5"])
-    ap.add_argument("--guess", default="prev", choices=["prev", "mlp"])
+    ap.add_argument("--guess", default="mlp", choices=["prev", "mlp"])
+    ap.add_argument("--train-steps", type=int, default=4, help="plain steps whose (U,P) pairs train the guess")
+    ap.add_argument("--train-pairs", type=int, default=2000000, help="pairs dumped over those steps")
+    ap.add_argument("--train-iters", type=int, default=15000, help="Adam steps of the training")
+    ap.add_argument("--start-bias", type=float, default=0.0, help="added to the predicted log(W'/D)")
     ap.add_argument("--seed", type=int, default=12345)
     ap.add_argument("--err-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)

@@ -259,16 +259,23 @@ __device__ __forceinline__ void para4_cell(const T* y, T& lout, T& rout) {
 // WENO3 lower-order weights, weight-ratio stencil reduction (compute_weights_ratios :2316,
 // choose_weno_order :2442), edge values (eno_cvt :884).  Sums use the symmetric pairwise
 // order of get_sum_of_elements.  The SMONO indicator is taken as 0 (pure WENO output).
+// eps: WENO_EPSILON = (500 DBL_EPSILON)^2 (desensitising and weight ratios), the same value
+// in both arithmetic types so that the FP32 reconstruction is the FP64 algorithm up to
+// rounding; weps: the epsilon of 1/(beta+eps)^2, which in FP32 is raised to 1e-18 so that its
+// square stays a normal number (it only acts where a normalised beta is below ~1e-18, far
+// under FP32 resolution); tiny: the smallest normal number (divisions by zero sums).
 template <typename T>
 struct WenoEps;
 template <>
 struct WenoEps<double> {
   static constexpr double eps = (500.0 * 2.220446049250313e-16) * (500.0 * 2.220446049250313e-16);
+  static constexpr double weps = eps;
   static constexpr double tiny = 2.2250738585072014e-308;  // DBL_MIN
 };
 template <>
 struct WenoEps<float> {
-  static constexpr float eps = (500.0f * 1.1920929e-07f) * (500.0f * 1.1920929e-07f);
+  static constexpr float eps = (float)((500.0 * 2.220446049250313e-16) * (500.0 * 2.220446049250313e-16));
+  static constexpr float weps = 1e-18f;
   static constexpr float tiny = 1.17549435e-38f;  // FLT_MIN
 };
 
@@ -334,7 +341,7 @@ __device__ __forceinline__ void weno5_unopt(const T* u, T* w) {
   for (int s = 0; s < 3; s++) b[s] = wdiv<T>(b[s], sb + WenoEps<T>::tiny);
 #pragma unroll
   for (int s = 0; s < 3; s++) {
-    T t = b[s] + WenoEps<T>::eps;
+    T t = b[s] + WenoEps<T>::weps;
     t *= t;
     w[s] = wdiv<T>(T(1), t);
   }
@@ -364,7 +371,7 @@ __device__ __forceinline__ void weno3_unopt(const T* u, T* w) {
   b[1] = wdiv<T>(b[1], sb + WenoEps<T>::tiny);
 #pragma unroll
   for (int s = 0; s < 2; s++) {
-    T t = b[s] + WenoEps<T>::eps;
+    T t = b[s] + WenoEps<T>::weps;
     t *= t;
     w[s] = wdiv<T>(T(1), t);
   }
