@@ -94,7 +94,7 @@ extern "C" int harm_b200_destroy(harm_ctx* c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   void* ptrs[] = {c->d_geom, c->d_geomf, c->d_conn, c->d_aux, c->d_F[0], c->d_F[1], c->d_F[2], c->d_Ff[0], c->d_Ff[1],
-                  c->d_Ff[2], c->d_emf, c->d_emff, c->d_pk, c->d_U, c->d_rare, c->d_pflag, c->d_fixrec, c->d_scal, c->d_Pdev, c->d_mlp,
+                  c->d_Ff[2], c->d_emf, c->d_emff, c->d_pk, c->d_U, c->d_rare, c->d_pflag, c->d_fixrec, c->d_scal, c->d_Pdev, c->d_mlp, c->d_wpg,
                   c->d_mlp_master, c->d_mlp_adam, c->d_mlp_work};
   for (void* p : ptrs)
     if (p) cudaFree(p);

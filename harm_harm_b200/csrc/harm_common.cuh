@@ -690,15 +690,19 @@ __global__ void __launch_bounds__(256, 2) k_conserved(Dims d, Phys ph, StepCoef 
 // and finished by k_invert_rare, so that the rarely taken branches (cold inversion, the
 // floor re-inversion) neither diverge warps nor enlarge the register footprint here.
 // PATH distinguishes the instantiation of each arithmetic path's translation unit.
-template <int PATH>
+// GUESS: the Newton iteration starts from wpg[t] (the learned start, k_mlp_guess) where it is
+// positive; a cell whose learned start does not converge starts again from the
+// previous-state W', exactly as without GUESS (counted in stats[2]).
+template <int PATH, bool GUESS = false>
 __global__ void __launch_bounds__(256, 2) k_invert(Dims d, Phys ph, const double* __restrict__ U,
                                                    const double* __restrict__ pb, double* __restrict__ pf,
                                                    int8_t* __restrict__ pflag, const double* __restrict__ geom,
                                                    const double* __restrict__ aux, unsigned int* __restrict__ rare,
-                                                   unsigned int* __restrict__ nrare, double* __restrict__ stats) {
+                                                   unsigned int* __restrict__ nrare, double* __restrict__ stats,
+                                                   const double* __restrict__ wpg = nullptr) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   long long ncell = (long long)d.n1 * d.n2 * d.n3;
-  double iters_d = 0.0;
+  double iters_d = 0.0, fb_d = 0.0;
   if (t < ncell) {
     int i = (int)(t % d.n1);
     long long r = t / d.n1;
@@ -712,7 +716,18 @@ __global__ void __launch_bounds__(256, 2) k_invert(Dims d, Phys ph, const double
     for (int p = 0; p < NPR; p++) { Ugf[p] = U[(size_t)p * d.cells + id] * g.igdet; pr[p] = pb[(size_t)p * d.cells + id]; }
     int8_t flag = 0;
     int it = 0;
-    utoprim_jon(false, Ugf, g, flag, pr, ph.gam, ph.gammafail, it, false, 0.0);
+    if (GUESS) {
+      JonSetup s;
+      jon_prepare(false, Ugf, g, pr, ph.gam, ph.gammafail, s);
+      const double w = wpg[t];
+      jon_solve(s, (w > 0.0) ? w : s.Wp_prev, pr, flag, it);
+      if (flag != 0 && w > 0.0) {  // the learned start did not converge: the plain start
+        fb_d = 1.0;
+        jon_solve(s, s.Wp_prev, pr, flag, it);
+      }
+    } else {
+      utoprim_jon(false, Ugf, g, flag, pr, ph.gam, ph.gammafail, it, false, 0.0);
+    }
     iters_d = (double)it;
     bool defer = (flag != 0);
     if (!defer) {
@@ -731,86 +746,56 @@ __global__ void __launch_bounds__(256, 2) k_invert(Dims d, Phys ph, const double
 #pragma unroll
     for (int p = 0; p < NPR; p++) pf[(size_t)p * d.cells + id] = pr[p];
   }
-  if (stats) warp_add_atomic(iters_d, stats + 0);
+  if (stats) {
+    warp_add_atomic(iters_d, stats + 0);
+    if (GUESS) warp_add_atomic(fb_d, stats + 2);
+  }
 }
 
-// Inversion with the learned guess: the same work as k_invert, except that the Newton
-// iteration starts from the network's W' (evaluated per warp on the tensor cores between
-// the setup and the solve) and, when that start does not converge, starts again from the
-// previous-state W' exactly as k_invert does (counted in stats[2]).  A persistent grid
-// (two blocks per SM) walks the cells in tiles of 256, so the packed network is copied to
-// shared memory once per block.
+// The learned start of the inversion, one kernel before k_invert: per cell the
+// alpha-scaled invariants of U (compute_setup_quantities), the features, the network on the
+// tensor cores (per warp, mma.sync BF16 with FP32 accumulation) and W' = D exp(log(W'/D) +
+// start_bias) into wpg (-1 where the prediction is not a positive finite number).  A
+// persistent grid walks the cells in tiles of 256, so the packed network is copied to shared
+// memory once per block.  Kept apart from the Newton iteration so that each kernel runs at
+// its own occupancy (this one needs few registers, the FP64 iteration many).
 template <int PATH>
-__global__ void __launch_bounds__(256, 2) k_invert_mlp(Dims d, Phys ph, const double* __restrict__ U,
-                                                       const double* __restrict__ pb, double* __restrict__ pf,
-                                                       int8_t* __restrict__ pflag, const double* __restrict__ geom,
-                                                       const double* __restrict__ aux, unsigned int* __restrict__ rare,
-                                                       unsigned int* __restrict__ nrare, double* __restrict__ stats,
-                                                       const MlpPacked* __restrict__ mlp) {
+__global__ void __launch_bounds__(256, 3) k_mlp_guess(Dims d, const double* __restrict__ U,
+                                                      const double* __restrict__ geom, double* __restrict__ wpg,
+                                                      const MlpPacked* __restrict__ mlp) {
   __shared__ MlpPacked sm;
   __shared__ MlpWarpScratch wsc[8];
   mlp_load_packed(sm, mlp);
   __syncthreads();
   const long long ncell = (long long)d.n1 * d.n2 * d.n3;
-  double iters_d = 0.0, fb_d = 0.0;
   for (long long base = (long long)blockIdx.x * 256; base < ncell; base += (long long)gridDim.x * 256) {
     const long long t = base + threadIdx.x;
     const bool valid = t < ncell;
-    size_t id = 0, c2 = 0;
-    JonSetup s;
-    double pr[NPR];
     float f[MLP_IN];
+    double D = 0.0;
     if (valid) {
       int i = (int)(t % d.n1);
       long long r = t / d.n1;
       int j = (int)(r % d.n2), k = (int)(r / d.n2);
       int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
-      id = cidx(d, ii, jj, kk);
-      c2 = (size_t)jj * d.n1e + ii;
+      const size_t id = cidx(d, ii, jj, kk), c2 = (size_t)jj * d.n1e + ii;
       Geo<double> g;
       load_geo<double, double>(geom, d.plane, c2, g);
-      double Ugf[NPR];
+      double Ua[NPR];
 #pragma unroll
-      for (int p = 0; p < NPR; p++) { Ugf[p] = U[(size_t)p * d.cells + id] * g.igdet; pr[p] = pb[(size_t)p * d.cells + id]; }
-      jon_prepare(false, Ugf, g, pr, ph.gam, ph.gammafail, s);
-      mlp_features(s.c, g, f);
+      for (int p = 0; p < NPR; p++) Ua[p] = g.alpha * (U[(size_t)p * d.cells + id] * g.igdet);
+      InvC c;
+      double Qtcon[4], Bcon[4];
+      inv_invariants(Ua, g, c, Qtcon, Bcon);
+      mlp_features(c, g, f);
+      D = c.D;
     }
     float y[MLP_OUT];
     mlp_warp_eval(sm, wsc[threadIdx.x >> 5], f, valid, y);
     if (valid) {
-      int8_t flag = 0;
-      int it = 0;
-      jon_solve(s, mlp_wp_guess(y[0], sm.start_bias, s), pr, flag, it);
-      if (flag != 0) {  // the learned start did not converge: the plain start
-        fb_d += 1.0;
-        jon_solve(s, s.Wp_prev, pr, flag, it);
-      }
-      iters_d += (double)it;
-      bool defer = (flag != 0);
-      if (!defer) {
-        double rhofl = __ldg(aux + (size_t)HARM_AUX_RHOFLOOR * d.plane + c2);
-        double ufl = __ldg(aux + (size_t)HARM_AUX_UFLOOR * d.plane + c2);
-        rhofl = (rhofl < kSMALL) ? kSMALL : rhofl;
-        ufl = (ufl < kSMALL) ? kSMALL : ufl;
-        defer = (rhofl > pr[HARM_RHO]) || (ufl > pr[HARM_UU]);
-        if (!defer) {
-          Geo<double> g;
-          load_geo<double, double>(geom, d.plane, c2, g);
-          limit_gamma<double>(ph.gammamax, pr, g);
-        }
-      }
-      if (defer) {
-        unsigned int slot = atomicAdd(nrare, 1u);
-        rare[slot] = (unsigned int)t;
-      }
-      pflag[id] = flag;
-#pragma unroll
-      for (int p = 0; p < NPR; p++) pf[(size_t)p * d.cells + id] = pr[p];
+      const double wp = D * exp((double)y[0] + (double)sm.start_bias);
+      wpg[t] = (wp > 0.0 && isfinite(wp)) ? wp : -1.0;
     }
-  }
-  if (stats) {
-    warp_add_atomic(iters_d, stats + 0);
-    warp_add_atomic(fb_d, stats + 2);
   }
 }
 

@@ -37,6 +37,7 @@ struct harm_ctx {
   double* d_Pdev;   // device state used by the host-buffer entry point
   // learned guess
   float* d_mlp;        // inference parameters (BF16 packed as float words) + normalisation
+  double* d_wpg;       // learned starting W' of each active cell (k_mlp_guess)
   float* d_mlp_master; // FP32 master parameters
   float* d_mlp_adam;   // Adam moments
   float* d_mlp_work;   // training workspace

@@ -148,8 +148,9 @@ static __device__ int newton(int8_t& flag, double& xio, const InvC& c, int& lntr
 
 // Setup scalars and the previous-state guess; returns retval contribution of the guess.
 // U and prim are alpha-scaled as in Utoprim_jon_nonrelcompat_inputnorestmass.
-static __device__ int inv_setup(const double* U, const Geo<double>& g, const double* prim, InvC& c, double Qtcon[4],
-                         double Bcon[4], double& Wp_last, int8_t& flag) {
+// compute_setup_quantities: the alpha-scaled invariants D, B^2, (Q.B)^2, Qt^2, Q.n' of U
+static __device__ __forceinline__ void inv_invariants(const double* U, const Geo<double>& g, InvC& c, double Qtcon[4],
+                                                      double Bcon[4]) {
   c.D = U[HARM_RHO];
   Bcon[0] = 0.;
   Bcon[1] = U[HARM_B1]; Bcon[2] = U[HARM_B2]; Bcon[3] = U[HARM_B3];
@@ -178,6 +179,11 @@ static __device__ int inv_setup(const double* U, const Geo<double>& g, const dou
   double alpha = g.alpha, alphasq = alpha * alpha;
   double Dfactor = (-g.gcovpert_tt + alphasq * g.betasqoalphasq) / (alphasq + alpha);
   c.Qdotnp = Qconp[0] * ncov[0] + c.D * Dfactor;
+}
+
+static __device__ int inv_setup(const double* U, const Geo<double>& g, const double* prim, InvC& c, double Qtcon[4],
+                         double Bcon[4], double& Wp_last, int8_t& flag) {
+  inv_invariants(U, g, c, Qtcon, Bcon);
   // set_guess_Wp
   double utsq = 0.;
 #pragma unroll

@@ -448,6 +448,9 @@ extern "C" int harm_b200_mlp_set(harm_ctx* c, const float* d_params, const float
   if (!c->d_mlp) {
     CK(cudaMalloc(&c->d_mlp, sizeof(MlpPacked)));
   }
+  if (!c->d_wpg) {
+    CK(cudaMalloc(&c->d_wpg, (size_t)c->g.n1 * c->g.n2 * c->g.n3 * sizeof(double)));
+  }
   k_mlp_pack<<<nblk(MLP_TILES * 32), 256, 0, c->stream>>>(d_params, d_norm, (float)start_bias,
                                                          reinterpret_cast<MlpPacked*>(c->d_mlp));
   c->launches++;

@@ -309,8 +309,11 @@ int hp_update_fp64(harm_ctx* c, const StepCoef& sc, const double* pi, const doub
                                                           c->d_F[2], c->d_emf, c->d_geom, c->d_conn, c->d_U);
   CK(cudaMemsetAsync(c->d_nrare, 0, sizeof(unsigned int), c->stream));
   if (sc.guess == HARM_GUESS_MLP) {
-    k_invert_mlp<0><<<2 * 148, 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
-                                                     c->d_nrare, stats, reinterpret_cast<const MlpPacked*>(c->d_mlp));
+    k_mlp_guess<0><<<3 * 148, 256, 0, c->stream>>>(d, c->d_U, c->d_geom, c->d_wpg,
+                                                    reinterpret_cast<const MlpPacked*>(c->d_mlp));
+    k_invert<0, true><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux,
+                                                          c->d_rare, c->d_nrare, stats, c->d_wpg);
+    c->launches++;
   } else {
     k_invert<0><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
                                                     c->d_nrare, stats);

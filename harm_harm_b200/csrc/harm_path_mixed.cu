@@ -40,8 +40,11 @@ int hp_update_mixed(harm_ctx* c, const StepCoef& sc, const double* pi, const dou
                                                          c->d_Ff[2], c->d_emff, c->d_geom, c->d_conn, c->d_U);
   CK(cudaMemsetAsync(c->d_nrare, 0, sizeof(unsigned int), c->stream));
   if (sc.guess == HARM_GUESS_MLP) {
-    k_invert_mlp<1><<<2 * 148, 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
-                                                     c->d_nrare, stats, reinterpret_cast<const MlpPacked*>(c->d_mlp));
+    k_mlp_guess<1><<<3 * 148, 256, 0, c->stream>>>(d, c->d_U, c->d_geom, c->d_wpg,
+                                                    reinterpret_cast<const MlpPacked*>(c->d_mlp));
+    k_invert<1, true><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux,
+                                                          c->d_rare, c->d_nrare, stats, c->d_wpg);
+    c->launches++;
   } else {
     k_invert<1><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
                                                     c->d_nrare, stats);
