@@ -68,8 +68,15 @@ def device_sources() -> list[str]:
 
 def device_flags(src: str) -> list[str]:
     """Per-file flags: the FP64 path is compiled without FMA contraction so that its FP64
-    operations are the IEEE operations of the C restatement, in the same order."""
-    return ["-fmad=false"] if src.endswith("_fp64.cu") else []
+    operations are the IEEE operations of the C restatement, in the same order; the mixed
+    path uses the fast FP32 division and square root."""
+    if src.endswith("_fp64.cu"):
+        return ["-fmad=false"]
+    if src.endswith("_mixed.cu"):
+        # FP32 flux path: fast single-precision division and square root (a few ulp); the
+        # FP64 update and inversion in the same file are not affected
+        return ["-prec-div=false", "-prec-sqrt=false"]
+    return []
 
 
 def build_device(force: bool = False, extra: list[str] | None = None, out_dir: str | None = None) -> str:

@@ -306,13 +306,44 @@ __device__ __forceinline__ float wdiv<float>(float a, float b) {
   return __fdividef(a, b);
 }
 
+// Division by a compile-time constant: FP64 divides; FP32 multiplies by the folded reciprocal.
+template <typename T>
+__device__ __forceinline__ T wdivk(T a, T b) {
+  return a / b;
+}
+template <>
+__device__ __forceinline__ float wdivk<float>(float a, float b) {
+  return a * (1.0f / b);
+}
+
+// Several values over one denominator: FP64 divides each (the oracle's operations); FP32
+// multiplies by one fast reciprocal.
+template <typename T>
+struct WScale {
+  T d;
+  __device__ __forceinline__ explicit WScale(T den) : d(den) {}
+  __device__ __forceinline__ T operator()(T a) const { return a / d; }
+};
+template <>
+struct WScale<float> {
+  float r;
+  __device__ __forceinline__ explicit WScale(float den) {
+#ifdef __CUDA_ARCH__
+    r = __fdividef(1.0f, den);
+#else
+    r = 1.0f / den;  // host pass only parses this; the kernels use the line above
+#endif
+  }
+  __device__ __forceinline__ float operator()(float a) const { return a * r; }
+};
+
 template <typename T>
 __device__ __forceinline__ T limit_weight(int order, T w) {
   const T avg = T(1) / T(order), w1 = T(0.2) * avg, w2 = (T(1) - T(0.2)) * avg, w3 = (T(1) + T(0.2)) * avg, w4 = T(1);
   if (w < w1) return T(0);
-  if (w < w2) return wdiv<T>(avg * (w - w1), w2 - w1);
+  if (w < w2) return wdivk<T>(avg * (w - w1), w2 - w1);
   if (w < w3) return avg;
-  return wdiv<T>((w - w3) * (w4 - avg), w4 - w3) + avg;
+  return wdivk<T>((w - w3) * (w4 - avg), w4 - w3) + avg;
 }
 
 // unoptimised (limited, normalised) weights of the three 3-point stencils of the cell at u
@@ -337,8 +368,9 @@ __device__ __forceinline__ void weno5_unopt(const T* u, T* w) {
 #pragma unroll
   for (int s = 0; s < 3; s++) b[s] += ee;
   T sb = symsum3(b[0], b[1], b[2]);
+  const WScale<T> nb(sb + WenoEps<T>::tiny);
 #pragma unroll
-  for (int s = 0; s < 3; s++) b[s] = wdiv<T>(b[s], sb + WenoEps<T>::tiny);
+  for (int s = 0; s < 3; s++) b[s] = nb(b[s]);
 #pragma unroll
   for (int s = 0; s < 3; s++) {
     T t = b[s] + WenoEps<T>::weps;
@@ -346,13 +378,15 @@ __device__ __forceinline__ void weno5_unopt(const T* u, T* w) {
     w[s] = wdiv<T>(T(1), t);
   }
   T sw = symsum3(w[0], w[1], w[2]);
+  const WScale<T> n1(sw + T(0));
 #pragma unroll
-  for (int s = 0; s < 3; s++) w[s] = wdiv<T>(w[s], sw + T(0));
+  for (int s = 0; s < 3; s++) w[s] = n1(w[s]);
 #pragma unroll
   for (int s = 0; s < 3; s++) w[s] = limit_weight<T>(3, w[s]);
   sw = symsum3(w[0], w[1], w[2]);
+  const WScale<T> n2(sw + T(0));
 #pragma unroll
-  for (int s = 0; s < 3; s++) w[s] = wdiv<T>(w[s], sw + T(0));
+  for (int s = 0; s < 3; s++) w[s] = n2(w[s]);
 }
 
 // the same for the two 2-point stencils (WENO3)
@@ -367,8 +401,9 @@ __device__ __forceinline__ void weno3_unopt(const T* u, T* w) {
   b[0] += ee;
   b[1] += ee;
   T sb = symsum2(b[0], b[1]);
-  b[0] = wdiv<T>(b[0], sb + WenoEps<T>::tiny);
-  b[1] = wdiv<T>(b[1], sb + WenoEps<T>::tiny);
+  const WScale<T> nb(sb + WenoEps<T>::tiny);
+  b[0] = nb(b[0]);
+  b[1] = nb(b[1]);
 #pragma unroll
   for (int s = 0; s < 2; s++) {
     T t = b[s] + WenoEps<T>::weps;
@@ -376,13 +411,15 @@ __device__ __forceinline__ void weno3_unopt(const T* u, T* w) {
     w[s] = wdiv<T>(T(1), t);
   }
   T sw = symsum2(w[0], w[1]);
-  w[0] = wdiv<T>(w[0], sw + T(0));
-  w[1] = wdiv<T>(w[1], sw + T(0));
+  const WScale<T> n1(sw + T(0));
+  w[0] = n1(w[0]);
+  w[1] = n1(w[1]);
   w[0] = limit_weight<T>(2, w[0]);
   w[1] = limit_weight<T>(2, w[1]);
   sw = symsum2(w[0], w[1]);
-  w[0] = wdiv<T>(w[0], sw + T(0));
-  w[1] = wdiv<T>(w[1], sw + T(0));
+  const WScale<T> n2(sw + T(0));
+  w[0] = n2(w[0]);
+  w[1] = n2(w[1]);
 }
 
 // left and right edge values of the cell at u, given its neighbours' unoptimised weights
@@ -393,16 +430,17 @@ __device__ __forceinline__ void weno5_edges(const T* u, const T* w, const T* wm,
   T rl = wdiv<T>(w[2] + E, wm[0] + E);
   T rr = wdiv<T>(w[0] + E, wp[2] + E);
   T ratio = fmin(rl, rr);
-  T f = wdiv<T>(ratio - T(1.3), T(1.6) - T(1.3));
+  T f = wdivk<T>(ratio - T(1.3), T(1.6) - T(1.3));
   f = fmax(T(0), fmin(f, T(1)));
   // optimal face weights (order 3)
   T wl[3] = {w[0] * T(1. / 16.), w[1] * T(5. / 8.), w[2] * T(5. / 16.)};
   T wr[3] = {w[0] * T(5. / 16.), w[1] * T(5. / 8.), w[2] * T(1. / 16.)};
   T sl = symsum3(wl[0], wl[1], wl[2]), sr = symsum3(wr[0], wr[1], wr[2]);
+  const WScale<T> nl(sl + WenoEps<T>::tiny), nr(sr + WenoEps<T>::tiny);
 #pragma unroll
   for (int s = 0; s < 3; s++) {
-    wl[s] = wdiv<T>(wl[s], sl + WenoEps<T>::tiny);
-    wr[s] = wdiv<T>(wr[s], sr + WenoEps<T>::tiny);
+    wl[s] = nl(wl[s]);
+    wr[s] = nr(wr[s]);
   }
   const bool two = (T(0) < f);
   if (two) {
@@ -434,10 +472,11 @@ __device__ __forceinline__ void weno5_edges(const T* u, const T* w, const T* wm,
     T l3[2] = {w3[0] * T(1. / 4.), w3[1] * T(3. / 4.)};
     T r3[2] = {w3[0] * T(3. / 4.), w3[1] * T(1. / 4.)};
     T sl3 = symsum2(l3[0], l3[1]), sr3 = symsum2(r3[0], r3[1]);
+    const WScale<T> nl3(sl3 + WenoEps<T>::tiny), nr3(sr3 + WenoEps<T>::tiny);
 #pragma unroll
     for (int s = 0; s < 2; s++) {
-      l3[s] = wdiv<T>(l3[s], sl3 + WenoEps<T>::tiny);
-      r3[s] = wdiv<T>(r3[s], sr3 + WenoEps<T>::tiny);
+      l3[s] = nl3(l3[s]);
+      r3[s] = nr3(r3[s]);
       l3[s] *= f;
       r3[s] *= f;
     }
