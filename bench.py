@@ -67,9 +67,10 @@ def flux_bytes_per_cell(n3: int, precision: int) -> float:
     return 3 * (64 + 8 * w + 28 * w / n3)
 
 
-# DRAM traffic per flux launch (bytes read + written, ncu dram__bytes_*.sum) per active
-# cell, from the captures summarised in profiles/, scaled to the workload's cell count
-FLUX_TRAFFIC = {}
+# DRAM traffic of the flux stage (three k_fluxt launches; ncu dram__bytes_read.sum +
+# dram__bytes_write.sum) per active cell, measured on the 192x96x64 torus (profiles/
+# k_fluxt_weno5_f32_torus3d_192x96x64.md) and scaled to a workload by its cell count
+FLUX_TRAFFIC_PER_CELL = {("weno5", "mixed"): 293.6}
 
 
 def clock_sampler(stop: threading.Event, out: list, dev: int):
@@ -382,7 +383,9 @@ def run_ours(args, ws, rank, local):
             "roofline": {"bound": "hbm", "kernel": "k_fluxt (WENO5/PPM/MC reconstruction + HLL, 3 directions)",
                          "achieved": ach_flux, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": ach_flux / peaks["hbm_gbs"], "peak_src": peaks["src"],
-                         "traffic": FLUX_TRAFFIC.get((args.config, lim, args.precision)),
+                         "traffic": (FLUX_TRAFFIC_PER_CELL[(LIMNAME[lim], args.precision)] * zones
+                                     if (LIMNAME[lim], args.precision) in FLUX_TRAFFIC_PER_CELL else None),
+                         "unit_of_launch": "one flux stage (three k_fluxt launches, all directions)",
                          "algorithmic_bytes_per_cell": flux_bytes_per_cell(n3, prec)},
             "roofline_update_invert": {"bound": "hbm", "kernel": "k_conserved + k_invert(_mlp) + k_invert_rare",
                                        "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
