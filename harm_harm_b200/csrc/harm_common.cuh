@@ -91,6 +91,31 @@ struct FixRec {
   double v[5];
 };
 
+// Cell tiles of the per-cell kernels: a block of 256 threads covers TI consecutive i times TK
+// consecutive k at one j (TK = 16 in 3-D, 1 in 2-D), so the per-(i,j) metric and connection
+// records a block reads serve TK cells each and come from L1 instead of L2; rows of TI
+// consecutive i keep the state loads coalesced.
+struct CellTile {
+  int lti, ltk;  // log2 TI, log2 TK
+};
+static inline CellTile cell_tile(int n3) {
+  CellTile ct;
+  ct.ltk = 0;
+  while (ct.ltk < 4 && (2 << ct.ltk) <= n3) ct.ltk++;
+  ct.lti = 8 - ct.ltk;
+  return ct;
+}
+static inline dim3 cell_grid(int n1, int n2, int n3, CellTile ct) {
+  return dim3((n1 + (1 << ct.lti) - 1) >> ct.lti, n2, (n3 + (1 << ct.ltk) - 1) >> ct.ltk);
+}
+// this thread's active cell (i, j, k) in tile (tx, ty, tz); false past the grid's edge
+__device__ __forceinline__ bool tile_cell(int n1, int n3, CellTile ct, int tx, int ty, int tz, int& i, int& j, int& k) {
+  i = (tx << ct.lti) + (int)(threadIdx.x & ((1u << ct.lti) - 1));
+  k = (tz << ct.ltk) + (int)(threadIdx.x >> ct.lti);
+  j = ty;
+  return i < n1 && k < n3;
+}
+
 static inline unsigned int nblk(long long n, int bs = 256) { return (unsigned int)((n + bs - 1) / bs); }
 
 // ------------------------------------------------------------------ flux kernel
@@ -644,19 +669,23 @@ __device__ __forceinline__ int fixup1zone(double* pr, const Geo<double>& g, doub
 
 // Conserved update of one substep: U_i = primtoU(p_i), flux divergence (field fluxes from
 // the EMFs), connection source of p_b, RK combination; U (UEVOLVE) to global memory.
+// minimum resident blocks per SM the FP64 kernels are compiled for (register budget)
+#ifndef HARM_CONSERVED_BLOCKS
+#define HARM_CONSERVED_BLOCKS 2
+#endif
+#ifndef HARM_INVERT_BLOCKS
+#define HARM_INVERT_BLOCKS 3
+#endif
+
 template <typename T>
-__global__ void __launch_bounds__(256, 2) k_conserved(Dims d, Phys ph, StepCoef sc, const double* __restrict__ dtp,
+__global__ void __launch_bounds__(256, HARM_CONSERVED_BLOCKS) k_conserved(Dims d, Phys ph, StepCoef sc, const double* __restrict__ dtp,
                                                       const double* __restrict__ pi, const double* __restrict__ pb,
                                                       const T* __restrict__ F1, const T* __restrict__ F2,
                                                       const T* __restrict__ F3, const T* __restrict__ emf,
                                                       const double* __restrict__ geom, const double* __restrict__ conn,
-                                                      double* __restrict__ Uout) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long ncell = (long long)d.n1 * d.n2 * d.n3;
-  if (t >= ncell) return;
-  int i = (int)(t % d.n1);
-  long long r = t / d.n1;
-  int j = (int)(r % d.n2), k = (int)(r / d.n2);
+                                                      double* __restrict__ Uout, CellTile ct) {
+  int i, j, k;
+  if (!tile_cell(d.n1, d.n3, ct, blockIdx.x, blockIdx.y, blockIdx.z, i, j, k)) return;
   int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
   const size_t id = cidx(d, ii, jj, kk), c2 = (size_t)jj * d.n1e + ii;
   Geo<double> g;
@@ -694,19 +723,16 @@ __global__ void __launch_bounds__(256, 2) k_conserved(Dims d, Phys ph, StepCoef 
 // positive; a cell whose learned start does not converge starts again from the
 // previous-state W', exactly as without GUESS (counted in stats[2]).
 template <int PATH, bool GUESS = false>
-__global__ void __launch_bounds__(256, 2) k_invert(Dims d, Phys ph, const double* __restrict__ U,
+__global__ void __launch_bounds__(256, HARM_INVERT_BLOCKS) k_invert(Dims d, Phys ph, const double* __restrict__ U,
                                                    const double* __restrict__ pb, double* __restrict__ pf,
                                                    int8_t* __restrict__ pflag, const double* __restrict__ geom,
                                                    const double* __restrict__ aux, unsigned int* __restrict__ rare,
                                                    unsigned int* __restrict__ nrare, double* __restrict__ stats,
-                                                   const double* __restrict__ wpg = nullptr) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long ncell = (long long)d.n1 * d.n2 * d.n3;
+                                                   CellTile ct, const double* __restrict__ wpg = nullptr) {
   double iters_d = 0.0, fb_d = 0.0;
-  if (t < ncell) {
-    int i = (int)(t % d.n1);
-    long long r = t / d.n1;
-    int j = (int)(r % d.n2), k = (int)(r / d.n2);
+  int i, j, k;
+  if (tile_cell(d.n1, d.n3, ct, blockIdx.x, blockIdx.y, blockIdx.z, i, j, k)) {
+    const long long t = i + (long long)d.n1 * (j + (long long)d.n2 * k);  // active-cell index
     int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
     const size_t id = cidx(d, ii, jj, kk), c2 = (size_t)jj * d.n1e + ii;
     Geo<double> g;
@@ -762,21 +788,21 @@ __global__ void __launch_bounds__(256, 2) k_invert(Dims d, Phys ph, const double
 template <int PATH>
 __global__ void __launch_bounds__(256, 3) k_mlp_guess(Dims d, const double* __restrict__ U,
                                                       const double* __restrict__ geom, double* __restrict__ wpg,
-                                                      const MlpPacked* __restrict__ mlp) {
+                                                      const MlpPacked* __restrict__ mlp, CellTile ct) {
   __shared__ MlpPacked sm;
   __shared__ MlpWarpScratch wsc[8];
   mlp_load_packed(sm, mlp);
   __syncthreads();
-  const long long ncell = (long long)d.n1 * d.n2 * d.n3;
-  for (long long base = (long long)blockIdx.x * 256; base < ncell; base += (long long)gridDim.x * 256) {
-    const long long t = base + threadIdx.x;
-    const bool valid = t < ncell;
+  const int gx = (d.n1 + (1 << ct.lti) - 1) >> ct.lti, gz = (d.n3 + (1 << ct.ltk) - 1) >> ct.ltk;
+  const long long ntiles = (long long)gx * d.n2 * gz;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    int i, j, k;
+    const long long rest = tile / gx;
+    const bool valid = tile_cell(d.n1, d.n3, ct, (int)(tile % gx), (int)(rest % d.n2), (int)(rest / d.n2), i, j, k);
+    const long long t = i + (long long)d.n1 * (j + (long long)d.n2 * k);
     float f[MLP_IN];
     double D = 0.0;
     if (valid) {
-      int i = (int)(t % d.n1);
-      long long r = t / d.n1;
-      int j = (int)(r % d.n2), k = (int)(r / d.n2);
       int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
       const size_t id = cidx(d, ii, jj, kk), c2 = (size_t)jj * d.n1e + ii;
       Geo<double> g;

@@ -36,18 +36,20 @@ int hp_update_mixed(harm_ctx* c, const StepCoef& sc, const double* pi, const dou
   Dims d = dims_of(c->g);
   Phys ph = phys_of(c->g);
   long long ncell = (long long)d.n1 * d.n2 * d.n3;
-  k_conserved<float><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, sc, c->d_dt, pi, pb, c->d_Ff[0], c->d_Ff[1],
-                                                         c->d_Ff[2], c->d_emff, c->d_geom, c->d_conn, c->d_U);
+  (void)ncell;
+  const CellTile ct = cell_tile(d.n3);
+  k_conserved<float><<<cell_grid(d.n1, d.n2, d.n3, ct), 256, 0, c->stream>>>(d, ph, sc, c->d_dt, pi, pb, c->d_Ff[0], c->d_Ff[1],
+                                                         c->d_Ff[2], c->d_emff, c->d_geom, c->d_conn, c->d_U, ct);
   CK(cudaMemsetAsync(c->d_nrare, 0, sizeof(unsigned int), c->stream));
   if (sc.guess == HARM_GUESS_MLP) {
     k_mlp_guess<1><<<3 * 148, 256, 0, c->stream>>>(d, c->d_U, c->d_geom, c->d_wpg,
-                                                    reinterpret_cast<const MlpPacked*>(c->d_mlp));
-    k_invert<1, true><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux,
-                                                          c->d_rare, c->d_nrare, stats, c->d_wpg);
+                                                    reinterpret_cast<const MlpPacked*>(c->d_mlp), ct);
+    k_invert<1, true><<<cell_grid(d.n1, d.n2, d.n3, ct), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag,
+                                                          c->d_geom, c->d_aux, c->d_rare, c->d_nrare, stats, ct, c->d_wpg);
     c->launches++;
   } else {
-    k_invert<1><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
-                                                    c->d_nrare, stats);
+    k_invert<1><<<cell_grid(d.n1, d.n2, d.n3, ct), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom,
+                                                    c->d_aux, c->d_rare, c->d_nrare, stats, ct);
   }
   k_invert_rare<1><<<2 * 148, 128, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
                                                      c->d_nrare, stats);
