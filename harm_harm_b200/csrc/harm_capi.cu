@@ -83,6 +83,15 @@ extern "C" int harm_b200_create(const harm_grid* g, const double* geom_h, const 
   c->d_stats = c->d_scal + 16;                          // 5
   c->d_nrec = (unsigned int*)(c->d_scal + 24);
   c->d_nrare = (unsigned int*)(c->d_scal + 25);
+  c->d_status = (unsigned int*)(c->d_scal + 28);
+  {
+    // FP32 flux tiles: plain coalesced loads (default) or TMA ("tma"); both feed the same
+    // arithmetic.  The TMA-staged kernel measured slower on B200 (it needs ~120 registers for
+    // its tile loop, halving the warps that hide the face physics' latency), so it is opt-in.
+    const char* e = getenv("HARM_B200_FLUX_STAGING");
+    c->flux_tma = (e && strcmp(e, "tma") == 0);
+    CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+  }
   CK(cudaMemset(c->d_dtslots, 0xFF, 6 * sizeof(unsigned long long)));
   CK(cudaMallocHost(&c->h_scal, 64 * sizeof(double)));
   *out = c;
@@ -156,6 +165,17 @@ static int substep(harm_ctx* c, int precision, int guess, int timeorder, int num
   return hp_update_mixed(c, sc, d_pi, d_pb, d_pf, d_pflag, st);
 }
 
+// the device error word, read after a synchronisation (it is cleared when reported)
+static int check_status(harm_ctx* c) {
+  unsigned int st = 0;
+  CK(cudaMemcpy(&st, c->d_status, sizeof(st), cudaMemcpyDeviceToHost));
+  if (st) {
+    CK(cudaMemset(c->d_status, 0, sizeof(st)));
+    return seterr_msg("a flux tile's TMA load did not complete (the step's fluxes are incomplete)", 5);
+  }
+  return 0;
+}
+
 static void add_stats(harm_ctx* c, harm_stats* stats, double inverted) {
   if (!stats) return;
   stats->newton_iters += c->h_scal[8];
@@ -179,6 +199,7 @@ extern "C" int harm_b200_advance(harm_ctx* c, int precision, int guess, int time
   CK(cudaMemcpyAsync(c->h_scal + 1, c->d_ndt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(c->h_scal + 8, c->d_stats, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  if (int rc = check_status(c)) return rc;
   if (ndt) *ndt = c->h_scal[1];
   add_stats(c, stats, (double)d.n1 * d.n2 * d.n3);
   return 0;
@@ -213,6 +234,7 @@ extern "C" int harm_b200_step_n(harm_ctx* c, int precision, int guess, double* d
   CK(cudaMemcpyAsync(c->h_scal, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   if (stats) CK(cudaMemcpyAsync(c->h_scal + 8, c->d_stats, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  if (int rc = check_status(c)) return rc;
   *dt = c->h_scal[0];
   add_stats(c, stats, 2.0 * nsteps * (double)d.n1 * d.n2 * d.n3);
   return 0;
@@ -285,5 +307,5 @@ extern "C" int harm_b200_time_stages(harm_ctx* c, int precision, int guess, cons
   CK(cudaMemsetAsync(c->d_dtslots, 0xFF, 6 * sizeof(unsigned long long), c->stream));
   CK(cudaStreamSynchronize(c->stream));
   for (int q = 0; q < 6; q++) cudaEventDestroy(ev[q]);
-  return 0;
+  return check_status(c);
 }

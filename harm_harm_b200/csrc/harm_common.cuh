@@ -284,6 +284,48 @@ struct FluxTile {
   static constexpr size_t smem = (size_t)VB * PLANE * (3 + NW) * sizeof(T);
 };
 
+// The face physics of k_fluxt: B^DIR continuity, limit_gamma, states, fluxes, wave speeds and
+// the HLL flux of one face (flux.c:852, vchar.c:34) into F at `id`; returns cour*dx/ctop.
+template <int DIR, typename T, typename GT>
+__device__ __forceinline__ double face_hll(const Dims& d, const Phys& ph, const GT* __restrict__ geom,
+                                           T* __restrict__ F, size_t id, int ii, int jj, T* pl, T* pr) {
+  constexpr int loc = (DIR == 1) ? HARM_LOC_FACE1 : (DIR == 2) ? HARM_LOC_FACE2 : HARM_LOC_CENT;
+  Geo<T> g;
+  load_geo<T, GT>(geom + (size_t)loc * HARM_NGF * d.plane, d.plane, (size_t)jj * d.n1e + ii, g);
+  const int bp = HARM_B1 + DIR - 1;
+  pl[bp] = pr[bp] = T(0.5) * (pl[bp] + pr[bp]);
+  const T gam = (T)ph.gam, gmax = (T)ph.gammamax;
+  limit_gamma<T>(gmax, pl, g);
+  limit_gamma<T>(gmax, pr, g);
+  State<T> ql, qr;
+  get_state<T>(pl, g, gam, ql);
+  get_state<T>(pr, g, gam, qr);
+  T Fl[NPR], Fr[NPR], Ul[NPR], Ur[NPR];
+  primtoflux<T>(pl, ql, DIR, g, g.gdet, Fl);
+  primtoflux<T>(pl, ql, 0, g, g.gdet, Ul);
+  primtoflux<T>(pr, qr, DIR, g, g.gdet, Fr);
+  primtoflux<T>(pr, qr, 0, g, g.gdet, Ur);
+  T cmaxl, cminl, cmaxr, cminr;
+  vchar<T>(pl, ql, DIR, g, gam, cmaxl, cminl);
+  vchar<T>(pr, qr, DIR, g, gam, cmaxr, cminr);
+  T lmin = fmin(cminl, cminr), lmax = fmax(cmaxl, cmaxr);
+  lmin = fabs(fmax(T(0), -lmin));
+  lmax = fabs(fmax(T(0), lmax));
+  const T cmin = lmin, cmax = lmax, ctop = fmax(lmax, lmin);
+  if (cmax + cmin != T(0)) {
+    const T inv = cmax + cmin;
+#pragma unroll
+    for (int p = 0; p < NPR; p++) F[(size_t)p * d.cells + id] = ((cmax * Fl[p] + cmin * Fr[p]) - (cmax * cmin) * (Ur[p] - Ul[p])) / inv;
+  } else {
+#pragma unroll
+    for (int p = 0; p < NPR; p++) F[(size_t)p * d.cells + id] = T(0.5) * ((Fl[p] + Fr[p]) - ctop * (Ur[p] - Ul[p]));
+  }
+  const double dxd = (DIR == 1) ? ph.dx1 : (DIR == 2) ? ph.dx2 : ph.dx3;
+  double dtij = ph.cour * dxd / (double)ctop;
+  if (!(dtij > 0.0)) dtij = 1.e300;
+  return dtij;
+}
+
 template <int DIR, int LIM, typename T, typename GT>
 __global__ void __launch_bounds__(256) k_fluxt(Dims d, Phys ph, FaceBox fb, const double* __restrict__ P,
                                                const GT* __restrict__ geom, T* __restrict__ F,
@@ -420,40 +462,7 @@ __global__ void __launch_bounds__(256) k_fluxt(Dims d, Phys ph, FaceBox fb, cons
     if (DIR == 1) { ii = lext; jj = text; }
     else if (DIR == 2) { ii = text; jj = lext; }
     else { ii = text; jj = o + d.ng; }
-    constexpr int loc = (DIR == 1) ? HARM_LOC_FACE1 : (DIR == 2) ? HARM_LOC_FACE2 : HARM_LOC_CENT;
-    Geo<T> g;
-    load_geo<T, GT>(geom + (size_t)loc * HARM_NGF * d.plane, d.plane, (size_t)jj * d.n1e + ii, g);
-    const int bp = HARM_B1 + DIR - 1;
-    pl[bp] = pr[bp] = T(0.5) * (pl[bp] + pr[bp]);
-    const T gam = (T)ph.gam, gmax = (T)ph.gammamax;
-    limit_gamma<T>(gmax, pl, g);
-    limit_gamma<T>(gmax, pr, g);
-    State<T> ql, qr;
-    get_state<T>(pl, g, gam, ql);
-    get_state<T>(pr, g, gam, qr);
-    T Fl[NPR], Fr[NPR], Ul[NPR], Ur[NPR];
-    primtoflux<T>(pl, ql, DIR, g, g.gdet, Fl);
-    primtoflux<T>(pl, ql, 0, g, g.gdet, Ul);
-    primtoflux<T>(pr, qr, DIR, g, g.gdet, Fr);
-    primtoflux<T>(pr, qr, 0, g, g.gdet, Ur);
-    T cmaxl, cminl, cmaxr, cminr;
-    vchar<T>(pl, ql, DIR, g, gam, cmaxl, cminl);
-    vchar<T>(pr, qr, DIR, g, gam, cmaxr, cminr);
-    T lmin = fmin(cminl, cminr), lmax = fmax(cmaxl, cmaxr);
-    lmin = fabs(fmax(T(0), -lmin));
-    lmax = fabs(fmax(T(0), lmax));
-    const T cmin = lmin, cmax = lmax, ctop = fmax(lmax, lmin);
-    if (cmax + cmin != T(0)) {
-      const T inv = cmax + cmin;
-#pragma unroll
-      for (int p = 0; p < NPR; p++) F[(size_t)p * d.cells + id] = ((cmax * Fl[p] + cmin * Fr[p]) - (cmax * cmin) * (Ur[p] - Ul[p])) / inv;
-    } else {
-#pragma unroll
-      for (int p = 0; p < NPR; p++) F[(size_t)p * d.cells + id] = T(0.5) * ((Fl[p] + Fr[p]) - ctop * (Ur[p] - Ul[p]));
-    }
-    const double dxd = (DIR == 1) ? ph.dx1 : (DIR == 2) ? ph.dx2 : ph.dx3;
-    dtij = ph.cour * dxd / (double)ctop;
-    if (!(dtij > 0.0)) dtij = 1.e300;
+    dtij = face_hll<DIR, T, GT>(d, ph, geom, F, id, ii, jj, pl, pr);
   }
   // block minimum and one atomic per block
   __shared__ double red[8];

@@ -43,5 +43,8 @@ struct harm_ctx {
   float* d_mlp_work;   // training workspace
   size_t mlp_work_n;
   int mlp_step;
+  unsigned int* d_status; // device error word (bit 0: a TMA tile wait timed out)
+  int flux_tma;            // stage the FP32 flux tiles with TMA (HARM_B200_FLUX_STAGING=tma)
+  int num_sms;
   unsigned long long launches;  // kernels launched by this context
 };

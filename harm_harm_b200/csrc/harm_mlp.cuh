@@ -53,20 +53,25 @@ struct MlpPacked {
 };
 static_assert(sizeof(MlpPacked) % 16 == 0, "packed record is copied as 16-byte words");
 
-__device__ __forceinline__ double mlp_slog(double x) { return copysign(log1p(fabs(x)), x); }
+// slog of a ratio formed in FP64 (so that no product of invariants overflows) and taken in
+// FP32: the features are FP32 inputs of a BF16 network, so FP32 logarithms lose nothing
+__device__ __forceinline__ float mlp_slog(double x) {
+  const float xf = (float)fmax(fmin(x, 1e38), -1e38);
+  return copysignf(log1pf(fabsf(xf)), xf);
+}
 
 // features of one cell from its inversion setup (alpha-scaled quantities) and metric
 __device__ __forceinline__ void mlp_features(const InvC& c, const Geo<double>& g, float* f) {
   const double D = (c.D > 1e-300) ? c.D : 1e-300;
   const double iD = 1.0 / D;
-  f[0] = (float)log(D);
-  f[1] = (float)mlp_slog(c.Bsq * iD);
-  f[2] = (float)mlp_slog(c.Qtsq * iD * iD);
-  f[3] = (float)mlp_slog(c.QdotBsq * iD * iD * iD);
-  f[4] = (float)mlp_slog(-c.Qdotnp * iD);
-  f[5] = (float)mlp_slog(c.Qtsq / (c.Qdotnp * c.Qdotnp + D * D));
+  f[0] = logf(fmaxf((float)fmin(D, 1e38), 1e-38f));
+  f[1] = mlp_slog(c.Bsq * iD);
+  f[2] = mlp_slog(c.Qtsq * iD * iD);
+  f[3] = mlp_slog(c.QdotBsq * iD * iD * iD);
+  f[4] = mlp_slog(-c.Qdotnp * iD);
+  f[5] = mlp_slog(c.Qtsq / (c.Qdotnp * c.Qdotnp + D * D));
   f[6] = (float)g.alpha;
-  f[7] = (float)log(fabs(g.gdet) + 1e-300);
+  f[7] = logf(fmaxf((float)fmin(fabs(g.gdet), 1e38), 1e-38f));
   f[8] = (float)g.betasqoalphasq;
   f[9] = (float)g.gcovpert_tt;
 }

@@ -1,12 +1,82 @@
 // harm_path_mixed.cu -- mixed-precision path of the step: FP32 reconstruction, HLL and
 // flux-CT; FP64 conserved update, sources and inversion (compiled with FMA contraction).
+#include <algorithm>
+#include <cudaTypedefs.h>
+#include <mutex>
 #include "harm_common.cuh"
+#include "harm_flux_tma.cuh"
 #include "harm_paths.h"
+
+int hb_setmsg(const char* msg, int code);
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link to libcuda)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// whether the TMA-staged flux kernel can load this primitive array: 16-byte aligned base
+// and row pitch (n1e even), and staging not switched off for the context
+static bool tma_usable(const harm_ctx* c, const double* P) {
+  return c->flux_tma && ((uintptr_t)P % 16 == 0) && (c->g.n1e % 2 == 0) && tensor_map_encoder() != nullptr;
+}
+
+// 4-D map of P[8][n3e][n2e][n1e] (FP64) with a box of bx x by x bz cells x 8 primitives
+static int make_p_map(CUtensorMap* m, const double* P, const Dims& d, int bx, int by, int bz) {
+  const cuuint64_t dims[4] = {(cuuint64_t)d.n1e, (cuuint64_t)d.n2e, (cuuint64_t)d.n3e, (cuuint64_t)NPR};
+  const cuuint64_t strides[3] = {(cuuint64_t)d.n1e * 8, (cuuint64_t)d.n1e * d.n2e * 8, (cuuint64_t)d.cells * 8};
+  const cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz, (cuuint32_t)NPR};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  CUresult r = tensor_map_encoder()(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(P), dims, strides, box, es,
+                                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return (r == CUDA_SUCCESS) ? 0 : hb_setmsg("cuTensorMapEncodeTiled failed for the primitive array", 4);
+}
+
+template <int DIR, int LIM>
+static int launch_fluxt_tma(harm_ctx* c, const Dims& d, const Phys& ph, const FaceBox& fb, const double* P, float* F,
+                            unsigned long long* slot) {
+  using TB = TmaBox<DIR, LIM>;
+  CUtensorMap map;
+  if (int rc = make_p_map(&map, P, d, TB::BX, TB::BY, TB::BZ)) return rc;
+  static unsigned long long attr_devices = 0;  // per instantiation: devices already raised
+  const unsigned long long bit = 1ull << (c->device & 63);
+  if (!(attr_devices & bit)) {
+    CK(cudaFuncSetAttribute(k_fluxt_tma<DIR, LIM, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TB::smem));
+    attr_devices |= bit;
+  }
+  constexpr int A = FluxTile<LIM, float>::A, NT = FluxTile<LIM, float>::NT;
+  const long long gx = (DIR == 1) ? (fb.cnt[0] + A - 1) / A : (fb.cnt[0] + NT - 1) / NT;
+  const long long gy = (DIR == 1) ? (fb.cnt[1] + NT - 1) / NT : (DIR == 2) ? (fb.cnt[1] + A - 1) / A : (fb.cnt[2] + A - 1) / A;
+  const long long gz = (DIR == 3) ? fb.cnt[1] : fb.cnt[2];
+  const unsigned int nb = (unsigned int)std::min<long long>(gx * gy * gz, (long long)TmaOcc<LIM>::blocks * c->num_sms);
+  k_fluxt_tma<DIR, LIM, float><<<nb, 256, TB::smem, c->stream>>>(d, ph, fb, map, c->d_geomf, F, slot, c->d_status);
+  CK(cudaGetLastError());
+  return 0;
+}
 
 template <int LIM>
 static int flux_dirs_float(harm_ctx* c, const Dims& d, const Phys& ph, const double* pb, float* F1, float* F2, float* F3,
                          unsigned long long* slots) {
   FaceBox b1 = face_box(d, 1), b2 = face_box(d, 2), b3 = face_box(d, 3);
+  if (tma_usable(c, pb)) {
+    if (int rc = launch_fluxt_tma<1, LIM>(c, d, ph, b1, pb, F1, slots + 0)) return rc;
+    if (int rc = launch_fluxt_tma<2, LIM>(c, d, ph, b2, pb, F2, slots + 1)) return rc;
+    c->launches += 2;
+    if (d.n3 > 1) {
+      if (int rc = launch_fluxt_tma<3, LIM>(c, d, ph, b3, pb, F3, slots + 2)) return rc;
+      c->launches++;
+    }
+    return 0;
+  }
   CK((launch_fluxt<1, LIM, float, float>(d, ph, b1, pb, c->d_geomf, F1, slots + 0, c->stream)));
   CK((launch_fluxt<2, LIM, float, float>(d, ph, b2, pb, c->d_geomf, F2, slots + 1, c->stream)));
   c->launches += 2;

@@ -36,7 +36,12 @@
 
 int orc_mlp_nparams(void) { return NPARAMS; }
 
-static double slog(double x) { return copysign(log1p(fabs(x)), x); }
+/* slog of a ratio formed in FP64 and taken in FP32 (as the device does) */
+static float slog(double x) {
+  float xf = (float)fmax(fmin(x, 1e38), -1e38);
+  return copysignf(log1pf(fabsf(xf)), xf);
+}
+static float flog(double x) { return logf(fmaxf((float)fmin(x, 1e38), 1e-38f)); }
 
 void orc_mlp_features(const harm_grid *hg, const double *geomrec, const double *U, const double *P,
                       float *feat, float *targ) {
@@ -46,14 +51,14 @@ void orc_mlp_features(const harm_grid *hg, const double *geomrec, const double *
   for (int p = 0; p < HARM_NPR; p++) Ugf[p] = U[p] * g.igdet;
   o_inv_invariants(Ugf, &g, q);
   const double D = (q[0] > 1e-300) ? q[0] : 1e-300, iD = 1.0 / D;
-  feat[0] = (float)log(D);
-  feat[1] = (float)slog(q[1] * iD);
-  feat[2] = (float)slog(q[2] * iD * iD);
-  feat[3] = (float)slog(q[3] * iD * iD * iD);
-  feat[4] = (float)slog(-q[4] * iD);
-  feat[5] = (float)slog(q[2] / (q[4] * q[4] + D * D));
+  feat[0] = flog(D);
+  feat[1] = slog(q[1] * iD);
+  feat[2] = slog(q[2] * iD * iD);
+  feat[3] = slog(q[3] * iD * iD * iD);
+  feat[4] = slog(-q[4] * iD);
+  feat[5] = slog(q[2] / (q[4] * q[4] + D * D));
   feat[6] = (float)g.alpha;
-  feat[7] = (float)log(fabs(g.gdet) + 1e-300);
+  feat[7] = flog(fabs(g.gdet));
   feat[8] = (float)g.betasqoalphasq;
   feat[9] = (float)g.gcovpert_tt;
   if (targ && P) {
