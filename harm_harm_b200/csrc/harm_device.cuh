@@ -340,10 +340,19 @@ struct WScale<float> {
 template <typename T>
 __device__ __forceinline__ T limit_weight(int order, T w) {
   const T avg = T(1) / T(order), w1 = T(0.2) * avg, w2 = (T(1) - T(0.2)) * avg, w3 = (T(1) + T(0.2)) * avg, w4 = T(1);
-  if (w < w1) return T(0);
-  if (w < w2) return wdivk<T>(avg * (w - w1), w2 - w1);
-  if (w < w3) return avg;
-  return wdivk<T>((w - w3) * (w4 - avg), w4 - w3) + avg;
+  if constexpr (sizeof(T) == 4) {
+    // FP32: both ramps evaluated and selected, no divergent branches (same values)
+    const T lo = wdivk<T>(avg * (w - w1), w2 - w1);
+    const T hi = wdivk<T>((w - w3) * (w4 - avg), w4 - w3) + avg;
+    T r = (w < w3) ? avg : hi;
+    r = (w < w2) ? lo : r;
+    return (w < w1) ? T(0) : r;
+  } else {
+    if (w < w1) return T(0);
+    if (w < w2) return wdivk<T>(avg * (w - w1), w2 - w1);
+    if (w < w3) return avg;
+    return wdivk<T>((w - w3) * (w4 - avg), w4 - w3) + avg;
+  }
 }
 
 // unoptimised (limited, normalised) weights of the three 3-point stencils of the cell at u

@@ -16,7 +16,8 @@
 // Parameters (FP32 master copy, 9154 floats): W1[10][64] b1[64] W2[64][64] b2[64]
 // W3[64][64] b3[64] W4[64][2] b4[2], W[in][out].  Inference uses a packed copy: BF16 weights
 // in the register-fragment order of mma.sync m16n8k16 (row.col) so that each lane loads
-// its B fragment with one 8-byte shared-memory read, FP32 biases and the normalisation.
+// the B fragments of two adjacent tiles with one 16-byte shared-memory read, FP32 biases and
+// the normalisation.
 // A warp evaluates its 32 cells as two 16-row tiles; the FP32 accumulator fragment of one
 // layer is, after SiLU and conversion to BF16, exactly the A fragment of the next layer,
 // so activations never leave registers.
@@ -45,7 +46,7 @@ constexpr int MLP_TILES = 8 + 32 + 32 + 4;
 constexpr int MLP_TILE_L1 = 0, MLP_TILE_L2 = 8, MLP_TILE_L3 = 40, MLP_TILE_L4 = 72;
 constexpr int MLP_NBIAS = 3 * MLP_H + MLP_OUT + 2;
 struct MlpPacked {
-  uint2 frag[MLP_TILES][32];
+  uint4 frag[MLP_TILES / 2][32];  // tile pair p, lane l: {tile 2p: b0b1, b2b3; tile 2p+1: b0b1, b2b3}
   float bias[MLP_NBIAS];
   float norm[MLP_NNORM];
   float start_bias;  // added to log(W'/D) before the Newton start (see mlp_wp_guess)
@@ -157,7 +158,12 @@ __device__ __forceinline__ void mlp_warp_eval(const MlpPacked& m, MlpWarpScratch
       for (int nt = 0; nt < 8; nt++) {
         const float bl = b1[nt * 8 + 2 * q], bh = b1[nt * 8 + 2 * q + 1];
         acc[nt][0] = bl; acc[nt][1] = bh; acc[nt][2] = bl; acc[nt][3] = bh;
-        mma_bf16_16816(acc[nt], a1, m.frag[MLP_TILE_L1 + nt][lane]);
+      }
+#pragma unroll
+      for (int np = 0; np < 4; np++) {
+        const uint4 bb = m.frag[MLP_TILE_L1 / 2 + np][lane];
+        mma_bf16_16816(acc[2 * np], a1, make_uint2(bb.x, bb.y));
+        mma_bf16_16816(acc[2 * np + 1], a1, make_uint2(bb.z, bb.w));
       }
     }
 #pragma unroll
@@ -174,7 +180,11 @@ __device__ __forceinline__ void mlp_warp_eval(const MlpPacked& m, MlpWarpScratch
 #pragma unroll
       for (int kt = 0; kt < 4; kt++)
 #pragma unroll
-        for (int nt = 0; nt < 8; nt++) mma_bf16_16816(acc[nt], a[kt], m.frag[base + kt * 8 + nt][lane]);
+        for (int np = 0; np < 4; np++) {
+          const uint4 bb = m.frag[(base + kt * 8) / 2 + np][lane];
+          mma_bf16_16816(acc[2 * np], a[kt], make_uint2(bb.x, bb.y));
+          mma_bf16_16816(acc[2 * np + 1], a[kt], make_uint2(bb.z, bb.w));
+        }
 #pragma unroll
       for (int kt = 0; kt < 4; kt++) mlp_act_to_a(acc[2 * kt], acc[2 * kt + 1], a[kt]);
     }
@@ -184,7 +194,11 @@ __device__ __forceinline__ void mlp_warp_eval(const MlpPacked& m, MlpWarpScratch
     o[2] = o[0];
     o[3] = o[1];
 #pragma unroll
-    for (int kt = 0; kt < 4; kt++) mma_bf16_16816(o, a[kt], m.frag[MLP_TILE_L4 + kt][lane]);
+    for (int kp = 0; kp < 2; kp++) {
+      const uint4 bb = m.frag[MLP_TILE_L4 / 2 + kp][lane];
+      mma_bf16_16816(o, a[2 * kp], make_uint2(bb.x, bb.y));
+      mma_bf16_16816(o, a[2 * kp + 1], make_uint2(bb.z, bb.w));
+    }
     if (q == 0) {
       ws.y[r0 * 2 + 0] = o[0];
       ws.y[r0 * 2 + 1] = o[1];

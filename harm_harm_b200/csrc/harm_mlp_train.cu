@@ -288,10 +288,9 @@ __global__ void k_mlp_pack(const float* __restrict__ params, const float* __rest
     else { woff = MLP_OFF_W4; K = MLP_H; N = MLP_OUT; kt = tile - MLP_TILE_L4; nt = 0; }
     const int k0 = kt * 16 + 2 * (lane & 3), n = nt * 8 + (lane >> 2);
     auto W = [&](int k) -> float { return (k < K && n < N) ? params[woff + k * N + n] : 0.0f; };
-    uint2 f;
-    f.x = pack_bf16x2(W(k0), W(k0 + 1));
-    f.y = pack_bf16x2(W(k0 + 8), W(k0 + 9));
-    out->frag[tile][lane] = f;
+    uint32_t* f = reinterpret_cast<uint32_t*>(&out->frag[tile >> 1][lane]) + 2 * (tile & 1);
+    f[0] = pack_bf16x2(W(k0), W(k0 + 1));
+    f[1] = pack_bf16x2(W(k0 + 8), W(k0 + 9));
   }
   if (t < MLP_NBIAS) {
     float b = 0.0f;
