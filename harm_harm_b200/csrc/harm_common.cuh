@@ -15,6 +15,7 @@
 #include "harm_device.cuh"
 #include "harm_invert.cuh"
 #include "harm_mlp.cuh"
+#include "harm_weno_f32x2.cuh"
 #include "harm_ctx.cuh"
 
 using namespace hb;
@@ -393,7 +394,67 @@ __global__ void __launch_bounds__(256) k_fluxt(Dims d, Phys ph, FaceBox fb, cons
       s_y[v * PL + sx(cl, ct)] = (T)__ldg(P + (size_t)(p0 + v) * d.cells + cell_index(lext, text));
     }
     __syncthreads();
-    if (LIM == HARM_LIM_WENO5) {
+    if constexpr (LIM == HARM_LIM_WENO5 && sizeof(T) == 4) {
+      // FP32: two cells per thread on the packed FP32 pipe (harm_weno_f32x2.cuh)
+      constexpr int NU = VB * (NL - 4) * NT, NU2 = (NU + 1) / 2;
+      for (int idx = tid; idx < NU2; idx += 256) {
+        const int ib = idx + NU2;
+        const bool hasb = ib < NU;
+        int va, ca, ta, vb, cb, tb;
+        split(idx, 2, NL - 4, va, ca, ta);
+        split(hasb ? ib : idx, 2, NL - 4, vb, cb, tb);
+        const T* ya = s_y + va * PL;
+        const T* yb = s_y + vb * PL;
+        F2 u5[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) u5[q] = f2((float)ya[sx(ca - 2 + q, ta)], (float)yb[sx(cb - 2 + q, tb)]);
+        F2 w[3];
+        weno5_unopt_f2(u5 + 2, w);
+        T* wsa = s_w + (va * PL + sx(ca, ta)) * 3;
+        T* wsb = s_w + (vb * PL + sx(cb, tb)) * 3;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          float a, b;
+          f2split(w[k], a, b);
+          wsa[k] = (T)a;
+          if (hasb) wsb[k] = (T)b;
+        }
+      }
+      __syncthreads();
+      constexpr int NE = VB * (A + 1) * NT, NE2 = (NE + 1) / 2;
+      for (int idx = tid; idx < NE2; idx += 256) {
+        const int ib = idx + NE2;
+        const bool hasb = ib < NE;
+        int va, ca, ta, vb, cb, tb;
+        split(idx, H - 1, A + 1, va, ca, ta);
+        split(hasb ? ib : idx, H - 1, A + 1, vb, cb, tb);
+        const T* ya = s_y + va * PL;
+        const T* yb = s_y + vb * PL;
+        F2 u5[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) u5[q] = f2((float)ya[sx(ca - 2 + q, ta)], (float)yb[sx(cb - 2 + q, tb)]);
+        const T* wa = s_w + va * PL * 3;
+        const T* wb = s_w + vb * PL * 3;
+        F2 w[3], wm[3], wp[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          w[k] = f2((float)wa[sx(ca, ta) * 3 + k], (float)wb[sx(cb, tb) * 3 + k]);
+          wm[k] = f2((float)wa[sx(ca - 2, ta) * 3 + k], (float)wb[sx(cb - 2, tb) * 3 + k]);
+          wp[k] = f2((float)wa[sx(ca + 2, ta) * 3 + k], (float)wb[sx(cb + 2, tb) * 3 + k]);
+        }
+        F2 yl, yr;
+        weno5_edges_f2(u5 + 2, w, wm, wp, yl, yr);
+        float la, lb, ra, rb;
+        f2split(yl, la, lb);
+        f2split(yr, ra, rb);
+        s_el[va * PL + sx(ca, ta)] = (T)la;
+        s_er[va * PL + sx(ca, ta)] = (T)ra;
+        if (hasb) {
+          s_el[vb * PL + sx(cb, tb)] = (T)lb;
+          s_er[vb * PL + sx(cb, tb)] = (T)rb;
+        }
+      }
+    } else if (LIM == HARM_LIM_WENO5) {
       // unoptimised weights of cells 2 .. NL-3
       for (int idx = tid; idx < VB * (NL - 4) * NT; idx += 256) {
         int v, c, t;

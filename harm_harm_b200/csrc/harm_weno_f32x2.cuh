@@ -1,0 +1,192 @@
+// harm_weno_f32x2.cuh -- the FP32 WENO5 weights and edge values of two cells at once on
+// Blackwell's packed FP32 pipe (add/sub/mul/fma .f32x2: one instruction, two lanes).
+//
+// The arithmetic is that of weno5_unopt / weno3_unopt / weno5_edges for T = float
+// (harm_device.cuh), lane by lane; operations without a packed form (reciprocals, compares,
+// selects, min/max) run on each lane.  Where the scalar code branches on f > 0 (the WENO3
+// blend of the stencil reduction), the packed code evaluates the blend for both lanes when
+// either needs it: with f = 0 it multiplies by 1 and adds zeros, so a lane's value is the
+// one its scalar branch gives (the WENO3 weights are finite: every epsilon keeps its square
+// a normal FP32 number).
+#pragma once
+#include "harm_device.cuh"
+
+namespace hb {
+
+struct F2 {
+  unsigned long long v;
+};
+
+__device__ __forceinline__ F2 f2(float a, float b) {
+  F2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ F2 f2(float a) { return f2(a, a); }
+__device__ __forceinline__ void f2split(F2 x, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(x.v));
+}
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) {
+  F2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) {
+  F2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) {
+  F2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 ffma2(F2 a, F2 b, F2 c) {
+  F2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+  return r;
+}
+// lane-wise helpers
+template <typename Fn>
+__device__ __forceinline__ F2 lanes(F2 x, Fn fn) {
+  float a, b;
+  f2split(x, a, b);
+  return f2(fn(a), fn(b));
+}
+template <typename Fn>
+__device__ __forceinline__ F2 lanes(F2 x, F2 y, Fn fn) {
+  float a, b, c, d;
+  f2split(x, a, b);
+  f2split(y, c, d);
+  return f2(fn(a, c), fn(b, d));
+}
+__device__ __forceinline__ F2 rcp2(F2 x) {
+  return lanes(x, [](float a) { return __fdividef(1.0f, a); });
+}
+
+__device__ __forceinline__ F2 symsum3(F2 a0, F2 a1, F2 a2) { return (a0 + a2) + a1; }
+__device__ __forceinline__ F2 symsum2(F2 a0, F2 a1) { return a0 + a1; }
+
+__device__ __forceinline__ F2 limit_weight3_f2(F2 w) {
+  return lanes(w, [](float x) { return limit_weight<float>(3, x); });
+}
+__device__ __forceinline__ F2 limit_weight2_f2(F2 w) {
+  return lanes(w, [](float x) { return limit_weight<float>(2, x); });
+}
+
+// weno5_unopt of two cells: u points at the cells' centre values (u[-2..2])
+__device__ __forceinline__ void weno5_unopt_f2(const F2* u, F2* w) {
+  const F2 c3 = f2(3.0f), c4 = f2(4.0f), c2 = f2(2.0f), k13 = f2((float)(13. / 12.)), k14 = f2(0.25f);
+  const F2 fd0 = (c4 * u[1]) - ffma2(c3, u[0], u[2]);
+  const F2 fd1 = u[1] - u[-1];
+  const F2 fd2 = ffma2(c3, u[0], u[-2]) - (c4 * u[-1]);
+  const F2 sd0 = (u[0] + u[2]) - (c2 * u[1]);
+  const F2 sd1 = (u[-1] + u[1]) - (c2 * u[0]);
+  const F2 sd2 = (u[0] + u[-2]) - (c2 * u[-1]);
+  F2 b[3];
+  b[0] = ffma2(k13 * sd0, sd0, k14 * fd0 * fd0);
+  b[1] = ffma2(k13 * sd1, sd1, k14 * fd1 * fd1);
+  b[2] = ffma2(k13 * sd2, sd2, k14 * fd2 * fd2);
+  const F2 normu = ffma2(u[0], u[0], ffma2(u[-1], u[-1], u[1] * u[1]) + ffma2(u[-2], u[-2], u[2] * u[2]));
+  const F2 ee = normu * f2(WenoEps<float>::eps);
+#pragma unroll
+  for (int s = 0; s < 3; s++) b[s] = b[s] + ee;
+  const F2 rb = rcp2(symsum3(b[0], b[1], b[2]) + f2(WenoEps<float>::tiny));
+#pragma unroll
+  for (int s = 0; s < 3; s++) {
+    const F2 t = b[s] * rb + f2(WenoEps<float>::weps);
+    w[s] = rcp2(t * t);
+  }
+  const F2 r1 = rcp2(symsum3(w[0], w[1], w[2]));
+#pragma unroll
+  for (int s = 0; s < 3; s++) w[s] = limit_weight3_f2(w[s] * r1);
+  const F2 r2 = rcp2(symsum3(w[0], w[1], w[2]));
+#pragma unroll
+  for (int s = 0; s < 3; s++) w[s] = w[s] * r2;
+}
+
+__device__ __forceinline__ void weno3_unopt_f2(const F2* u, F2* w) {
+  const F2 fd0 = u[1] - u[0], fd1 = u[0] - u[-1];
+  F2 b[2] = {fd0 * fd0, fd1 * fd1};
+  const F2 normu = ffma2(u[0], u[0], ffma2(u[-1], u[-1], u[1] * u[1]));
+  const F2 ee = normu * f2(WenoEps<float>::eps);
+  b[0] = b[0] + ee;
+  b[1] = b[1] + ee;
+  const F2 rb = rcp2(symsum2(b[0], b[1]) + f2(WenoEps<float>::tiny));
+#pragma unroll
+  for (int s = 0; s < 2; s++) {
+    const F2 t = b[s] * rb + f2(WenoEps<float>::weps);
+    w[s] = rcp2(t * t);
+  }
+  const F2 r1 = rcp2(symsum2(w[0], w[1]));
+  w[0] = limit_weight2_f2(w[0] * r1);
+  w[1] = limit_weight2_f2(w[1] * r1);
+  const F2 r2 = rcp2(symsum2(w[0], w[1]));
+  w[0] = w[0] * r2;
+  w[1] = w[1] * r2;
+}
+
+// keep x where the weight is non-zero (eno_cvt skips zero weights)
+__device__ __forceinline__ F2 nz_mul(F2 wgt, F2 x) {
+  const F2 p = wgt * x;
+  return lanes(wgt, p, [](float wv, float pv) { return (wv != 0.0f) ? pv : 0.0f; });
+}
+
+// weno5_edges of two cells
+__device__ __forceinline__ void weno5_edges_f2(const F2* u, const F2* w, const F2* wm, const F2* wp, F2& yl, F2& yr) {
+  const F2 E = f2(WenoEps<float>::eps);
+  const F2 rl = lanes(w[2] + E, wm[0] + E, [](float a, float b) { return __fdividef(a, b); });
+  const F2 rr = lanes(w[0] + E, wp[2] + E, [](float a, float b) { return __fdividef(a, b); });
+  const F2 ratio = lanes(rl, rr, [](float a, float b) { return fminf(a, b); });
+  const F2 f = lanes((ratio - f2(1.3f)) * f2(1.0f / (1.6f - 1.3f)), [](float a) { return fmaxf(0.0f, fminf(a, 1.0f)); });
+  F2 wl[3] = {w[0] * f2(1.f / 16.f), w[1] * f2(5.f / 8.f), w[2] * f2(5.f / 16.f)};
+  F2 wr[3] = {w[0] * f2(5.f / 16.f), w[1] * f2(5.f / 8.f), w[2] * f2(1.f / 16.f)};
+  const F2 nl = rcp2(symsum3(wl[0], wl[1], wl[2]) + f2(WenoEps<float>::tiny));
+  const F2 nr = rcp2(symsum3(wr[0], wr[1], wr[2]) + f2(WenoEps<float>::tiny));
+  float fa, fb;
+  f2split(f, fa, fb);
+  const bool two = (0.0f < fa) || (0.0f < fb);
+  const F2 omf = f2(1.0f) - f;
+#pragma unroll
+  for (int s = 0; s < 3; s++) {
+    wl[s] = wl[s] * nl;
+    wr[s] = wr[s] * nr;
+    if (two) {
+      wl[s] = wl[s] * omf;
+      wr[s] = wr[s] * omf;
+    }
+  }
+  const F2 k158 = f2(15.f / 8.f), k54 = f2(-5.f / 4.f), k38 = f2(3.f / 8.f), k34 = f2(3.f / 4.f), k18 = f2(-1.f / 8.f);
+  const F2 recl0 = symsum3(k158 * u[0], k54 * u[1], k38 * u[2]);
+  const F2 recl1 = symsum3(k38 * u[-1], k34 * u[0], k18 * u[1]);
+  const F2 recl2 = symsum3(k18 * u[-2], k34 * u[-1], k38 * u[0]);
+  const F2 recr0 = symsum3(k38 * u[0], k34 * u[1], k18 * u[2]);
+  const F2 recr1 = symsum3(k18 * u[-1], k34 * u[0], k38 * u[1]);
+  const F2 recr2 = symsum3(k38 * u[-2], k54 * u[-1], k158 * u[0]);
+  F2 outl = symsum3(nz_mul(wl[0], recl0), nz_mul(wl[1], recl1), nz_mul(wl[2], recl2));
+  F2 outr = symsum3(nz_mul(wr[0], recr0), nz_mul(wr[1], recr1), nz_mul(wr[2], recr2));
+  if (two) {
+    F2 w3[2];
+    weno3_unopt_f2(u, w3);
+    F2 l3[2] = {w3[0] * f2(0.25f), w3[1] * f2(0.75f)};
+    F2 r3[2] = {w3[0] * f2(0.75f), w3[1] * f2(0.25f)};
+    const F2 nl3 = rcp2(symsum2(l3[0], l3[1]) + f2(WenoEps<float>::tiny));
+    const F2 nr3 = rcp2(symsum2(r3[0], r3[1]) + f2(WenoEps<float>::tiny));
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      l3[s] = (l3[s] * nl3) * f;
+      r3[s] = (r3[s] * nr3) * f;
+    }
+    const F2 h = f2(0.5f), k32 = f2(1.5f), km12 = f2(-0.5f);
+    const F2 rl0 = symsum2(k32 * u[0], km12 * u[1]);
+    const F2 rl1 = symsum2(h * u[-1], h * u[0]);
+    const F2 rr0 = symsum2(h * u[0], h * u[1]);
+    const F2 rr1 = symsum2(km12 * u[-1], k32 * u[0]);
+    outl = outl + symsum2(nz_mul(l3[0], rl0), nz_mul(l3[1], rl1));
+    outr = outr + symsum2(nz_mul(r3[0], rr0), nz_mul(r3[1], rr1));
+  }
+  yl = outl;
+  yr = outr;
+}
+
+}  // namespace hb
