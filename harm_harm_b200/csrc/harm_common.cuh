@@ -753,9 +753,15 @@ __global__ void __launch_bounds__(256, HARM_CONSERVED_BLOCKS) k_conserved(Dims d
                                                       const T* __restrict__ F1, const T* __restrict__ F2,
                                                       const T* __restrict__ F3, const T* __restrict__ emf,
                                                       const double* __restrict__ geom, const double* __restrict__ conn,
-                                                      double* __restrict__ Uout, CellTile ct) {
-  int i, j, k;
-  if (!tile_cell(d.n1, d.n3, ct, blockIdx.x, blockIdx.y, blockIdx.z, i, j, k)) return;
+                                                      double* __restrict__ Uout) {
+  // one thread per active cell, i fastest (the (i,k) tiles of the inversion kernels measured
+  // slower here: this kernel's neighbour reads of the fluxes favour whole i rows)
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long ncell = (long long)d.n1 * d.n2 * d.n3;
+  if (t >= ncell) return;
+  int i = (int)(t % d.n1);
+  long long r = t / d.n1;
+  int j = (int)(r % d.n2), k = (int)(r / d.n2);
   int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
   const size_t id = cidx(d, ii, jj, kk), c2 = (size_t)jj * d.n1e + ii;
   Geo<double> g;
