@@ -93,24 +93,44 @@ struct FixRec {
 };
 
 // Cell tiles of the per-cell kernels: a block of 256 threads covers TI consecutive i times TK
-// consecutive k at one j (TK = 16 in 3-D, 1 in 2-D), so the per-(i,j) metric and connection
-// records a block reads serve TK cells each and come from L1 instead of L2; rows of TI
-// consecutive i keep the state loads coalesced.
+// consecutive k at one j, so the per-(i,j) metric and connection records a block reads serve
+// TK cells each and come from L1 instead of L2, while rows of TI consecutive i keep the state
+// loads coalesced.  TI = 256 / TK; lti < 0 selects one thread per cell in i-fastest order.
 struct CellTile {
   int lti, ltk;  // log2 TI, log2 TK
 };
-static inline CellTile cell_tile(int n3) {
+static inline CellTile cell_tile(int n3, int ltk_max) {
   CellTile ct;
   ct.ltk = 0;
-  while (ct.ltk < 4 && (2 << ct.ltk) <= n3) ct.ltk++;
+  while (ct.ltk < ltk_max && (2 << ct.ltk) <= n3) ct.ltk++;
   ct.lti = 8 - ct.ltk;
   return ct;
 }
+static inline CellTile cell_linear() {
+  CellTile ct;
+  ct.lti = -1;
+  ct.ltk = 0;
+  return ct;
+}
 static inline dim3 cell_grid(int n1, int n2, int n3, CellTile ct) {
+  if (ct.lti < 0) return dim3((unsigned)(((long long)n1 * n2 * n3 + 255) / 256), 1, 1);
   return dim3((n1 + (1 << ct.lti) - 1) >> ct.lti, n2, (n3 + (1 << ct.ltk) - 1) >> ct.ltk);
 }
+__device__ __forceinline__ dim3 cell_grid_dev(const Dims& d, CellTile ct) {
+  if (ct.lti < 0) return dim3((unsigned)(((long long)d.n1 * d.n2 * d.n3 + 255) / 256), 1, 1);
+  return dim3((d.n1 + (1 << ct.lti) - 1) >> ct.lti, d.n2, (d.n3 + (1 << ct.ltk) - 1) >> ct.ltk);
+}
 // this thread's active cell (i, j, k) in tile (tx, ty, tz); false past the grid's edge
-__device__ __forceinline__ bool tile_cell(int n1, int n3, CellTile ct, int tx, int ty, int tz, int& i, int& j, int& k) {
+__device__ __forceinline__ bool tile_cell(int n1, int n2, int n3, CellTile ct, int tx, int ty, int tz, int& i, int& j,
+                                          int& k) {
+  if (ct.lti < 0) {
+    const long long t = (long long)tx * 256 + threadIdx.x;
+    i = (int)(t % n1);
+    const long long r = t / n1;
+    j = (int)(r % n2);
+    k = (int)(r / n2);
+    return t < (long long)n1 * n2 * n3;
+  }
   i = (tx << ct.lti) + (int)(threadIdx.x & ((1u << ct.lti) - 1));
   k = (tz << ct.ltk) + (int)(threadIdx.x >> ct.lti);
   j = ty;
@@ -743,6 +763,13 @@ __device__ __forceinline__ int fixup1zone(double* pr, const Geo<double>& g, doub
 #ifndef HARM_CONSERVED_BLOCKS
 #define HARM_CONSERVED_BLOCKS 2
 #endif
+// log2 of the k extent of the cell tiles (0: whole i rows, one thread per cell in order)
+#ifndef HARM_CONSERVED_LTK
+#define HARM_CONSERVED_LTK 0
+#endif
+#ifndef HARM_INVERT_LTK
+#define HARM_INVERT_LTK 4
+#endif
 #ifndef HARM_INVERT_BLOCKS
 #define HARM_INVERT_BLOCKS 3
 #endif
@@ -753,15 +780,9 @@ __global__ void __launch_bounds__(256, HARM_CONSERVED_BLOCKS) k_conserved(Dims d
                                                       const T* __restrict__ F1, const T* __restrict__ F2,
                                                       const T* __restrict__ F3, const T* __restrict__ emf,
                                                       const double* __restrict__ geom, const double* __restrict__ conn,
-                                                      double* __restrict__ Uout) {
-  // one thread per active cell, i fastest (the (i,k) tiles of the inversion kernels measured
-  // slower here: this kernel's neighbour reads of the fluxes favour whole i rows)
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long ncell = (long long)d.n1 * d.n2 * d.n3;
-  if (t >= ncell) return;
-  int i = (int)(t % d.n1);
-  long long r = t / d.n1;
-  int j = (int)(r % d.n2), k = (int)(r / d.n2);
+                                                      double* __restrict__ Uout, CellTile ct) {
+  int i, j, k;
+  if (!tile_cell(d.n1, d.n2, d.n3, ct, blockIdx.x, blockIdx.y, blockIdx.z, i, j, k)) return;
   int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
   const size_t id = cidx(d, ii, jj, kk), c2 = (size_t)jj * d.n1e + ii;
   Geo<double> g;
@@ -807,7 +828,7 @@ __global__ void __launch_bounds__(256, HARM_INVERT_BLOCKS) k_invert(Dims d, Phys
                                                    CellTile ct, const double* __restrict__ wpg = nullptr) {
   double iters_d = 0.0, fb_d = 0.0;
   int i, j, k;
-  if (tile_cell(d.n1, d.n3, ct, blockIdx.x, blockIdx.y, blockIdx.z, i, j, k)) {
+  if (tile_cell(d.n1, d.n2, d.n3, ct, blockIdx.x, blockIdx.y, blockIdx.z, i, j, k)) {
     const long long t = i + (long long)d.n1 * (j + (long long)d.n2 * k);  // active-cell index
     int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
     const size_t id = cidx(d, ii, jj, kk), c2 = (size_t)jj * d.n1e + ii;
@@ -869,12 +890,13 @@ __global__ void __launch_bounds__(256, 3) k_mlp_guess(Dims d, const double* __re
   __shared__ MlpWarpScratch wsc[8];
   mlp_load_packed(sm, mlp);
   __syncthreads();
-  const int gx = (d.n1 + (1 << ct.lti) - 1) >> ct.lti, gz = (d.n3 + (1 << ct.ltk) - 1) >> ct.ltk;
-  const long long ntiles = (long long)gx * d.n2 * gz;
+  const dim3 gg = cell_grid_dev(d, ct);
+  const int gx = (int)gg.x;
+  const long long ntiles = (long long)gg.x * gg.y * gg.z;
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     int i, j, k;
     const long long rest = tile / gx;
-    const bool valid = tile_cell(d.n1, d.n3, ct, (int)(tile % gx), (int)(rest % d.n2), (int)(rest / d.n2), i, j, k);
+    const bool valid = tile_cell(d.n1, d.n2, d.n3, ct, (int)(tile % gx), (int)(rest % gg.y), (int)(rest / gg.y), i, j, k);
     const long long t = i + (long long)d.n1 * (j + (long long)d.n2 * k);
     float f[MLP_IN];
     double D = 0.0;

@@ -106,9 +106,10 @@ int hp_update_mixed(harm_ctx* c, const StepCoef& sc, const double* pi, const dou
   Dims d = dims_of(c->g);
   Phys ph = phys_of(c->g);
   long long ncell = (long long)d.n1 * d.n2 * d.n3;
-  const CellTile ct = cell_tile(d.n3);
-  k_conserved<float><<<nblk(ncell), 256, 0, c->stream>>>(d, ph, sc, c->d_dt, pi, pb, c->d_Ff[0], c->d_Ff[1],
-                                                         c->d_Ff[2], c->d_emff, c->d_geom, c->d_conn, c->d_U);
+  const CellTile ct = cell_tile(d.n3, HARM_INVERT_LTK);
+  const CellTile cct = (HARM_CONSERVED_LTK > 0 && d.n3 >= 8) ? cell_tile(d.n3, HARM_CONSERVED_LTK) : cell_linear();
+  k_conserved<float><<<cell_grid(d.n1, d.n2, d.n3, cct), 256, 0, c->stream>>>(d, ph, sc, c->d_dt, pi, pb, c->d_Ff[0], c->d_Ff[1],
+                                                         c->d_Ff[2], c->d_emff, c->d_geom, c->d_conn, c->d_U, cct);
   CK(cudaMemsetAsync(c->d_nrare, 0, sizeof(unsigned int), c->stream));
   if (sc.guess == HARM_GUESS_MLP) {
     k_mlp_guess<1><<<3 * 148, 256, 0, c->stream>>>(d, c->d_U, c->d_geom, c->d_wpg,
