@@ -126,11 +126,10 @@ __device__ __forceinline__ void weno3_unopt_f2(const F2* u, F2* w) {
   w[1] = w[1] * r2;
 }
 
-// keep x where the weight is non-zero (eno_cvt skips zero weights)
-__device__ __forceinline__ F2 nz_mul(F2 wgt, F2 x) {
-  const F2 p = wgt * x;
-  return lanes(wgt, p, [](float wv, float pv) { return (wv != 0.0f) ? pv : 0.0f; });
-}
+// Weights times stencil values: eno_cvt skips zero weights; for the finite stencil values of
+// finite data the product of a zero weight is a zero anyway (at most of the other sign, which
+// no later sum can tell apart), so the packed path multiplies (and fuses the sums).
+__device__ __forceinline__ F2 nz_mul(F2 wgt, F2 x) { return wgt * x; }
 
 // weno5_edges of two cells
 __device__ __forceinline__ void weno5_edges_f2(const F2* u, const F2* w, const F2* wm, const F2* wp, F2& yl, F2& yr) {
@@ -157,14 +156,16 @@ __device__ __forceinline__ void weno5_edges_f2(const F2* u, const F2* w, const F
     }
   }
   const F2 k158 = f2(15.f / 8.f), k54 = f2(-5.f / 4.f), k38 = f2(3.f / 8.f), k34 = f2(3.f / 4.f), k18 = f2(-1.f / 8.f);
-  const F2 recl0 = symsum3(k158 * u[0], k54 * u[1], k38 * u[2]);
-  const F2 recl1 = symsum3(k38 * u[-1], k34 * u[0], k18 * u[1]);
-  const F2 recl2 = symsum3(k18 * u[-2], k34 * u[-1], k38 * u[0]);
-  const F2 recr0 = symsum3(k38 * u[0], k34 * u[1], k18 * u[2]);
-  const F2 recr1 = symsum3(k18 * u[-1], k34 * u[0], k38 * u[1]);
-  const F2 recr2 = symsum3(k38 * u[-2], k54 * u[-1], k158 * u[0]);
-  F2 outl = symsum3(nz_mul(wl[0], recl0), nz_mul(wl[1], recl1), nz_mul(wl[2], recl2));
-  F2 outr = symsum3(nz_mul(wr[0], recr0), nz_mul(wr[1], recr1), nz_mul(wr[2], recr2));
+  // the symmetric sums (a0 + a2) + a1 of the scalar code, contracted into packed FMAs
+  auto poly3 = [](F2 k0, F2 x0, F2 k1, F2 x1, F2 k2, F2 x2) { return ffma2(k1, x1, ffma2(k0, x0, k2 * x2)); };
+  const F2 recl0 = poly3(k158, u[0], k54, u[1], k38, u[2]);
+  const F2 recl1 = poly3(k38, u[-1], k34, u[0], k18, u[1]);
+  const F2 recl2 = poly3(k18, u[-2], k34, u[-1], k38, u[0]);
+  const F2 recr0 = poly3(k38, u[0], k34, u[1], k18, u[2]);
+  const F2 recr1 = poly3(k18, u[-1], k34, u[0], k38, u[1]);
+  const F2 recr2 = poly3(k38, u[-2], k54, u[-1], k158, u[0]);
+  F2 outl = poly3(wl[0], recl0, wl[1], recl1, wl[2], recl2);
+  F2 outr = poly3(wr[0], recr0, wr[1], recr1, wr[2], recr2);
   if (two) {
     F2 w3[2];
     weno3_unopt_f2(u, w3);
@@ -178,12 +179,12 @@ __device__ __forceinline__ void weno5_edges_f2(const F2* u, const F2* w, const F
       r3[s] = (r3[s] * nr3) * f;
     }
     const F2 h = f2(0.5f), k32 = f2(1.5f), km12 = f2(-0.5f);
-    const F2 rl0 = symsum2(k32 * u[0], km12 * u[1]);
-    const F2 rl1 = symsum2(h * u[-1], h * u[0]);
-    const F2 rr0 = symsum2(h * u[0], h * u[1]);
-    const F2 rr1 = symsum2(km12 * u[-1], k32 * u[0]);
-    outl = outl + symsum2(nz_mul(l3[0], rl0), nz_mul(l3[1], rl1));
-    outr = outr + symsum2(nz_mul(r3[0], rr0), nz_mul(r3[1], rr1));
+    const F2 rl0 = ffma2(k32, u[0], km12 * u[1]);
+    const F2 rl1 = ffma2(h, u[-1], h * u[0]);
+    const F2 rr0 = ffma2(h, u[0], h * u[1]);
+    const F2 rr1 = ffma2(km12, u[-1], k32 * u[0]);
+    outl = outl + ffma2(l3[0], rl0, nz_mul(l3[1], rl1));
+    outr = outr + ffma2(r3[0], rr0, nz_mul(r3[1], rr1));
   }
   yl = outl;
   yr = outr;
