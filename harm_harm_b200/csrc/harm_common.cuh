@@ -301,8 +301,10 @@ struct FluxTile {
   static constexpr int NL = A + H + ReconGeom<LIM>::X;         // staged cells along DIR
   static constexpr int VB = (sizeof(T) == 4) ? 8 : 4;          // primitives per stage
   static constexpr int NW = (LIM == HARM_LIM_WENO5) ? 3 : 0;   // weights per cell
-  static constexpr int PLANE = NL * NT;
-  static constexpr size_t smem = (size_t)VB * PLANE * (3 + NW) * sizeof(T);
+  static constexpr int PLANE = NL * NT;               // staged values of one primitive
+  static constexpr int PE = (A + 1) * NT;              // edge values: cells H-1 .. H+A-1
+  static constexpr int PW = (NL - 4) * NT;             // WENO5 weights: cells 2 .. NL-3
+  static constexpr size_t smem = (size_t)VB * (PLANE + 2 * PE + NW * PW) * sizeof(T);
 };
 
 // The face physics of k_fluxt: B^DIR continuity, limit_gamma, states, fluxes, wave speeds and
@@ -352,14 +354,17 @@ __global__ void __launch_bounds__(256) k_fluxt(Dims d, Phys ph, FaceBox fb, cons
                                                const GT* __restrict__ geom, T* __restrict__ F,
                                                unsigned long long* __restrict__ dtslot) {
   using TL = FluxTile<LIM, T>;
-  constexpr int A = TL::A, NT = TL::NT, H = TL::H, NL = TL::NL, VB = TL::VB, PL = TL::PLANE;
+  constexpr int A = TL::A, NT = TL::NT, H = TL::H, NL = TL::NL, VB = TL::VB, PL = TL::PLANE, PE = TL::PE, PW = TL::PW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s_y = reinterpret_cast<T*>(smem_raw);   // [VB][plane]
-  T* s_el = s_y + VB * PL;                    // left edge of each cell
-  T* s_er = s_el + VB * PL;                   // right edge of each cell
-  T* s_w = s_er + VB * PL;                    // WENO5 unoptimised weights, [VB][plane][3]
+  T* s_el = s_y + VB * PL;                    // left edge of each cell, [VB][PE]
+  T* s_er = s_el + VB * PE;                   // right edge of each cell, [VB][PE]
+  T* s_w = s_er + VB * PE;                    // WENO5 unoptimised weights, [VB][PW][3]
   // a plane is [NT][NL] for DIR 1 and [NL][NT] otherwise: the index along i is contiguous
   auto sx = [](int c, int t) -> int { return (DIR == 1) ? t * NL + c : c * NT + t; };
+  // edge planes hold cells H-1 .. H+A-1, weight planes cells 2 .. NL-3, in the same layout
+  auto ex = [](int c, int t) -> int { return (DIR == 1) ? t * (A + 1) + c - (H - 1) : (c - (H - 1)) * NT + t; };
+  auto wx = [](int c, int t) -> int { return (DIR == 1) ? t * (NL - 4) + c - 2 : (c - 2) * NT + t; };
   // item idx over VB x nc cells (from c0) x NT lines, fastest along i
   auto split = [](int idx, int c0, int nc, int& v, int& c, int& t) {
     if (DIR == 1) {
@@ -430,8 +435,8 @@ __global__ void __launch_bounds__(256) k_fluxt(Dims d, Phys ph, FaceBox fb, cons
         for (int q = 0; q < 5; q++) u5[q] = f2((float)ya[sx(ca - 2 + q, ta)], (float)yb[sx(cb - 2 + q, tb)]);
         F2 w[3];
         weno5_unopt_f2(u5 + 2, w);
-        T* wsa = s_w + (va * PL + sx(ca, ta)) * 3;
-        T* wsb = s_w + (vb * PL + sx(cb, tb)) * 3;
+        T* wsa = s_w + (va * PW + wx(ca, ta)) * 3;
+        T* wsb = s_w + (vb * PW + wx(cb, tb)) * 3;
 #pragma unroll
         for (int k = 0; k < 3; k++) {
           float a, b;
@@ -453,25 +458,25 @@ __global__ void __launch_bounds__(256) k_fluxt(Dims d, Phys ph, FaceBox fb, cons
         F2 u5[5];
 #pragma unroll
         for (int q = 0; q < 5; q++) u5[q] = f2((float)ya[sx(ca - 2 + q, ta)], (float)yb[sx(cb - 2 + q, tb)]);
-        const T* wa = s_w + va * PL * 3;
-        const T* wb = s_w + vb * PL * 3;
+        const T* wa = s_w + va * PW * 3;
+        const T* wb = s_w + vb * PW * 3;
         F2 w[3], wm[3], wp[3];
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-          w[k] = f2((float)wa[sx(ca, ta) * 3 + k], (float)wb[sx(cb, tb) * 3 + k]);
-          wm[k] = f2((float)wa[sx(ca - 2, ta) * 3 + k], (float)wb[sx(cb - 2, tb) * 3 + k]);
-          wp[k] = f2((float)wa[sx(ca + 2, ta) * 3 + k], (float)wb[sx(cb + 2, tb) * 3 + k]);
+          w[k] = f2((float)wa[wx(ca, ta) * 3 + k], (float)wb[wx(cb, tb) * 3 + k]);
+          wm[k] = f2((float)wa[wx(ca - 2, ta) * 3 + k], (float)wb[wx(cb - 2, tb) * 3 + k]);
+          wp[k] = f2((float)wa[wx(ca + 2, ta) * 3 + k], (float)wb[wx(cb + 2, tb) * 3 + k]);
         }
         F2 yl, yr;
         weno5_edges_f2(u5 + 2, w, wm, wp, yl, yr);
         float la, lb, ra, rb;
         f2split(yl, la, lb);
         f2split(yr, ra, rb);
-        s_el[va * PL + sx(ca, ta)] = (T)la;
-        s_er[va * PL + sx(ca, ta)] = (T)ra;
+        s_el[va * PE + ex(ca, ta)] = (T)la;
+        s_er[va * PE + ex(ca, ta)] = (T)ra;
         if (hasb) {
-          s_el[vb * PL + sx(cb, tb)] = (T)lb;
-          s_er[vb * PL + sx(cb, tb)] = (T)rb;
+          s_el[vb * PE + ex(cb, tb)] = (T)lb;
+          s_er[vb * PE + ex(cb, tb)] = (T)rb;
         }
       }
     } else if (LIM == HARM_LIM_WENO5) {
@@ -483,7 +488,7 @@ __global__ void __launch_bounds__(256) k_fluxt(Dims d, Phys ph, FaceBox fb, cons
         T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
         T w[3];
         weno5_unopt<T>(u5 + 2, w);
-        T* ws = s_w + (v * PL + sx(c, t)) * 3;
+        T* ws = s_w + (v * PW + wx(c, t)) * 3;
         ws[0] = w[0]; ws[1] = w[1]; ws[2] = w[2];
       }
       __syncthreads();
@@ -493,18 +498,18 @@ __global__ void __launch_bounds__(256) k_fluxt(Dims d, Phys ph, FaceBox fb, cons
         split(idx, H - 1, A + 1, v, c, t);
         const T* y = s_y + v * PL;
         T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
-        const T* ws = s_w + v * PL * 3;
+        const T* ws = s_w + v * PW * 3;
         T w[3], wm[3], wp[3];
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-          w[k] = ws[sx(c, t) * 3 + k];
-          wm[k] = ws[sx(c - 2, t) * 3 + k];
-          wp[k] = ws[sx(c + 2, t) * 3 + k];
+          w[k] = ws[wx(c, t) * 3 + k];
+          wm[k] = ws[wx(c - 2, t) * 3 + k];
+          wp[k] = ws[wx(c + 2, t) * 3 + k];
         }
         T yl, yr;
         weno5_edges<T>(u5 + 2, w, wm, wp, yl, yr);
-        s_el[v * PL + sx(c, t)] = yl;
-        s_er[v * PL + sx(c, t)] = yr;
+        s_el[v * PE + ex(c, t)] = yl;
+        s_er[v * PE + ex(c, t)] = yr;
       }
     } else if (LIM == HARM_LIM_PARA) {
       for (int idx = tid; idx < VB * (A + 1) * NT; idx += 256) {
@@ -514,8 +519,8 @@ __global__ void __launch_bounds__(256) k_fluxt(Dims d, Phys ph, FaceBox fb, cons
         T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
         T yl, yr;
         para4_cell<T>(u5 + 2, yl, yr);
-        s_el[v * PL + sx(c, t)] = yl;
-        s_er[v * PL + sx(c, t)] = yr;
+        s_el[v * PE + ex(c, t)] = yl;
+        s_er[v * PE + ex(c, t)] = yr;
       }
     } else {
       for (int idx = tid; idx < VB * (A + 1) * NT; idx += 256) {
@@ -524,15 +529,15 @@ __global__ void __launch_bounds__(256) k_fluxt(Dims d, Phys ph, FaceBox fb, cons
         const T* y = s_y + v * PL;
         const T y0 = y[sx(c, t)];
         T dq = mc_slope(y[sx(c - 1, t)], y0, y[sx(c + 1, t)]);
-        s_el[v * PL + sx(c, t)] = y0 - T(0.5) * dq;
-        s_er[v * PL + sx(c, t)] = y0 + T(0.5) * dq;
+        s_el[v * PE + ex(c, t)] = y0 - T(0.5) * dq;
+        s_er[v * PE + ex(c, t)] = y0 + T(0.5) * dq;
       }
     }
     __syncthreads();
 #pragma unroll
     for (int v = 0; v < VB; v++) {
-      pl[p0 + v] = s_er[v * PL + sx(H + lme - 1, tme)];
-      pr[p0 + v] = s_el[v * PL + sx(H + lme, tme)];
+      pl[p0 + v] = s_er[v * PE + ex(H + lme - 1, tme)];
+      pr[p0 + v] = s_el[v * PE + ex(H + lme, tme)];
     }
   }
   double dtij = 1.e300;

@@ -83,18 +83,21 @@ __global__ void __launch_bounds__(256, TmaOcc<LIM>::blocks) k_fluxt_tma(Dims d, 
   using T = float;
   using TL = FluxTile<LIM, T>;
   using TB = TmaBox<DIR, LIM>;
-  constexpr int A = TL::A, NT = TL::NT, H = TL::H, NL = TL::NL, PL = TL::PLANE;
+  constexpr int A = TL::A, NT = TL::NT, H = TL::H, NL = TL::NL, PL = TL::PLANE, PE = TL::PE, PW = TL::PW;
   static_assert(TL::VB == NPR, "the FP32 tile holds all primitives at once");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double* raw = reinterpret_cast<double*>(smem_raw);
   T* s_y = reinterpret_cast<T*>(smem_raw + TB::RAW_BYTES);
-  T* s_el = s_y + NPR * PL;
-  T* s_er = s_el + NPR * PL;
-  T* s_w = s_er + NPR * PL;
+  T* s_el = s_y + NPR * PL;   // [NPR][PE]
+  T* s_er = s_el + NPR * PE;  // [NPR][PE]
+  T* s_w = s_er + NPR * PE;   // [NPR][PW][3]
   __shared__ uint64_t bar;
   __shared__ int s_ok;
   __shared__ double red[8];
   auto sx = [](int c, int t) -> int { return (DIR == 1) ? t * NL + c : c * NT + t; };
+  // edge planes hold cells H-1 .. H+A-1, weight planes cells 2 .. NL-3, in the same layout
+  auto ex = [](int c, int t) -> int { return (DIR == 1) ? t * (A + 1) + c - (H - 1) : (c - (H - 1)) * NT + t; };
+  auto wx = [](int c, int t) -> int { return (DIR == 1) ? t * (NL - 4) + c - 2 : (c - 2) * NT + t; };
   auto split = [](int idx, int c0, int nc, int& v, int& c, int& t) {
     if (DIR == 1) {
       c = c0 + idx % nc;
@@ -188,8 +191,8 @@ __global__ void __launch_bounds__(256, TmaOcc<LIM>::blocks) k_fluxt_tma(Dims d, 
         for (int q = 0; q < 5; q++) u5[q] = f2((float)ya[sx(ca - 2 + q, ta)], (float)yb[sx(cb - 2 + q, tb)]);
         F2 w[3];
         weno5_unopt_f2(u5 + 2, w);
-        T* wsa = s_w + (va * PL + sx(ca, ta)) * 3;
-        T* wsb = s_w + (vb * PL + sx(cb, tb)) * 3;
+        T* wsa = s_w + (va * PW + wx(ca, ta)) * 3;
+        T* wsb = s_w + (vb * PW + wx(cb, tb)) * 3;
 #pragma unroll
         for (int k = 0; k < 3; k++) {
           float a, b;
@@ -211,25 +214,25 @@ __global__ void __launch_bounds__(256, TmaOcc<LIM>::blocks) k_fluxt_tma(Dims d, 
         F2 u5[5];
 #pragma unroll
         for (int q = 0; q < 5; q++) u5[q] = f2((float)ya[sx(ca - 2 + q, ta)], (float)yb[sx(cb - 2 + q, tb)]);
-        const T* wa = s_w + va * PL * 3;
-        const T* wb = s_w + vb * PL * 3;
+        const T* wa = s_w + va * PW * 3;
+        const T* wb = s_w + vb * PW * 3;
         F2 w[3], wm[3], wp[3];
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-          w[k] = f2((float)wa[sx(ca, ta) * 3 + k], (float)wb[sx(cb, tb) * 3 + k]);
-          wm[k] = f2((float)wa[sx(ca - 2, ta) * 3 + k], (float)wb[sx(cb - 2, tb) * 3 + k]);
-          wp[k] = f2((float)wa[sx(ca + 2, ta) * 3 + k], (float)wb[sx(cb + 2, tb) * 3 + k]);
+          w[k] = f2((float)wa[wx(ca, ta) * 3 + k], (float)wb[wx(cb, tb) * 3 + k]);
+          wm[k] = f2((float)wa[wx(ca - 2, ta) * 3 + k], (float)wb[wx(cb - 2, tb) * 3 + k]);
+          wp[k] = f2((float)wa[wx(ca + 2, ta) * 3 + k], (float)wb[wx(cb + 2, tb) * 3 + k]);
         }
         F2 yl, yr;
         weno5_edges_f2(u5 + 2, w, wm, wp, yl, yr);
         float la, lb, ra, rb;
         f2split(yl, la, lb);
         f2split(yr, ra, rb);
-        s_el[va * PL + sx(ca, ta)] = (T)la;
-        s_er[va * PL + sx(ca, ta)] = (T)ra;
+        s_el[va * PE + ex(ca, ta)] = (T)la;
+        s_er[va * PE + ex(ca, ta)] = (T)ra;
         if (hasb) {
-          s_el[vb * PL + sx(cb, tb)] = (T)lb;
-          s_er[vb * PL + sx(cb, tb)] = (T)rb;
+          s_el[vb * PE + ex(cb, tb)] = (T)lb;
+          s_er[vb * PE + ex(cb, tb)] = (T)rb;
         }
       }
     } else if (LIM == HARM_LIM_WENO5) {
@@ -240,7 +243,7 @@ __global__ void __launch_bounds__(256, TmaOcc<LIM>::blocks) k_fluxt_tma(Dims d, 
         T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
         T w[3];
         weno5_unopt<T>(u5 + 2, w);
-        T* ws = s_w + (v * PL + sx(c, t)) * 3;
+        T* ws = s_w + (v * PW + wx(c, t)) * 3;
         ws[0] = w[0]; ws[1] = w[1]; ws[2] = w[2];
       }
       __syncthreads();
@@ -249,18 +252,18 @@ __global__ void __launch_bounds__(256, TmaOcc<LIM>::blocks) k_fluxt_tma(Dims d, 
         split(idx, H - 1, A + 1, v, c, t);
         const T* y = s_y + v * PL;
         T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
-        const T* ws = s_w + v * PL * 3;
+        const T* ws = s_w + v * PW * 3;
         T w[3], wm[3], wp[3];
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-          w[k] = ws[sx(c, t) * 3 + k];
-          wm[k] = ws[sx(c - 2, t) * 3 + k];
-          wp[k] = ws[sx(c + 2, t) * 3 + k];
+          w[k] = ws[wx(c, t) * 3 + k];
+          wm[k] = ws[wx(c - 2, t) * 3 + k];
+          wp[k] = ws[wx(c + 2, t) * 3 + k];
         }
         T yl, yr;
         weno5_edges<T>(u5 + 2, w, wm, wp, yl, yr);
-        s_el[v * PL + sx(c, t)] = yl;
-        s_er[v * PL + sx(c, t)] = yr;
+        s_el[v * PE + ex(c, t)] = yl;
+        s_er[v * PE + ex(c, t)] = yr;
       }
     } else if (LIM == HARM_LIM_PARA) {
       for (int idx = tid; idx < NPR * (A + 1) * NT; idx += 256) {
@@ -270,8 +273,8 @@ __global__ void __launch_bounds__(256, TmaOcc<LIM>::blocks) k_fluxt_tma(Dims d, 
         T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
         T yl, yr;
         para4_cell<T>(u5 + 2, yl, yr);
-        s_el[v * PL + sx(c, t)] = yl;
-        s_er[v * PL + sx(c, t)] = yr;
+        s_el[v * PE + ex(c, t)] = yl;
+        s_er[v * PE + ex(c, t)] = yr;
       }
     } else {
       for (int idx = tid; idx < NPR * (A + 1) * NT; idx += 256) {
@@ -280,16 +283,16 @@ __global__ void __launch_bounds__(256, TmaOcc<LIM>::blocks) k_fluxt_tma(Dims d, 
         const T* y = s_y + v * PL;
         const T y0 = y[sx(c, t)];
         T dq = mc_slope(y[sx(c - 1, t)], y0, y[sx(c + 1, t)]);
-        s_el[v * PL + sx(c, t)] = y0 - T(0.5) * dq;
-        s_er[v * PL + sx(c, t)] = y0 + T(0.5) * dq;
+        s_el[v * PE + ex(c, t)] = y0 - T(0.5) * dq;
+        s_er[v * PE + ex(c, t)] = y0 + T(0.5) * dq;
       }
     }
     __syncthreads();
     T pl[NPR], pr[NPR];
 #pragma unroll
     for (int v = 0; v < NPR; v++) {
-      pl[v] = s_er[v * PL + sx(H + lme - 1, tme)];
-      pr[v] = s_el[v * PL + sx(H + lme, tme)];
+      pl[v] = s_er[v * PE + ex(H + lme - 1, tme)];
+      pr[v] = s_el[v * PE + ex(H + lme, tme)];
     }
     const int lhi = fb.hi[DIR - 1];
     const int thi = (DIR == 1) ? fb.hi[1] : fb.hi[0];
