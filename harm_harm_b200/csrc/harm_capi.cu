@@ -212,13 +212,15 @@ static int enqueue_step(harm_ctx* c, int precision, int guess, double* d_P, bool
   static const double CUf[2][4] = {{1.0, 0.0, 0.5, 0.0}, {1.0, 0.0, 1.0, 0.0}};
   static const double Cun[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 1.0, 0.5}};
   if (substep(c, precision, guess, 0, 2, d_P, d_P, c->d_pk, c->d_pflag, CUf[0], Cun[0], c->d_dtslots, with_stats)) return 1;
-  if (hp_bound(c, c->d_pk, nullptr)) return 1;
-  if (hp_fixup(c, c->d_pk, c->d_pflag)) return 1;
+  // bound_prim of p_f and of the flags in one pass (neither depends on the other), post_fixup,
+  // bound_prim (post_advance step_ch.c:288-330)
+  if (hp_bound(c, c->d_pk, c->d_pflag)) return 1;
+  if (hp_fixup(c, c->d_pk, c->d_pflag, false)) return 1;
   if (hp_bound(c, c->d_pk, nullptr)) return 1;
   if (substep(c, precision, guess, 1, 2, d_P, c->d_pk, d_P, c->d_pflag, CUf[1], Cun[1], c->d_dtslots + 3, with_stats))
     return 1;
-  if (hp_bound(c, d_P, nullptr)) return 1;
-  if (hp_fixup(c, d_P, c->d_pflag)) return 1;
+  if (hp_bound(c, d_P, c->d_pflag)) return 1;
+  if (hp_fixup(c, d_P, c->d_pflag, false)) return 1;
   if (hp_bound(c, d_P, nullptr)) return 1;
   return hp_finalize_dt(c, c->d_dt, c->d_ndt, 2);
 }

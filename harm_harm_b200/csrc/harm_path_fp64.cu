@@ -358,10 +358,10 @@ int hp_copy_ghosts(harm_ctx* c, const double* pb, double* pf) {
   return 0;
 }
 
-int hp_fixup(harm_ctx* c, double* pf, int8_t* pflag) {
+int hp_fixup(harm_ctx* c, double* pf, int8_t* pflag, bool bound_flags) {
   Dims d = dims_of(c->g);
   Phys ph = phys_of(c->g);
-  if (hp_bound(c, nullptr, pflag)) return 1;
+  if (bound_flags && hp_bound(c, nullptr, pflag)) return 1;
   CK(cudaMemsetAsync(c->d_nrec, 0, sizeof(unsigned int), c->stream));
   long long ncell = (long long)d.n1 * d.n2 * d.n3;
   k_fixup_compute<<<nblk(ncell), 256, 0, c->stream>>>(d, ph, pf, pflag, c->d_geom, (FixRec*)c->d_fixrec, c->d_nrec,

@@ -16,6 +16,7 @@ int hp_update_mixed(harm_ctx* c, const StepCoef& sc, const double* pi, const dou
 int hp_emf_to_flux_fp64(harm_ctx* c, const double* emf, double* F1, double* F2, double* F3);
 int hp_bound(harm_ctx* c, double* P, int8_t* flag);
 int hp_copy_ghosts(harm_ctx* c, const double* pb, double* pf);
-int hp_fixup(harm_ctx* c, double* pf, int8_t* pflag);
+// post_fixup; bound_flags = false when the caller has already filled the flags' ghost zones
+int hp_fixup(harm_ctx* c, double* pf, int8_t* pflag, bool bound_flags = true);
 int hp_finalize_dt(harm_ctx* c, double* dt, double* ndt_out, int nsub);
 int hp_points(harm_ctx* c, size_t n, int guess, const double* U, const double* geom, double* P, int8_t* pflag, int32_t* iters);
