@@ -355,7 +355,7 @@ __global__ void __launch_bounds__(256) k_fluxt(Dims d, Phys ph, FaceBox fb, cons
                                                unsigned long long* __restrict__ dtslot) {
   using TL = FluxTile<LIM, T>;
   constexpr int A = TL::A, NT = TL::NT, H = TL::H, NL = TL::NL, VB = TL::VB, PL = TL::PLANE, PE = TL::PE, PW = TL::PW;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   T* s_y = reinterpret_cast<T*>(smem_raw);   // [VB][plane]
   T* s_el = s_y + VB * PL;                    // left edge of each cell, [VB][PE]
   T* s_er = s_el + VB * PE;                   // right edge of each cell, [VB][PE]

@@ -105,7 +105,6 @@ int hp_update_mixed(harm_ctx* c, const StepCoef& sc, const double* pi, const dou
                     double* stats) {
   Dims d = dims_of(c->g);
   Phys ph = phys_of(c->g);
-  long long ncell = (long long)d.n1 * d.n2 * d.n3;
   const CellTile ct = cell_tile(d.n3, HARM_INVERT_LTK);
   const CellTile cct = (HARM_CONSERVED_LTK > 0 && d.n3 >= 8) ? cell_tile(d.n3, HARM_CONSERVED_LTK) : cell_linear();
   k_conserved<float><<<cell_grid(d.n1, d.n2, d.n3, cct), 256, 0, c->stream>>>(d, ph, sc, c->d_dt, pi, pb, c->d_Ff[0], c->d_Ff[1],
