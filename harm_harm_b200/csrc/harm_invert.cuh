@@ -30,11 +30,35 @@ constexpr double kBIG = 1.e100;
 constexpr double kSQRTMIN = 1.4916681462400413e-154;
 constexpr double kSMALL = 1e-300;
 
+// Division inside the Newton iteration.  By default IEEE FP64 division (the operations of the
+// C restatement, so the FP64 path matches it to round-off).  A translation unit that defines
+// HARM_INVERT_FAST_DIV before including this header (the mixed-precision path) gets the
+// reciprocal from the hardware FP64 approximation refined by two Newton-Raphson steps
+// (r <- r + r (1 - b r), quadratic convergence from the approximation's relative error), a
+// multiply, and reciprocals shared between the divisions of one residual evaluation: within
+// an ulp or two of the IEEE quotients for normal operands, with fewer FP64 instructions.
+#ifdef HARM_INVERT_FAST_DIV
+constexpr bool kFastDiv = true;
+__device__ __forceinline__ double frcp(double b) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
+  double e = fma(-b, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-b, r, 1.0);
+  return fma(r, e, r);
+}
+__device__ __forceinline__ double fdiv(double a, double b) { return a * frcp(b); }
+#else
+constexpr bool kFastDiv = false;
+__device__ __forceinline__ double frcp(double b) { return 1.0 / b; }
+__device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
+#endif
+
 __device__ __forceinline__ double utsq_calc(double W, const InvC& c) {
-  double SoW = c.QdotB / W;
+  double SoW = fdiv(c.QdotB, W);
   double top = c.Qtsq + (c.Bsq + 2.0 * W) * SoW * SoW;
   double bot = (c.Bsq * c.Bsq - c.Qtsq) + 2.0 * c.Bsq * W + W * W - SoW * SoW * (c.Bsq + 2.0 * W);
-  return top / bot;
+  return fdiv(top, bot);
 }
 __device__ __forceinline__ bool vsqgtr1(double W, const InvC& c) {
   return W * W * W * (W + 2. * c.Bsq) - c.QdotBsq * (2. * W + c.Bsq) <= W * W * (c.Qtsq - c.Bsq * c.Bsq);
@@ -48,6 +72,32 @@ __device__ __forceinline__ bool coldgrhd(double Qtsq, double D, double& Wp) {
 
 // residual, derivative and Newton step of the hot (E') or cold (P^2) equation
 __device__ __forceinline__ void inv_func(double Wp, const InvC& c, double& resid, double& jac, double& dx, double& f) {
+  if (kFastDiv && !c.cold) {
+    // the same residual and derivative with the divisors' reciprocals formed once
+    const double W = Wp + c.D, iW = frcp(W), X = c.Bsq + W + kSMALL, iX = frcp(X), iX2 = iX * iX, iX3 = iX2 * iX;
+    const double utsq = utsq_calc(W, c);
+    const double gammasq = 1.0 + utsq, gamma = sqrt(gammasq), igsq = frcp(gammasq);
+    const double wmrho0 = (Wp - c.D * utsq * frcp(1.0 + gamma)) * igsq;
+    if (utsq < -0.9 * c.utsq_too_big || utsq != utsq) {
+      resid = -kVERYBIG; jac = 0.0; dx = kVERYBIG; f = 0.5 * resid * resid;
+      return;
+    }
+    const double gm1 = c.gam - 1.0, dpdchi = gm1 / c.gam;
+    const double pofchi = dpdchi * wmrho0;
+    const double BQ = c.Bsq * c.Qtsq - c.QdotBsq;
+    double Ep = c.Qdotnp + Wp - pofchi + 0.5 * c.Bsq + 0.5 * BQ * iX2;
+    if (pofchi != pofchi || Ep != Ep) Ep = -kVERYBIG;
+    const double Xd = c.Bsq + W, iW3 = iW * iW * iW, iXd = frcp(Xd), iXd3 = iXd * iXd * iXd;
+    const double dvsq = -2.0 * iXd3 * (c.Qtsq + c.QdotBsq * (3.0 * W * Xd + c.Bsq * c.Bsq) * iW3);
+    const double dwmrho0dvsq = (c.D * (gamma * 0.5 - 1.0) - Wp), drho0dvsq = -c.D * gamma * 0.5;
+    const double dpdW = igsq * dpdchi;
+    const double dpdvsq = drho0dvsq * 0.0 + dwmrho0dvsq * dpdchi;
+    const double dpdWp = dpdW + dpdvsq * dvsq;
+    double dE = (1.0 - dpdWp) - BQ * iX3;
+    if (dvsq != dvsq || dpdW != dpdW || dpdvsq != dpdvsq || dpdWp != dpdWp || dE != dE) dE = 0.0;
+    resid = Ep; jac = dE; dx = -Ep * frcp(dE); f = 0.5 * Ep * Ep;
+    return;
+  }
   if (!c.cold) {
     double W = Wp + c.D, X = c.Bsq + W + kSMALL, X2 = X * X, X3 = X2 * X;
     double utsq = utsq_calc(W, c);
@@ -86,7 +136,7 @@ __device__ __forceinline__ void validate_Wp(double Wpold, double& Wpnew, const I
     coldgrhd(c.Qtsq, c.D, Wp);
     Wpnew = Wp * 10.0;
   }
-  Wpnew = (fabs(Wpnew / c.w1) > c.gsq_too_big) ? 0.5 * (Wpold + Wpnew) : Wpnew;
+  Wpnew = (fabs(fdiv(Wpnew, c.w1)) > c.gsq_too_big) ? 0.5 * (Wpold + Wpnew) : Wpnew;
 }
 
 __device__ __forceinline__ bool ultrarel(double x0, const InvC& c) {
@@ -125,7 +175,7 @@ static __device__ int newton(int8_t& flag, double& xio, const InvC& c, int& lntr
       }
     }
     x += damp * dx;
-    errx = (c.w0 == 0.) ? fabs(dx_old) : fabs(dx_old / fmax(fabs(c.w0), fabs(x)));
+    errx = (c.w0 == 0.) ? fabs(dx_old) : fabs(fdiv(dx_old, fmax(fabs(c.w0), fabs(x))));
     validate_Wp(x_old, x, c);
     dx_old = dx;
     if (errcheck(errx, x, c) && doing_extra == 0 && extracheck(x, c) > 0) doing_extra = 1;

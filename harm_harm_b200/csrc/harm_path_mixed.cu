@@ -1,5 +1,7 @@
 // harm_path_mixed.cu -- mixed-precision path of the step: FP32 reconstruction, HLL and
 // flux-CT; FP64 conserved update, sources and inversion (compiled with FMA contraction).
+// the inversion of this path shares reciprocals between its FP64 divisions (harm_invert.cuh)
+#define HARM_INVERT_FAST_DIV 1
 #include <algorithm>
 #include <cudaTypedefs.h>
 #include <mutex>
