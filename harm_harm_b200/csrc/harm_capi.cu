@@ -90,6 +90,13 @@ extern "C" int harm_b200_create(const harm_grid* g, const double* geom_h, const 
     // its tile loop, halving the warps that hide the face physics' latency), so it is opt-in.
     const char* e = getenv("HARM_B200_FLUX_STAGING");
     c->flux_tma = (e && strcmp(e, "tma") == 0);
+    // learned start: the mma.sync network as a kernel ahead of the inversion (default), the
+    // tcgen05 network as a kernel ahead of it ("tc") or inside the inversion kernel
+    // ("tc-fused").  The network's arithmetic is the same; on B200 the mma.sync kernel measured
+    // fastest (its activations stay in registers; the tcgen05 kernels stage each layer's
+    // activations through shared memory and synchronise a warpgroup per layer).
+    const char* m = getenv("HARM_B200_MLP_ENGINE");
+    c->mlp_tc = (m && strcmp(m, "tc") == 0) ? 1 : (m && strcmp(m, "tc-fused") == 0) ? 2 : 0;
     CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
   }
   CK(cudaMemset(c->d_dtslots, 0xFF, 6 * sizeof(unsigned long long)));
@@ -171,7 +178,8 @@ static int check_status(harm_ctx* c) {
   CK(cudaMemcpy(&st, c->d_status, sizeof(st), cudaMemcpyDeviceToHost));
   if (st) {
     CK(cudaMemset(c->d_status, 0, sizeof(st)));
-    return seterr_msg("a flux tile's TMA load did not complete (the step's fluxes are incomplete)", 5);
+    if (st & 1u) return seterr_msg("a flux tile's TMA load did not complete (the step's fluxes are incomplete)", 5);
+    return seterr_msg("a tensor-core MMA of the learned start did not complete (the step's inversion is incomplete)", 5);
   }
   return 0;
 }

@@ -824,6 +824,55 @@ __global__ void __launch_bounds__(256, HARM_CONSERVED_BLOCKS) k_conserved(Dims d
 // GUESS: the Newton iteration starts from wpg[t] (the learned start, k_mlp_guess) where it is
 // positive; a cell whose learned start does not converge starts again from the
 // previous-state W', exactly as without GUESS (counted in stats[2]).
+// The common-path inversion of active cell (i, j, k), as described above; w is the learned
+// start (GUESS), iters_d and fb_d receive the Newton iterations and the fallback count.
+template <bool GUESS>
+__device__ __forceinline__ void invert_cell(const Dims& d, const Phys& ph, const double* __restrict__ U,
+                                            const double* __restrict__ pb, double* __restrict__ pf,
+                                            int8_t* __restrict__ pflag, const double* __restrict__ geom,
+                                            const double* __restrict__ aux, unsigned int* __restrict__ rare,
+                                            unsigned int* __restrict__ nrare, int i, int j, int k, double w,
+                                            double& iters_d, double& fb_d) {
+  const long long t = i + (long long)d.n1 * (j + (long long)d.n2 * k);  // active-cell index
+  int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
+  const size_t id = cidx(d, ii, jj, kk), c2 = (size_t)jj * d.n1e + ii;
+  Geo<double> g;
+  load_geo<double, double>(geom, d.plane, c2, g);
+  double Ugf[NPR], pr[NPR];
+#pragma unroll
+  for (int p = 0; p < NPR; p++) { Ugf[p] = U[(size_t)p * d.cells + id] * g.igdet; pr[p] = pb[(size_t)p * d.cells + id]; }
+  int8_t flag = 0;
+  int it = 0;
+  if (GUESS) {
+    JonSetup s;
+    jon_prepare(false, Ugf, g, pr, ph.gam, ph.gammafail, s);
+    jon_solve(s, (w > 0.0) ? w : s.Wp_prev, pr, flag, it);
+    if (flag != 0 && w > 0.0) {  // the learned start did not converge: the plain start
+      fb_d += 1.0;
+      jon_solve(s, s.Wp_prev, pr, flag, it);
+    }
+  } else {
+    utoprim_jon(false, Ugf, g, flag, pr, ph.gam, ph.gammafail, it, false, 0.0);
+  }
+  iters_d += (double)it;
+  bool defer = (flag != 0);
+  if (!defer) {
+    double rhofl = __ldg(aux + (size_t)HARM_AUX_RHOFLOOR * d.plane + c2);
+    double ufl = __ldg(aux + (size_t)HARM_AUX_UFLOOR * d.plane + c2);
+    rhofl = (rhofl < kSMALL) ? kSMALL : rhofl;
+    ufl = (ufl < kSMALL) ? kSMALL : ufl;
+    defer = (rhofl > pr[HARM_RHO]) || (ufl > pr[HARM_UU]);
+    if (!defer) limit_gamma<double>(ph.gammamax, pr, g);
+  }
+  if (defer) {
+    unsigned int slot = atomicAdd(nrare, 1u);
+    rare[slot] = (unsigned int)t;
+  }
+  pflag[id] = flag;
+#pragma unroll
+  for (int p = 0; p < NPR; p++) pf[(size_t)p * d.cells + id] = pr[p];
+}
+
 template <int PATH, bool GUESS = false>
 __global__ void __launch_bounds__(256, HARM_INVERT_BLOCKS) k_invert(Dims d, Phys ph, const double* __restrict__ U,
                                                    const double* __restrict__ pb, double* __restrict__ pf,
@@ -834,45 +883,8 @@ __global__ void __launch_bounds__(256, HARM_INVERT_BLOCKS) k_invert(Dims d, Phys
   double iters_d = 0.0, fb_d = 0.0;
   int i, j, k;
   if (tile_cell(d.n1, d.n2, d.n3, ct, blockIdx.x, blockIdx.y, blockIdx.z, i, j, k)) {
-    const long long t = i + (long long)d.n1 * (j + (long long)d.n2 * k);  // active-cell index
-    int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
-    const size_t id = cidx(d, ii, jj, kk), c2 = (size_t)jj * d.n1e + ii;
-    Geo<double> g;
-    load_geo<double, double>(geom, d.plane, c2, g);
-    double Ugf[NPR], pr[NPR];
-#pragma unroll
-    for (int p = 0; p < NPR; p++) { Ugf[p] = U[(size_t)p * d.cells + id] * g.igdet; pr[p] = pb[(size_t)p * d.cells + id]; }
-    int8_t flag = 0;
-    int it = 0;
-    if (GUESS) {
-      JonSetup s;
-      jon_prepare(false, Ugf, g, pr, ph.gam, ph.gammafail, s);
-      const double w = wpg[t];
-      jon_solve(s, (w > 0.0) ? w : s.Wp_prev, pr, flag, it);
-      if (flag != 0 && w > 0.0) {  // the learned start did not converge: the plain start
-        fb_d = 1.0;
-        jon_solve(s, s.Wp_prev, pr, flag, it);
-      }
-    } else {
-      utoprim_jon(false, Ugf, g, flag, pr, ph.gam, ph.gammafail, it, false, 0.0);
-    }
-    iters_d = (double)it;
-    bool defer = (flag != 0);
-    if (!defer) {
-      double rhofl = __ldg(aux + (size_t)HARM_AUX_RHOFLOOR * d.plane + c2);
-      double ufl = __ldg(aux + (size_t)HARM_AUX_UFLOOR * d.plane + c2);
-      rhofl = (rhofl < kSMALL) ? kSMALL : rhofl;
-      ufl = (ufl < kSMALL) ? kSMALL : ufl;
-      defer = (rhofl > pr[HARM_RHO]) || (ufl > pr[HARM_UU]);
-      if (!defer) limit_gamma<double>(ph.gammamax, pr, g);
-    }
-    if (defer) {
-      unsigned int slot = atomicAdd(nrare, 1u);
-      rare[slot] = (unsigned int)t;
-    }
-    pflag[id] = flag;
-#pragma unroll
-    for (int p = 0; p < NPR; p++) pf[(size_t)p * d.cells + id] = pr[p];
+    const double w = GUESS ? wpg[i + (long long)d.n1 * (j + (long long)d.n2 * k)] : 0.0;
+    invert_cell<GUESS>(d, ph, U, pb, pf, pflag, geom, aux, rare, nrare, i, j, k, w, iters_d, fb_d);
   }
   if (stats) {
     warp_add_atomic(iters_d, stats + 0);

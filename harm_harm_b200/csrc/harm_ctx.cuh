@@ -36,15 +36,20 @@ struct harm_ctx {
   double* h_scal;   // pinned host mirror
   double* d_Pdev;   // device state used by the host-buffer entry point
   // learned guess
-  float* d_mlp;        // inference parameters (BF16 packed as float words) + normalisation
+  float* d_mlp;        // inference records (MlpPacked for mma.sync, then MlpTc for tcgen05)
   double* d_wpg;       // learned starting W' of each active cell (k_mlp_guess)
   float* d_mlp_master; // FP32 master parameters
   float* d_mlp_adam;   // Adam moments
   float* d_mlp_work;   // training workspace
   size_t mlp_work_n;
   int mlp_step;
-  unsigned int* d_status; // device error word (bit 0: a TMA tile wait timed out)
+  unsigned int* d_status; // device error word (bit 0: a TMA tile wait timed out, bit 1: a
+                          // tensor-core MMA wait of the learned start timed out)
   int flux_tma;            // stage the FP32 flux tiles with TMA (HARM_B200_FLUX_STAGING=tma)
+  int mlp_tc;              // learned start: 0 mma.sync network kernel ahead of the inversion
+                           // (default), 1 tcgen05 network kernel ahead of it
+                           // (HARM_B200_MLP_ENGINE=tc), 2 tcgen05 inside the inversion
+                           // kernel (=tc-fused)
   int num_sms;
   unsigned long long launches;  // kernels launched by this context
 };

@@ -17,13 +17,14 @@
 // W3[64][64] b3[64] W4[64][2] b4[2], W[in][out].  Inference uses a packed copy: BF16 weights
 // in the register-fragment order of mma.sync m16n8k16 (row.col) so that each lane loads
 // the B fragments of two adjacent tiles with one 16-byte shared-memory read, FP32 biases and
-// the normalisation.
+// the normalisation; the weights and biases of layers 1-3 are halved (see mlp_tanh).
 // A warp evaluates its 32 cells as two 16-row tiles; the FP32 accumulator fragment of one
 // layer is, after SiLU and conversion to BF16, exactly the A fragment of the next layer,
 // so activations never leave registers.
 #pragma once
 #include <cuda_bf16.h>
 #include "harm_invert.cuh"
+#include "harm_weno_f32x2.cuh"
 
 namespace hb {
 
@@ -86,19 +87,28 @@ __device__ __forceinline__ void mlp_targets(double Wp, const InvC& c, float* t) 
   t[1] = (float)log1p(utsq > 0.0 ? utsq : 0.0);
 }
 
-// SiLU of the inference: x sigmoid(x) = h + h tanh(h), h = x/2, with the hardware tanh
-// approximation (one special-function operation; its error, about 2^-11, is below the BF16
-// rounding the activation receives next)
-__device__ __forceinline__ float mlp_silu(float x) {
-  const float h = 0.5f * x;
+// SiLU of the inference.  x sigmoid(x) = h + h tanh(h) with h = x/2; the packed records hold
+// the weights and biases of layers 1-3 halved (exact in BF16 and FP32: a power of two), so
+// the accumulators are h itself.  Hardware tanh approximation (one special-function operation;
+// its error, about 2^-11, is below the BF16 rounding the activation receives next), then one
+// packed FP32x2 FMA for two activations.
+__device__ __forceinline__ float mlp_tanh(float h) {
   float t;
   asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(h));
-  return fmaf(h, t, h);
+  return t;
 }
-
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
   __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);  // .x = lo (low half), .y = hi
   return *reinterpret_cast<uint32_t*>(&v);
+}
+
+// two activations from their halves h, as BF16x2 (the first in the low half)
+__device__ __forceinline__ uint32_t mlp_silu2_bf16(F2 h) {
+  float h0, h1;
+  f2split(h, h0, h1);
+  float s0, s1;
+  f2split(ffma2(h, f2(mlp_tanh(h0), mlp_tanh(h1)), h), s0, s1);
+  return pack_bf16x2(s0, s1);
 }
 
 __device__ __forceinline__ void mma_bf16_16816(float* c, const uint32_t* a, uint2 b) {
@@ -118,10 +128,10 @@ struct MlpWarpScratch {
 
 // SiLU of two accumulator tiles (n-tiles 2q, 2q+1) as the A fragment of k-tile q
 __device__ __forceinline__ void mlp_act_to_a(const float* c0, const float* c1, uint32_t* a) {
-  a[0] = pack_bf16x2(mlp_silu(c0[0]), mlp_silu(c0[1]));
-  a[1] = pack_bf16x2(mlp_silu(c0[2]), mlp_silu(c0[3]));
-  a[2] = pack_bf16x2(mlp_silu(c1[0]), mlp_silu(c1[1]));
-  a[3] = pack_bf16x2(mlp_silu(c1[2]), mlp_silu(c1[3]));
+  a[0] = mlp_silu2_bf16(f2(c0[0], c0[1]));
+  a[1] = mlp_silu2_bf16(f2(c0[2], c0[3]));
+  a[2] = mlp_silu2_bf16(f2(c1[0], c1[1]));
+  a[3] = mlp_silu2_bf16(f2(c1[2], c1[3]));
 }
 
 // Evaluate the network for the 32 cells of this warp.  All 32 lanes must call it (lanes

@@ -17,6 +17,7 @@
 #include <vector>
 #include "harm_common.cuh"
 #include "harm_mlp.cuh"
+#include "harm_mlp_tc.cuh"
 
 int hb_setmsg(const char* msg, int code);
 
@@ -287,16 +288,55 @@ __global__ void k_mlp_pack(const float* __restrict__ params, const float* __rest
     else if (tile < MLP_TILE_L4) { woff = MLP_OFF_W3; K = MLP_H; N = MLP_H; kt = (tile - MLP_TILE_L3) >> 3; nt = (tile - MLP_TILE_L3) & 7; }
     else { woff = MLP_OFF_W4; K = MLP_H; N = MLP_OUT; kt = tile - MLP_TILE_L4; nt = 0; }
     const int k0 = kt * 16 + 2 * (lane & 3), n = nt * 8 + (lane >> 2);
-    auto W = [&](int k) -> float { return (k < K && n < N) ? params[woff + k * N + n] : 0.0f; };
+    const float scale = (tile < MLP_TILE_L4) ? 0.5f : 1.0f;  // layers 1-3 halved (mlp_tanh)
+    auto W = [&](int k) -> float { return (k < K && n < N) ? scale * params[woff + k * N + n] : 0.0f; };
     uint32_t* f = reinterpret_cast<uint32_t*>(&out->frag[tile >> 1][lane]) + 2 * (tile & 1);
     f[0] = pack_bf16x2(W(k0), W(k0 + 1));
     f[1] = pack_bf16x2(W(k0 + 8), W(k0 + 9));
   }
   if (t < MLP_NBIAS) {
     float b = 0.0f;
-    if (t < MLP_H) b = params[MLP_OFF_B1 + t];
-    else if (t < 2 * MLP_H) b = params[MLP_OFF_B2 + t - MLP_H];
-    else if (t < 3 * MLP_H) b = params[MLP_OFF_B3 + t - 2 * MLP_H];
+    if (t < MLP_H) b = 0.5f * params[MLP_OFF_B1 + t];
+    else if (t < 2 * MLP_H) b = 0.5f * params[MLP_OFF_B2 + t - MLP_H];
+    else if (t < 3 * MLP_H) b = 0.5f * params[MLP_OFF_B3 + t - 2 * MLP_H];
+    else if (t < 3 * MLP_H + MLP_OUT) b = params[MLP_OFF_B4 + t - 3 * MLP_H];
+    out->bias[t] = b;
+  }
+  if (t < MLP_NNORM) out->norm[t] = norm[t];
+  if (t == 0) {
+    out->start_bias = start_bias;
+    out->pad[0] = out->pad[1] = out->pad[2] = 0.0f;
+  }
+}
+
+// BF16 B operands in the tensor-core canonical layout of harm_mlp_tc.cuh (one 16-byte chunk of
+// 8 K-consecutive weights per thread), biases, normalisation, start bias
+__global__ void k_mlp_pack_tc(const float* __restrict__ params, const float* __restrict__ norm, float start_bias,
+                              MlpTc* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < TC_WBYTES / 16) {
+    const int off = t * 16;
+    int base, kc, woff, K, N;
+    if (off < TC_W2) { base = TC_W1; kc = 2; woff = MLP_OFF_W1; K = MLP_IN; N = MLP_H; }
+    else if (off < TC_W3) { base = TC_W2; kc = 8; woff = MLP_OFF_W2; K = MLP_H; N = MLP_H; }
+    else if (off < TC_W4) { base = TC_W3; kc = 8; woff = MLP_OFF_W3; K = MLP_H; N = MLP_H; }
+    else { base = TC_W4; kc = 8; woff = MLP_OFF_W4; K = MLP_H; N = MLP_OUT; }
+    const int rel = off - base, cm = rel >> 7;
+    const int n = (cm / kc) * 8 + ((rel & 127) >> 4), k0 = (cm % kc) * 8;  // tc_off(n, k0, kc) == rel
+    const float scale = (base < TC_W4) ? 0.5f : 1.0f;  // layers 1-3 halved (mlp_tanh)
+    auto W = [&](int k) -> float { return (k < K && n < N) ? scale * params[woff + k * N + n] : 0.0f; };
+    uint4 v;
+    v.x = pack_bf16x2(W(k0), W(k0 + 1));
+    v.y = pack_bf16x2(W(k0 + 2), W(k0 + 3));
+    v.z = pack_bf16x2(W(k0 + 4), W(k0 + 5));
+    v.w = pack_bf16x2(W(k0 + 6), W(k0 + 7));
+    out->w[t] = v;
+  }
+  if (t < MLP_NBIAS) {
+    float b = 0.0f;
+    if (t < MLP_H) b = 0.5f * params[MLP_OFF_B1 + t];
+    else if (t < 2 * MLP_H) b = 0.5f * params[MLP_OFF_B2 + t - MLP_H];
+    else if (t < 3 * MLP_H) b = 0.5f * params[MLP_OFF_B3 + t - 2 * MLP_H];
     else if (t < 3 * MLP_H + MLP_OUT) b = params[MLP_OFF_B4 + t - 3 * MLP_H];
     out->bias[t] = b;
   }
@@ -445,28 +485,71 @@ extern "C" int harm_b200_mlp_train(harm_ctx* c, size_t n, const float* d_feat, c
 extern "C" int harm_b200_mlp_set(harm_ctx* c, const float* d_params, const float* d_norm, double start_bias) {
   if (!c || !d_params || !d_norm) return hb_setmsg("null argument", 1);
   if (!c->d_mlp) {
-    CK(cudaMalloc(&c->d_mlp, sizeof(MlpPacked)));
+    CK(cudaMalloc(&c->d_mlp, sizeof(MlpPacked) + sizeof(MlpTc)));
   }
   if (!c->d_wpg) {
     CK(cudaMalloc(&c->d_wpg, (size_t)c->g.n1 * c->g.n2 * c->g.n3 * sizeof(double)));
   }
   k_mlp_pack<<<nblk(MLP_TILES * 32), 256, 0, c->stream>>>(d_params, d_norm, (float)start_bias,
                                                          reinterpret_cast<MlpPacked*>(c->d_mlp));
-  c->launches++;
+  k_mlp_pack_tc<<<nblk(TC_WBYTES / 16), 256, 0, c->stream>>>(d_params, d_norm, (float)start_bias, mlp_tc_of(c));
+  c->launches += 2;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
   c->mlp_step = 1;  // a packed network is present
   return 0;
 }
 
+// Network outputs for n feature rows (the tensor-core counterpart of k_mlp_predict).
+__global__ void __launch_bounds__(256) k_mlp_predict_tc(size_t n, const float* __restrict__ feat,
+                                                        const MlpTc* __restrict__ mlp, float* __restrict__ out,
+                                                        unsigned int* __restrict__ status) {
+  extern __shared__ __align__(128) unsigned char tc_smem[];
+  MlpTcBlock& B = *reinterpret_cast<MlpTcBlock*>(tc_smem);
+  mlp_tc_begin(B, mlp);
+  const int wg = threadIdx.x >> 7, r = threadIdx.x & 127;
+  const long long ntiles = (long long)((n + 127) / 128);
+  TcState st = {0u, false};
+  for (long long tile = 2ll * blockIdx.x + wg; tile < ntiles; tile += 2ll * gridDim.x) {
+    const size_t t = (size_t)tile * 128 + r;
+    const bool valid = t < n;
+    float f[MLP_IN], x[MLP_IN];
+#pragma unroll
+    for (int i = 0; i < MLP_IN; i++) f[i] = valid ? feat[t * MLP_IN + i] : 0.0f;
+    mlp_tc_standardise(B.net, f, valid, x);
+    float y[MLP_OUT];
+    if (!mlp_tc_eval(B, x, st, status, y)) break;
+    if (valid) {
+      out[t * MLP_OUT + 0] = y[0];
+      out[t * MLP_OUT + 1] = y[1];
+    }
+  }
+  mlp_tc_end(B, st);
+}
+
 extern "C" int harm_b200_mlp_predict(harm_ctx* c, size_t n, const float* d_feat, float* d_out) {
   if (!c || !d_feat || !d_out) return hb_setmsg("null argument", 1);
   if (!c->d_mlp || !c->mlp_step) return hb_setmsg("no network set (harm_b200_mlp_set)", 3);
   if (n == 0) return 0;
-  const unsigned int nb = (unsigned int)std::min<size_t>((n + 255) / 256, (size_t)4 * 148);
-  k_mlp_predict<<<nb, 256, 0, c->stream>>>(n, d_feat, reinterpret_cast<const MlpPacked*>(c->d_mlp), d_out);
+  if (c->mlp_tc) {
+    static unsigned configured = 0;
+    static int per_sm = 1;
+    if (int rc = tc_blocks_per_sm(c, k_mlp_predict_tc, configured, per_sm)) return rc;
+    const size_t pairs = (n + 255) / 256;
+    const unsigned int nb = (unsigned int)std::min<size_t>(pairs, (size_t)per_sm * c->num_sms);
+    k_mlp_predict_tc<<<nb, 256, sizeof(MlpTcBlock), c->stream>>>(n, d_feat, mlp_tc_of(c), d_out, c->d_status);
+  } else {
+    const unsigned int nb = (unsigned int)std::min<size_t>((n + 255) / 256, (size_t)4 * 148);
+    k_mlp_predict<<<nb, 256, 0, c->stream>>>(n, d_feat, reinterpret_cast<const MlpPacked*>(c->d_mlp), d_out);
+  }
   c->launches++;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
+  unsigned int st = 0;
+  CK(cudaMemcpy(&st, c->d_status, sizeof(st), cudaMemcpyDeviceToHost));
+  if (st) {
+    CK(cudaMemset(c->d_status, 0, sizeof(st)));
+    return hb_setmsg("a tensor-core MMA of the network did not complete", 5);
+  }
   return 0;
 }

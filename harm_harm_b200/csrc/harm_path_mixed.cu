@@ -6,6 +6,7 @@
 #include <cudaTypedefs.h>
 #include <mutex>
 #include "harm_common.cuh"
+#include "harm_mlp_tc.cuh"
 #include "harm_flux_tma.cuh"
 #include "harm_paths.h"
 
@@ -112,19 +113,27 @@ int hp_update_mixed(harm_ctx* c, const StepCoef& sc, const double* pi, const dou
   k_conserved<float><<<cell_grid(d.n1, d.n2, d.n3, cct), 256, 0, c->stream>>>(d, ph, sc, c->d_dt, pi, pb, c->d_Ff[0], c->d_Ff[1],
                                                          c->d_Ff[2], c->d_emff, c->d_geom, c->d_conn, c->d_U, cct);
   CK(cudaMemsetAsync(c->d_nrare, 0, sizeof(unsigned int), c->stream));
-  if (sc.guess == HARM_GUESS_MLP) {
-    k_mlp_guess<1><<<3 * 148, 256, 0, c->stream>>>(d, c->d_U, c->d_geom, c->d_wpg,
-                                                    reinterpret_cast<const MlpPacked*>(c->d_mlp), ct);
+  if (sc.guess == HARM_GUESS_MLP && c->mlp_tc == 2) {
+    if (int rc = launch_invert_tc<1>(c, d, ph, pb, pf, pflag, stats)) return rc;
+  } else if (sc.guess == HARM_GUESS_MLP) {
+    if (c->mlp_tc == 1) {
+      if (int rc = launch_mlp_guess_tc<1>(c, d)) return rc;
+    } else {
+      k_mlp_guess<1><<<3 * 148, 256, 0, c->stream>>>(d, c->d_U, c->d_geom, c->d_wpg,
+                                                      reinterpret_cast<const MlpPacked*>(c->d_mlp), ct);
+      c->launches++;
+    }
     k_invert<1, true><<<cell_grid(d.n1, d.n2, d.n3, ct), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag,
                                                           c->d_geom, c->d_aux, c->d_rare, c->d_nrare, stats, ct, c->d_wpg);
     c->launches++;
   } else {
     k_invert<1><<<cell_grid(d.n1, d.n2, d.n3, ct), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom,
                                                     c->d_aux, c->d_rare, c->d_nrare, stats, ct);
+    c->launches++;
   }
   k_invert_rare<1><<<2 * 148, 128, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
                                                      c->d_nrare, stats);
-  c->launches += 3;
+  c->launches += 2;
   CK(cudaGetLastError());
   return 0;
 }

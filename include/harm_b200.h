@@ -151,7 +151,15 @@ typedef struct harm_ctx harm_ctx;
 
 /* Create a context on CUDA device `device`: uploads the metric tables (once, as
    set_grid does once) and allocates the scratch of the step (fluxes, EMFs, U arrays).
-   The caller owns the primitive arrays. */
+   The caller owns the primitive arrays.  Read at creation, from the environment:
+     HARM_B200_FLUX_STAGING=tma   stage the FP32 flux tiles with TMA tensor loads
+                                  (default: coalesced loads; same arithmetic)
+     HARM_B200_MLP_ENGINE=tc      learned start on tcgen05 tensor cores, in a kernel ahead
+                                  of the inversion
+     HARM_B200_MLP_ENGINE=tc-fused  the same inside the inversion kernel
+                                  (default: mma.sync tensor cores, in a kernel ahead of the
+                                  inversion; same network, same results to the BF16
+                                  rounding of its activations) */
 int harm_b200_create(const harm_grid *g, const double *geom_h, const double *conn_h,
                      const double *aux_h, int device, harm_ctx **out);
 int harm_b200_destroy(harm_ctx *ctx);
@@ -285,7 +293,7 @@ int harm_b200_mlp_set(harm_ctx *ctx, const float *d_params, const float *d_norm,
                       double start_bias);
 
 /* Outputs d_out[n][2] (de-standardised) of the packed network for features d_feat[n][10],
-   on the tensor cores as inside the inversion. */
+   on the tensor cores of the context's engine (HARM_B200_MLP_ENGINE), as in the inversion. */
 int harm_b200_mlp_predict(harm_ctx *ctx, size_t n, const float *d_feat, float *d_out);
 
 /* Largest grid (extended cells n1e*n2e*n3e) harm_b200_fluxcalc_noalloc accepts: its EMF
