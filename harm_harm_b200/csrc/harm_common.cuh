@@ -701,6 +701,7 @@ __device__ __forceinline__ double dU_cell(const Dims& d, int ii, int jj, int kk,
 }
 
 // connection source (source_conn): dU^{UU+l} = gdet [ T^j_k Gamma^k_{l j} - rho u^j Gamma^t_{l j} ]
+template <bool LDG = true>
 __device__ __forceinline__ void source_conn(const double* pr, const State<double>& q, const Geo<double>& g,
                                             const double* __restrict__ conn, size_t plane, size_t c2, double* dUg) {
   double mhd[4][4];
@@ -717,9 +718,9 @@ __device__ __forceinline__ void source_conn(const double* pr, const State<double
 #pragma unroll
     for (int j = 0; j < 4; j++)
 #pragma unroll
-      for (int k = 0; k < 4; k++) s += mhd[j][k] * __ldg(conn + (size_t)((k * 4 + l) * 4 + j) * plane + c2);
+      for (int k = 0; k < 4; k++) s += mhd[j][k] * tab_ld<LDG>(conn + (size_t)((k * 4 + l) * 4 + j) * plane + c2);
 #pragma unroll
-    for (int j = 0; j < 4; j++) s += -pr[HARM_RHO] * q.ucon[j] * __ldg(conn + (size_t)((0 * 4 + l) * 4 + j) * plane + c2);
+    for (int j = 0; j < 4; j++) s += -pr[HARM_RHO] * q.ucon[j] * tab_ld<LDG>(conn + (size_t)((0 * 4 + l) * 4 + j) * plane + c2);
     dUg[HARM_UU + l] = g.gdet * s;
   }
   dUg[HARM_RHO] = g.gdet * 0.0;
@@ -764,6 +765,7 @@ __device__ __forceinline__ int fixup1zone(double* pr, const Geo<double>& g, doub
 
 // Conserved update of one substep: U_i = primtoU(p_i), flux divergence (field fluxes from
 // the EMFs), connection source of p_b, RK combination; U (UEVOLVE) to global memory.
+// (One pass, in the reference's order of operations: the FP64 path.)
 // minimum resident blocks per SM the FP64 kernels are compiled for (register budget)
 #ifndef HARM_CONSERVED_BLOCKS
 #define HARM_CONSERVED_BLOCKS 2
@@ -779,19 +781,45 @@ __device__ __forceinline__ int fixup1zone(double* pr, const Geo<double>& g, doub
 #define HARM_INVERT_BLOCKS 3
 #endif
 
-template <typename T>
+// STAGE (the conserved-update kernels): cell tiles of 16 i x 16 k at one j (CellTile lti = 4);
+// the connection and CENT metric records of the tile's 16 (i,j) columns are staged in shared
+// memory once per block (each serves 16 cells) instead of being loaded by every cell, which
+// also frees the registers the per-cell loads held in flight.
+constexpr int kStageTI = 16;
+constexpr int kStageF = 64 + HARM_NGF;  // connection entries, then the metric record
+template <bool STAGE>
+__device__ __forceinline__ void stage_conn_geom(const Dims& d, const double* __restrict__ geom,
+                                                const double* __restrict__ conn, double* s_tab) {
+  if constexpr (STAGE) {
+    const int i0 = blockIdx.x * kStageTI, jj0 = blockIdx.y + d.ng;
+    for (int e = threadIdx.x; e < kStageF * kStageTI; e += blockDim.x) {
+      const int f = e / kStageTI, il = e % kStageTI;
+      const int ii0 = min(i0 + il, d.n1 - 1) + d.ng;
+      const size_t c = (size_t)jj0 * d.n1e + ii0;
+      s_tab[e] = (f < 64) ? __ldg(conn + (size_t)f * d.plane + c) : __ldg(geom + (size_t)(f - 64) * d.plane + c);
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T, bool STAGE = false>
 __global__ void __launch_bounds__(256, HARM_CONSERVED_BLOCKS) k_conserved(Dims d, Phys ph, StepCoef sc, const double* __restrict__ dtp,
                                                       const double* __restrict__ pi, const double* __restrict__ pb,
                                                       const T* __restrict__ F1, const T* __restrict__ F2,
                                                       const T* __restrict__ F3, const T* __restrict__ emf,
                                                       const double* __restrict__ geom, const double* __restrict__ conn,
                                                       double* __restrict__ Uout, CellTile ct) {
+  __shared__ double s_tab[STAGE ? kStageF * kStageTI : 1];
   int i, j, k;
-  if (!tile_cell(d.n1, d.n2, d.n3, ct, blockIdx.x, blockIdx.y, blockIdx.z, i, j, k)) return;
+  const bool ok = tile_cell(d.n1, d.n2, d.n3, ct, blockIdx.x, blockIdx.y, blockIdx.z, i, j, k);
+  stage_conn_geom<STAGE>(d, geom, conn, s_tab);
+  if (!ok) return;
   int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
   const size_t id = cidx(d, ii, jj, kk), c2 = (size_t)jj * d.n1e + ii;
+  const int il = i & (kStageTI - 1);
   Geo<double> g;
-  load_geo<double, double>(geom, d.plane, c2, g);
+  if constexpr (STAGE) load_geo<double, double, false>(s_tab + 64 * kStageTI, kStageTI, il, g);
+  else load_geo<double, double>(geom, d.plane, c2, g);
   double pr[NPR];
 #pragma unroll
   for (int p = 0; p < NPR; p++) pr[p] = pi[(size_t)p * d.cells + id];
@@ -803,7 +831,8 @@ __global__ void __launch_bounds__(256, HARM_CONSERVED_BLOCKS) k_conserved(Dims d
   for (int p = 0; p < NPR; p++) pr[p] = pb[(size_t)p * d.cells + id];
   get_state<double>(pr, g, ph.gam, q);
   double dUg[NPR];
-  source_conn(pr, q, g, conn, d.plane, c2, dUg);
+  if constexpr (STAGE) source_conn<false>(pr, q, g, s_tab, kStageTI, il, dUg);
+  else source_conn(pr, q, g, conn, d.plane, c2, dUg);
   const double idx1 = 1.0 / ph.dx1, idx2 = 1.0 / ph.dx2, idx3 = 1.0 / ph.dx3;
   const double dt = *dtp;
 #pragma unroll
@@ -812,6 +841,76 @@ __global__ void __launch_bounds__(256, HARM_CONSERVED_BLOCKS) k_conserved(Dims d
     double Uf = sc.CUf0 * Ui[p] + sc.CUf2 * dt * (dU + dUg[p]);
     double ucum = sc.Cun0 * Ui[p] + sc.Cun1 * dt * (dU + dUg[p]) + sc.Cun2 * Uf;
     Uout[(size_t)p * d.cells + id] = sc.finalstep ? ucum : Uf;
+  }
+}
+
+// The conserved update in two passes (the mixed path): k_conserved_src writes
+// U = a Ui + b dt dUg (U_i = primtoU(p_i), dUg the connection source of p_b) and
+// k_conserved_div adds b dt dU (the flux divergence), with a = CUf0, b = CUf2 for an
+// intermediate substep and a = Cun0 + Cun2 CUf0, b = Cun1 + Cun2 CUf2 for the final one
+// (Uf and ucum of k_conserved expanded: both are linear in U_i and dU + dUg).  Each pass needs
+// fewer registers than the single kernel, so both run at a higher occupancy.
+#ifndef HARM_CONSERVED_SRC_BLOCKS
+#define HARM_CONSERVED_SRC_BLOCKS 3
+#endif
+__device__ __forceinline__ void conserved_ab(const StepCoef& sc, double& a, double& b) {
+  a = sc.finalstep ? sc.Cun0 + sc.Cun2 * sc.CUf0 : sc.CUf0;
+  b = sc.finalstep ? sc.Cun1 + sc.Cun2 * sc.CUf2 : sc.CUf2;
+}
+
+template <typename T, bool STAGE>
+__global__ void __launch_bounds__(256, HARM_CONSERVED_SRC_BLOCKS) k_conserved_src(Dims d, Phys ph, StepCoef sc, const double* __restrict__ dtp,
+                                                      const double* __restrict__ pi, const double* __restrict__ pb,
+                                                      const double* __restrict__ geom, const double* __restrict__ conn,
+                                                      double* __restrict__ Uout, CellTile ct) {
+  __shared__ double s_tab[STAGE ? kStageF * kStageTI : 1];
+  int i, j, k;
+  const bool ok = tile_cell(d.n1, d.n2, d.n3, ct, blockIdx.x, blockIdx.y, blockIdx.z, i, j, k);
+  stage_conn_geom<STAGE>(d, geom, conn, s_tab);
+  if (!ok) return;
+  int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
+  const size_t id = cidx(d, ii, jj, kk), c2 = (size_t)jj * d.n1e + ii;
+  const int il = i & (kStageTI - 1);
+  Geo<double> g;
+  if constexpr (STAGE) load_geo<double, double, false>(s_tab + 64 * kStageTI, kStageTI, il, g);
+  else load_geo<double, double>(geom, d.plane, c2, g);
+  double pr[NPR];
+#pragma unroll
+  for (int p = 0; p < NPR; p++) pr[p] = pi[(size_t)p * d.cells + id];
+  State<double> q;
+  get_state<double>(pr, g, ph.gam, q);
+  double Ui[NPR];
+  primtoflux<double>(pr, q, 0, g, g.gdet, Ui);
+#pragma unroll
+  for (int p = 0; p < NPR; p++) pr[p] = pb[(size_t)p * d.cells + id];
+  get_state<double>(pr, g, ph.gam, q);
+  double dUg[NPR];
+  if constexpr (STAGE) source_conn<false>(pr, q, g, s_tab, kStageTI, il, dUg);
+  else source_conn(pr, q, g, conn, d.plane, c2, dUg);
+  double a, b;
+  conserved_ab(sc, a, b);
+  const double bdt = b * *dtp;
+#pragma unroll
+  for (int p = 0; p < NPR; p++) Uout[(size_t)p * d.cells + id] = a * Ui[p] + bdt * dUg[p];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_conserved_div(Dims d, Phys ph, StepCoef sc, const double* __restrict__ dtp,
+                                                      const T* __restrict__ F1, const T* __restrict__ F2,
+                                                      const T* __restrict__ F3, const T* __restrict__ emf,
+                                                      double* __restrict__ U, CellTile ct) {
+  int i, j, k;
+  if (!tile_cell(d.n1, d.n2, d.n3, ct, blockIdx.x, blockIdx.y, blockIdx.z, i, j, k)) return;
+  int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
+  const size_t id = cidx(d, ii, jj, kk);
+  const double idx1 = 1.0 / ph.dx1, idx2 = 1.0 / ph.dx2, idx3 = 1.0 / ph.dx3;
+  double a, b;
+  conserved_ab(sc, a, b);
+  const double bdt = b * *dtp;
+#pragma unroll
+  for (int p = 0; p < NPR; p++) {
+    const double dU = dU_cell<T>(d, ii, jj, kk, p, F1, F2, F3, emf, idx1, idx2, idx3);
+    U[(size_t)p * d.cells + id] += bdt * dU;
   }
 }
 

@@ -32,21 +32,27 @@ __host__ __device__ constexpr int sym(int m, int n) {
                   : ((n == 0) ? m : (n == 1) ? 3 + m : (n == 2) ? 5 + m : 9);
 }
 
-// Load a record from a plane-major table tab[field][plane] at 2-D offset c.
-template <typename T, typename S>
+// Load a record from a plane-major table tab[field][plane] at 2-D offset c: a read-only
+// global table (LDG), or a copy staged in shared memory (plain loads).
+template <bool LDG, typename S>
+__device__ __forceinline__ S tab_ld(const S* p) {
+  if constexpr (LDG) return __ldg(p);
+  else return *p;
+}
+template <typename T, typename S, bool LDG = true>
 __device__ __forceinline__ void load_geo(const S* __restrict__ tab, size_t plane, size_t c, Geo<T>& g) {
 #pragma unroll
-  for (int f = 0; f < 10; f++) g.gcov[f] = (T)__ldg(tab + (size_t)(HARM_G_GCOV + f) * plane + c);
+  for (int f = 0; f < 10; f++) g.gcov[f] = (T)tab_ld<LDG>(tab + (size_t)(HARM_G_GCOV + f) * plane + c);
 #pragma unroll
-  for (int f = 0; f < 10; f++) g.gcon[f] = (T)__ldg(tab + (size_t)(HARM_G_GCON + f) * plane + c);
-  g.gcovpert_tt = (T)__ldg(tab + (size_t)HARM_G_GCOVPERT_TT * plane + c);
-  g.alpha = (T)__ldg(tab + (size_t)HARM_G_ALPHA * plane + c);
-  g.betasqoalphasq = (T)__ldg(tab + (size_t)HARM_G_BETASQOALPHASQ * plane + c);
-  g.beta1 = (T)__ldg(tab + (size_t)(HARM_G_BETA + 0) * plane + c);
-  g.beta2 = (T)__ldg(tab + (size_t)(HARM_G_BETA + 1) * plane + c);
-  g.beta3 = (T)__ldg(tab + (size_t)(HARM_G_BETA + 2) * plane + c);
-  g.gdet = (T)__ldg(tab + (size_t)HARM_G_GDET * plane + c);
-  g.igdet = (T)__ldg(tab + (size_t)HARM_G_IGDET * plane + c);
+  for (int f = 0; f < 10; f++) g.gcon[f] = (T)tab_ld<LDG>(tab + (size_t)(HARM_G_GCON + f) * plane + c);
+  g.gcovpert_tt = (T)tab_ld<LDG>(tab + (size_t)HARM_G_GCOVPERT_TT * plane + c);
+  g.alpha = (T)tab_ld<LDG>(tab + (size_t)HARM_G_ALPHA * plane + c);
+  g.betasqoalphasq = (T)tab_ld<LDG>(tab + (size_t)HARM_G_BETASQOALPHASQ * plane + c);
+  g.beta1 = (T)tab_ld<LDG>(tab + (size_t)(HARM_G_BETA + 0) * plane + c);
+  g.beta2 = (T)tab_ld<LDG>(tab + (size_t)(HARM_G_BETA + 1) * plane + c);
+  g.beta3 = (T)tab_ld<LDG>(tab + (size_t)(HARM_G_BETA + 2) * plane + c);
+  g.gdet = (T)tab_ld<LDG>(tab + (size_t)HARM_G_GDET * plane + c);
+  g.igdet = (T)tab_ld<LDG>(tab + (size_t)HARM_G_IGDET * plane + c);
 }
 
 template <typename T>

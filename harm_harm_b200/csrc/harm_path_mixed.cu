@@ -110,8 +110,16 @@ int hp_update_mixed(harm_ctx* c, const StepCoef& sc, const double* pi, const dou
   Phys ph = phys_of(c->g);
   const CellTile ct = cell_tile(d.n3, HARM_INVERT_LTK);
   const CellTile cct = (HARM_CONSERVED_LTK > 0 && d.n3 >= 8) ? cell_tile(d.n3, HARM_CONSERVED_LTK) : cell_linear();
-  k_conserved<float><<<cell_grid(d.n1, d.n2, d.n3, cct), 256, 0, c->stream>>>(d, ph, sc, c->d_dt, pi, pb, c->d_Ff[0], c->d_Ff[1],
-                                                         c->d_Ff[2], c->d_emff, c->d_geom, c->d_conn, c->d_U, cct);
+  if (ct.lti == 4) {  // 16 i x 16 k tiles: the metric and connection staged per block
+    k_conserved_src<float, true><<<cell_grid(d.n1, d.n2, d.n3, ct), 256, 0, c->stream>>>(d, ph, sc, c->d_dt, pi, pb,
+                                                                                        c->d_geom, c->d_conn, c->d_U, ct);
+  } else {
+    k_conserved_src<float, false><<<cell_grid(d.n1, d.n2, d.n3, cct), 256, 0, c->stream>>>(d, ph, sc, c->d_dt, pi, pb,
+                                                                                          c->d_geom, c->d_conn, c->d_U, cct);
+  }
+  k_conserved_div<float><<<cell_grid(d.n1, d.n2, d.n3, cct), 256, 0, c->stream>>>(d, ph, sc, c->d_dt, c->d_Ff[0], c->d_Ff[1],
+                                                                                 c->d_Ff[2], c->d_emff, c->d_U, cct);
+  c->launches++;
   CK(cudaMemsetAsync(c->d_nrare, 0, sizeof(unsigned int), c->stream));
   if (sc.guess == HARM_GUESS_MLP && c->mlp_tc == 2) {
     if (int rc = launch_invert_tc<1>(c, d, ph, pb, pf, pflag, stats)) return rc;
