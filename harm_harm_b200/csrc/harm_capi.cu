@@ -31,9 +31,9 @@ int hb_setmsg(const char* msg, int code) { return seterr_msg(msg, code); }
 
 extern "C" const char* harm_b200_last_error(void) { return g_errbuf; }
 
-extern "C" int harm_b200_create(const harm_grid* g, const double* geom_h, const double* conn_h, const double* aux_h,
-                                int device, harm_ctx** out) {
-  if (!g || !geom_h || !conn_h || !aux_h || !out) return seterr_msg("null argument", 1);
+// the context of grid g on `device` with every buffer allocated; the tables are filled by
+// the caller (upload or device build)
+static int create_ctx(const harm_grid* g, int device, harm_ctx** out) {
   if (g->lim != HARM_LIM_MC && g->lim != HARM_LIM_PARA && g->lim != HARM_LIM_WENO5)
     return seterr_msg("unknown reconstruction", 2);
   if (g->lim == HARM_LIM_WENO5 && g->ng < 6) return seterr_msg("WENO5 needs ng >= 6", 2);
@@ -51,17 +51,6 @@ extern "C" int harm_b200_create(const harm_grid* g, const double* geom_h, const 
   CK(cudaMalloc(&c->d_geomf, gsz * sizeof(float)));
   CK(cudaMalloc(&c->d_conn, 64 * d.plane * sizeof(double)));
   CK(cudaMalloc(&c->d_aux, HARM_NAUX * d.plane * sizeof(double)));
-  CK(cudaMemcpy(c->d_geom, geom_h, gsz * sizeof(double), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(c->d_conn, conn_h, 64 * d.plane * sizeof(double), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(c->d_aux, aux_h, HARM_NAUX * d.plane * sizeof(double), cudaMemcpyHostToDevice));
-  {
-    float* tmp = (float*)malloc(gsz * sizeof(float));
-    if (!tmp) return seterr_msg("host allocation failed", 3);
-    for (size_t q = 0; q < gsz; q++) tmp[q] = (float)geom_h[q];
-    cudaError_t e = cudaMemcpy(c->d_geomf, tmp, gsz * sizeof(float), cudaMemcpyHostToDevice);
-    free(tmp);
-    if (e != cudaSuccess) return hb_seterr("upload FP32 metric", e);
-  }
   for (int q = 0; q < 3; q++) {
     CK(cudaMalloc(&c->d_F[q], NPR * d.cells * sizeof(double)));
     CK(cudaMalloc(&c->d_Ff[q], NPR * d.cells * sizeof(float)));
@@ -102,6 +91,39 @@ extern "C" int harm_b200_create(const harm_grid* g, const double* geom_h, const 
   CK(cudaMemset(c->d_dtslots, 0xFF, 6 * sizeof(unsigned long long)));
   CK(cudaMallocHost(&c->h_scal, 64 * sizeof(double)));
   *out = c;
+  return 0;
+}
+
+extern "C" int harm_b200_create(const harm_grid* g, const double* geom_h, const double* conn_h, const double* aux_h,
+                                int device, harm_ctx** out) {
+  if (!g || !geom_h || !conn_h || !aux_h || !out) return seterr_msg("null argument", 1);
+  harm_ctx* c = nullptr;
+  if (int rc = create_ctx(g, device, &c)) return rc;
+  const size_t gsz = (size_t)HARM_NLOC * HARM_NGF * c->plane;
+  CK(cudaMemcpy(c->d_geom, geom_h, gsz * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_conn, conn_h, 64 * c->plane * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_aux, aux_h, HARM_NAUX * c->plane * sizeof(double), cudaMemcpyHostToDevice));
+  if (int rc = hp_geometry_f32(c)) return rc;
+  *out = c;
+  return 0;
+}
+
+extern "C" int harm_b200_create_grid(const harm_grid* g, int device, harm_ctx** out) {
+  if (!g || !out) return seterr_msg("null argument", 1);
+  harm_ctx* c = nullptr;
+  if (int rc = create_ctx(g, device, &c)) return rc;
+  if (int rc = hp_geometry_build(c)) return rc;
+  if (int rc = hp_geometry_f32(c)) return rc;
+  *out = c;
+  return 0;
+}
+
+extern "C" int harm_b200_get_tables(harm_ctx* c, double* geom_h, double* conn_h, double* aux_h) {
+  if (!c) return seterr_msg("null argument", 1);
+  const size_t gsz = (size_t)HARM_NLOC * HARM_NGF * c->plane;
+  if (geom_h) CK(cudaMemcpy(geom_h, c->d_geom, gsz * sizeof(double), cudaMemcpyDeviceToHost));
+  if (conn_h) CK(cudaMemcpy(conn_h, c->d_conn, 64 * c->plane * sizeof(double), cudaMemcpyDeviceToHost));
+  if (aux_h) CK(cudaMemcpy(aux_h, c->d_aux, HARM_NAUX * c->plane * sizeof(double), cudaMemcpyDeviceToHost));
   return 0;
 }
 

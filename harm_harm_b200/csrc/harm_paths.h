@@ -20,3 +20,6 @@ int hp_copy_ghosts(harm_ctx* c, const double* pb, double* pf);
 int hp_fixup(harm_ctx* c, double* pf, int8_t* pflag, bool bound_flags = true);
 int hp_finalize_dt(harm_ctx* c, double* dt, double* ndt_out, int nsub);
 int hp_points(harm_ctx* c, size_t n, int guess, const double* U, const double* geom, double* P, int8_t* pflag, int32_t* iters);
+// the metric, connection and floor tables computed on the device; their FP32 copy
+int hp_geometry_build(harm_ctx* c);
+int hp_geometry_f32(harm_ctx* c);

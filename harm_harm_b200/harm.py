@@ -92,16 +92,33 @@ class Grid:
 class Harm:
     """One grid on one GPU: the device context of libharm_b200.so."""
 
-    def __init__(self, grid: Grid, geom: np.ndarray, conn: np.ndarray, aux: np.ndarray, device: int = 0):
+    def __init__(self, grid: Grid, geom: np.ndarray | None = None, conn: np.ndarray | None = None,
+                 aux: np.ndarray | None = None, device: int = 0):
+        """Upload the host-built tables (geom, conn, aux), or, when all three are None, build
+        the metric, connection and floor tables on the device (harm_b200_create_grid)."""
         self.grid = grid
         self.lib = N.device_lib()
         self._ctx = C.c_void_p()
+        if geom is None and conn is None and aux is None:
+            rc = self.lib.harm_b200_create_grid(C.byref(grid.g), device, C.byref(self._ctx))
+            self._check(rc, "harm_b200_create_grid")
+            return
         geom = np.ascontiguousarray(geom, dtype=np.float64)
         conn = np.ascontiguousarray(conn, dtype=np.float64)
         aux = np.ascontiguousarray(aux, dtype=np.float64)
         rc = self.lib.harm_b200_create(C.byref(grid.g), _ptr(geom), _ptr(conn), _ptr(aux), device,
                                        C.byref(self._ctx))
         self._check(rc, "harm_b200_create")
+
+    def tables(self):
+        """The context's metric, connection and floor tables as host arrays
+        (geom[4][28][n2e][n1e], conn[64][n2e][n1e], aux[3][n2e][n1e])."""
+        g = self.grid.g
+        geom = np.empty((4, 28, g.n2e, g.n1e), dtype=np.float64)
+        conn = np.empty((64, g.n2e, g.n1e), dtype=np.float64)
+        aux = np.empty((3, g.n2e, g.n1e), dtype=np.float64)
+        self._check(self.lib.harm_b200_get_tables(self._ctx, _ptr(geom), _ptr(conn), _ptr(aux)), "get_tables")
+        return geom, conn, aux
 
     def _check(self, rc: int, what: str) -> None:
         if rc:

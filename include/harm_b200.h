@@ -162,6 +162,16 @@ typedef struct harm_ctx harm_ctx;
                                   rounding of its activations) */
 int harm_b200_create(const harm_grid *g, const double *geom_h, const double *conn_h,
                      const double *aux_h, int device, harm_ctx **out);
+/* Create a context whose metric (CENT/FACE1/FACE2/CORN3), connection and floor tables are
+   computed on the device from the grid (set_grid set_grid.c:114, set_connection
+   set_grid.c:1033): Kerr-Schild in MKS coordinates, closed-form inverse metric, connection
+   from Ridders-extrapolated central differences of the metric -- the algorithm of the host
+   builder harm_geometry_build, whose tables it matches to the last bits of the math library.
+   No host tables are needed. */
+int harm_b200_create_grid(const harm_grid *g, int device, harm_ctx **out);
+/* Copy the context's tables to host arrays in the layout harm_b200_create takes (any
+   pointer may be NULL). */
+int harm_b200_get_tables(harm_ctx *ctx, double *geom_h, double *conn_h, double *aux_h);
 int harm_b200_destroy(harm_ctx *ctx);
 
 /* CUDA stream the context launches on (cudaStream_t as void*). */
