@@ -52,6 +52,7 @@ _DEVICE_SIGS = {
     "harm_b200_create": (Ip, [C.POINTER(harm_grid), P, P, P, Ip, C.POINTER(P)]),
     "harm_b200_create_grid": (Ip, [C.POINTER(harm_grid), Ip, C.POINTER(P)]),
     "harm_b200_get_tables": (Ip, [P, P, P, P]),
+    "harm_b200_dump": (Ip, [P, P, P, C.c_double, C.c_double, C.c_long, Ip, C.c_char_p]),
     "harm_b200_destroy": (Ip, [P]),
     "harm_b200_stream": (P, [P]),
     "harm_b200_launch_count": (C.c_ulonglong, [P]),

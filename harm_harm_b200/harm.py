@@ -110,6 +110,14 @@ class Harm:
                                        C.byref(self._ctx))
         self._check(rc, "harm_b200_create")
 
+    def dump(self, P, path: str, t: float = 0.0, dt: float = 0.0, nstep: int = 0, U=None, fmt: str = "text") -> None:
+        """the reference's main dump file of P (bounded ghost zones) at `path`: "text" (the
+        reference's default), "binary" or "mixed" (harm_b200_dump)"""
+        code = {"text": 0, "binary": 1, "mixed": 2}[fmt]
+        rc = self.lib.harm_b200_dump(self._ctx, _ptr(P), None if U is None else _ptr(U), float(t), float(dt), int(nstep),
+                                     code, path.encode())
+        self._check(rc, "harm_b200_dump")
+
     def tables(self):
         """The context's metric, connection and floor tables as host arrays
         (geom[4][28][n2e][n1e], conn[64][n2e][n1e], aux[3][n2e][n1e])."""

@@ -306,6 +306,24 @@ int harm_b200_mlp_set(harm_ctx *ctx, const float *d_params, const float *d_norm,
    on the tensor cores of the context's engine (HARM_B200_MLP_ENGINE), as in the inversion. */
 int harm_b200_mlp_predict(harm_ctx *ctx, size_t n, const float *d_feat, float *d_out);
 
+/* ------------------------------------------------------------------------------------
+ * The reference's main dump file (dump() dump.c:256 through dump_gen dumpgen.c:5) written
+ * from device state: the header of dump_header_general (dump.c:320) and, for every active
+ * cell in the order k, j, i (i fastest), the 52 columns of dump_content (dump.c:449):
+ *   ti tj tk  x1 x2 x3  r th ph  rho u v1 v2 v3 B1 B2 B3  p cs2 Sden  U0..U7  divb
+ *   uu0..uu3  ud0..ud3  bu0..bu3  bd0..bd3  v1m v1p v2m v2p v3m v3p  gdet
+ * TEXT: the header line and one line of "%21.15g " columns per cell (the reference's default
+ * output without MPI-IO); BINARY: header fields and columns as raw native values (the
+ * header then has no defcoord); MIXED: the text header and raw columns.
+ * d_P: primitives with bounded ghost zones; d_U: the conserved state to record (NULL:
+ * primtoU of d_P); t, dt, nstep: the header's time, time step and step count.
+ * ------------------------------------------------------------------------------------ */
+#define HARM_DUMP_TEXT 0
+#define HARM_DUMP_BINARY 1
+#define HARM_DUMP_MIXED 2
+int harm_b200_dump(harm_ctx *ctx, const double *d_P, const double *d_U, double t, double dt,
+                   long nstep, int format, const char *path);
+
 /* Largest grid (extended cells n1e*n2e*n3e) harm_b200_fluxcalc_noalloc accepts: its EMF
    scratch is 3 doubles per cell, 48 MiB at this size. */
 #define HARM_NOALLOC_MAX_CELLS 2097152

@@ -54,6 +54,10 @@ int orc_step(orc *o, double *P, double *dt, harm_stats *st);
 /* reconstruction of one line (tests): y[n] -> left/right face states of faces 3..n-3 */
 void orc_reconstruct_line(int lim, int n, const double *y, double *pl, double *pr);
 
+/* the 52 columns of one row of the main dump file (dump_content, dump.c:449) for active cell
+   (i, j, k); U may be NULL (primtoU of P) */
+void orc_dump_row(const orc *o, const double *P, const double *U, int i, int j, int k, double *out);
+
 /* learned-guess network oracle (double precision; same parameter layout as the device) */
 int orc_mlp_nparams(void);
 void orc_mlp_features(const harm_grid *g, const double *geomrec, const double *U,

@@ -63,6 +63,7 @@ def lib() -> C.CDLL:
             "orc_mlp_nparams": (I, []),
             "orc_mlp_features": (None, [C.POINTER(N.harm_grid), P, P, P, P, P]),
             "orc_mlp_loss_grad": (D, [I, P, P, P, P, P, P]),
+            "orc_dump_row": (None, [C.POINTER(orc), P, P, I, I, I, P]),
         }
         for fn, (res, args) in sigs.items():
             f = getattr(L, fn)
@@ -107,6 +108,17 @@ class Oracle:
 
     def post_fixup(self, pf, pflag):
         lib().orc_post_fixup(C.byref(self.o), _p(pf), _p(pflag))
+
+    def dump_rows(self, P, cells, U=None):
+        """the main dump's 52 columns (dump_content, dump.c:449) of the active cells (i, j, k)"""
+        Pc = np.ascontiguousarray(P, dtype=np.float64)
+        Uc = None if U is None else np.ascontiguousarray(U, dtype=np.float64)
+        out = np.zeros((len(cells), 52))
+        row = np.zeros(52)
+        for n, (i, j, k) in enumerate(cells):
+            lib().orc_dump_row(C.byref(self.o), _p(Pc), None if Uc is None else _p(Uc), int(i), int(j), int(k), _p(row))
+            out[n] = row
+        return out
 
     def step_ch(self, P, dt):
         d = C.c_double(dt)

@@ -56,3 +56,31 @@ def geom_records(geom, grid, idx2d):
     """CENT records [HARM_NGF][n] at flattened (j*n1e+i) positions"""
     cent = geom[0].reshape(geom.shape[1], -1)
     return np.ascontiguousarray(cent[:, idx2d])
+
+
+DUMP_NCOL = 52
+
+
+def read_dump(path, fmt="text"):
+    """Parse a main dump file in the reference's layout (dump_header_general dump.c:320 and
+    the rows of dump_content dump.c:449): returns (header dict, columns [cells][52])."""
+    import struct
+    names = ["t", "n1", "n2", "n3", "startx1", "startx2", "startx3", "dx1", "dx2", "dx3", "nstep", "gam", "a",
+             "R0", "Rin", "Rout", "hslope", "dt", "MBH", "QBH", "is", "ie", "js", "je", "ks", "ke", "whichdump",
+             "version", "ncol"]
+    with open(path, "rb") as f:
+        data = f.read()
+    if fmt == "binary":
+        layout = "<d3i6dq9d9i"
+        size = struct.calcsize(layout)
+        head = dict(zip(names, struct.unpack(layout, data[:size])))
+        body = np.frombuffer(data[size:], dtype=np.float64)
+    else:
+        nl = data.index(b"\n")
+        tok = data[:nl].split()
+        text_names = names[:18] + ["defcoord"] + names[18:]
+        conv = [float] + [int] * 3 + [float] * 6 + [int] + [float] * 7 + [int] + [float] * 2 + [int] * 9
+        head = {n: c(t) for n, c, t in zip(text_names, conv, tok)}
+        rest = data[nl + 1:]
+        body = np.frombuffer(rest, dtype=np.float64) if fmt == "mixed" else np.array(rest.split(), dtype=np.float64)
+    return head, body.reshape(-1, head["ncol"])
