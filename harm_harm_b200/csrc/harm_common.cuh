@@ -670,27 +670,30 @@ __device__ __forceinline__ double dU_cell(const Dims& d, int ii, int jj, int kk,
     const T* e3 = emf + 2 * cells;
     auto E = [&](const T* e, int a, int b, int c) -> T { return e[cidx(d, a, b, c)]; };
     const int kq = has3 ? kk + 1 : kk;
+    // a face's field flux is the average of its two edge EMFs, added in FP64: the sum of two
+    // FP32 values is exact there, so the flux-CT telescoping that keeps the corner div B at
+    // round-off holds exactly (rounded FP32 sums leave ~1e-7 of |EMF| per step in div B)
     if (p == HARM_B1) {
       f1a = 0.0; f1b = 0.0;
-      f2a = (double)(T(-0.5) * (E(e3, ii, jj, kk) + E(e3, ii + 1, jj, kk)));
-      f2b = (double)(T(-0.5) * (E(e3, ii, jj + 1, kk) + E(e3, ii + 1, jj + 1, kk)));
+      f2a = -0.5 * ((double)E(e3, ii, jj, kk) + (double)E(e3, ii + 1, jj, kk));
+      f2b = -0.5 * ((double)E(e3, ii, jj + 1, kk) + (double)E(e3, ii + 1, jj + 1, kk));
       if (has3) {
-        f3a = (double)(T(0.5) * (E(e2, ii, jj, kk) + E(e2, ii + 1, jj, kk)));
-        f3b = (double)(T(0.5) * (E(e2, ii, jj, kk + 1) + E(e2, ii + 1, jj, kk + 1)));
+        f3a = 0.5 * ((double)E(e2, ii, jj, kk) + (double)E(e2, ii + 1, jj, kk));
+        f3b = 0.5 * ((double)E(e2, ii, jj, kk + 1) + (double)E(e2, ii + 1, jj, kk + 1));
       }
     } else if (p == HARM_B2) {
-      f1a = (double)(T(0.5) * (E(e3, ii, jj, kk) + E(e3, ii, jj + 1, kk)));
-      f1b = (double)(T(0.5) * (E(e3, ii + 1, jj, kk) + E(e3, ii + 1, jj + 1, kk)));
+      f1a = 0.5 * ((double)E(e3, ii, jj, kk) + (double)E(e3, ii, jj + 1, kk));
+      f1b = 0.5 * ((double)E(e3, ii + 1, jj, kk) + (double)E(e3, ii + 1, jj + 1, kk));
       f2a = 0.0; f2b = 0.0;
       if (has3) {
-        f3a = (double)(T(-0.5) * (E(e1, ii, jj, kk) + E(e1, ii, jj + 1, kk)));
-        f3b = (double)(T(-0.5) * (E(e1, ii, jj, kk + 1) + E(e1, ii, jj + 1, kk + 1)));
+        f3a = -0.5 * ((double)E(e1, ii, jj, kk) + (double)E(e1, ii, jj + 1, kk));
+        f3b = -0.5 * ((double)E(e1, ii, jj, kk + 1) + (double)E(e1, ii, jj + 1, kk + 1));
       }
     } else {
-      f1a = (double)(T(-0.5) * (E(e2, ii, jj, kk) + E(e2, ii, jj, kq)));
-      f1b = (double)(T(-0.5) * (E(e2, ii + 1, jj, kk) + E(e2, ii + 1, jj, kq)));
-      f2a = (double)(T(0.5) * (E(e1, ii, jj, kk) + E(e1, ii, jj, kq)));
-      f2b = (double)(T(0.5) * (E(e1, ii, jj + 1, kk) + E(e1, ii, jj + 1, kq)));
+      f1a = -0.5 * ((double)E(e2, ii, jj, kk) + (double)E(e2, ii, jj, kq));
+      f1b = -0.5 * ((double)E(e2, ii + 1, jj, kk) + (double)E(e2, ii + 1, jj, kq));
+      f2a = 0.5 * ((double)E(e1, ii, jj, kk) + (double)E(e1, ii, jj, kq));
+      f2b = 0.5 * ((double)E(e1, ii, jj + 1, kk) + (double)E(e1, ii, jj + 1, kq));
       f3a = 0.0; f3b = 0.0;
     }
   }

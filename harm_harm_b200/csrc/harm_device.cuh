@@ -347,12 +347,13 @@ template <typename T>
 __device__ __forceinline__ T limit_weight(int order, T w) {
   const T avg = T(1) / T(order), w1 = T(0.2) * avg, w2 = (T(1) - T(0.2)) * avg, w3 = (T(1) + T(0.2)) * avg, w4 = T(1);
   if constexpr (sizeof(T) == 4) {
-    // FP32: both ramps evaluated and selected, no divergent branches (same values)
+    // FP32: the limiter is continuous and piecewise linear, 0 | ramp to avg | avg | ramp to 1,
+    // so it is the lower ramp clamped to [0, avg] plus the part of the upper ramp above avg:
+    // min/max instead of compares and selects, no divergent branches (the same values away
+    // from the break points, within a rounding at them)
     const T lo = wdivk<T>(avg * (w - w1), w2 - w1);
-    const T hi = wdivk<T>((w - w3) * (w4 - avg), w4 - w3) + avg;
-    T r = (w < w3) ? avg : hi;
-    r = (w < w2) ? lo : r;
-    return (w < w1) ? T(0) : r;
+    const T up = wdivk<T>((w - w3) * (w4 - avg), w4 - w3);
+    return fmaxf(fminf(lo, avg), T(0)) + fmaxf(up, T(0));
   } else {
     if (w < w1) return T(0);
     if (w < w2) return wdivk<T>(avg * (w - w1), w2 - w1);

@@ -1,5 +1,5 @@
 // harm_weno_f32x2.cuh -- the FP32 WENO5 weights and edge values of two cells at once on
-// Blackwell's packed FP32 pipe (add/sub/mul/fma .f32x2: one instruction, two lanes).
+// Blackwell's packed FP32 pipe (add/mul/fma on float2: one instruction, two lanes).
 //
 // The arithmetic is that of weno5_unopt / weno3_unopt / weno5_edges for T = float
 // (harm_device.cuh), lane by lane; operations without a packed form (reciprocals, compares,
@@ -13,39 +13,21 @@
 
 namespace hb {
 
-struct F2 {
-  unsigned long long v;
-};
+// F2 is a float2: the compiler's float2 intrinsics of the packed pipe (add, mul, fma with
+// round-to-nearest; no contraction across them) let it keep the pairs in adjacent registers,
+// so packing and unpacking cost no moves
+using F2 = float2;
 
-__device__ __forceinline__ F2 f2(float a, float b) {
-  F2 r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
-  return r;
-}
-__device__ __forceinline__ F2 f2(float a) { return f2(a, a); }
+__device__ __forceinline__ F2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ F2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ void f2split(F2 x, float& a, float& b) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(x.v));
+  a = x.x;
+  b = x.y;
 }
-__device__ __forceinline__ F2 operator+(F2 a, F2 b) {
-  F2 r;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
-  return r;
-}
-__device__ __forceinline__ F2 operator-(F2 a, F2 b) {
-  F2 r;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
-  return r;
-}
-__device__ __forceinline__ F2 operator*(F2 a, F2 b) {
-  F2 r;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
-  return r;
-}
-__device__ __forceinline__ F2 ffma2(F2 a, F2 b, F2 c) {
-  F2 r;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
-  return r;
-}
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ F2 ffma2(F2 a, F2 b, F2 c) { return __ffma2_rn(a, b, c); }
 // lane-wise helpers
 template <typename Fn>
 __device__ __forceinline__ F2 lanes(F2 x, Fn fn) {

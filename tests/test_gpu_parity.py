@@ -158,7 +158,9 @@ def test_mixed_precision_close_to_fp64(setup, cuda):
     assert np.isfinite(b).all()
     assert l1_rho < 1e-5, l1_rho
     scale = np.abs(Pb.cpu().numpy()[5:8] * geom[0, 26][None, None]).max() / min(g.g.dx[1], g.g.dx[2])
-    assert divb_corner(g, geom, Pb.cpu().numpy()).max() / scale < 1e-6
+    # flux-CT keeps the corner divergence at round-off in the mixed path too (the field
+    # fluxes average their FP32 edge EMFs exactly, in FP64)
+    assert divb_corner(g, geom, Pb.cpu().numpy()).max() / scale < 1e-10
 
 
 @pytest.mark.parametrize("lim", [0, 1, 2])
