@@ -49,12 +49,18 @@ __device__ __forceinline__ F2 rcp2(F2 x) {
 __device__ __forceinline__ F2 symsum3(F2 a0, F2 a1, F2 a2) { return (a0 + a2) + a1; }
 __device__ __forceinline__ F2 symsum2(F2 a0, F2 a1) { return a0 + a1; }
 
-__device__ __forceinline__ F2 limit_weight3_f2(F2 w) {
-  return lanes(w, [](float x) { return limit_weight<float>(3, x); });
+// limit_weight<float> of two weights: the two ramps in the scalar code's operations on the
+// packed pipe, the clamps per lane
+template <int ORDER>
+__device__ __forceinline__ F2 limit_weight_f2(F2 w) {
+  constexpr float avg = 1.0f / (float)ORDER, w1 = 0.2f * avg, w2 = (1.0f - 0.2f) * avg, w3 = (1.0f + 0.2f) * avg,
+                  w4 = 1.0f;
+  const F2 lo = (f2(avg) * (w - f2(w1))) * f2(1.0f / (w2 - w1));
+  const F2 up = ((w - f2(w3)) * f2(w4 - avg)) * f2(1.0f / (w4 - w3));
+  return f2(fmaxf(fminf(lo.x, avg), 0.0f), fmaxf(fminf(lo.y, avg), 0.0f)) + f2(fmaxf(up.x, 0.0f), fmaxf(up.y, 0.0f));
 }
-__device__ __forceinline__ F2 limit_weight2_f2(F2 w) {
-  return lanes(w, [](float x) { return limit_weight<float>(2, x); });
-}
+__device__ __forceinline__ F2 limit_weight3_f2(F2 w) { return limit_weight_f2<3>(w); }
+__device__ __forceinline__ F2 limit_weight2_f2(F2 w) { return limit_weight_f2<2>(w); }
 
 // weno5_unopt of two cells: u points at the cells' centre values (u[-2..2])
 __device__ __forceinline__ void weno5_unopt_f2(const F2* u, F2* w) {
@@ -76,7 +82,7 @@ __device__ __forceinline__ void weno5_unopt_f2(const F2* u, F2* w) {
   const F2 rb = rcp2(symsum3(b[0], b[1], b[2]) + f2(WenoEps<float>::tiny));
 #pragma unroll
   for (int s = 0; s < 3; s++) {
-    const F2 t = b[s] * rb + f2(WenoEps<float>::weps);
+    const F2 t = ffma2(b[s], rb, f2(WenoEps<float>::weps));  // contracted, as the scalar FP32 code
     w[s] = rcp2(t * t);
   }
   const F2 r1 = rcp2(symsum3(w[0], w[1], w[2]));
@@ -97,7 +103,7 @@ __device__ __forceinline__ void weno3_unopt_f2(const F2* u, F2* w) {
   const F2 rb = rcp2(symsum2(b[0], b[1]) + f2(WenoEps<float>::tiny));
 #pragma unroll
   for (int s = 0; s < 2; s++) {
-    const F2 t = b[s] * rb + f2(WenoEps<float>::weps);
+    const F2 t = ffma2(b[s], rb, f2(WenoEps<float>::weps));  // contracted, as the scalar FP32 code
     w[s] = rcp2(t * t);
   }
   const F2 r1 = rcp2(symsum2(w[0], w[1]));
@@ -116,8 +122,8 @@ __device__ __forceinline__ F2 nz_mul(F2 wgt, F2 x) { return wgt * x; }
 // weno5_edges of two cells
 __device__ __forceinline__ void weno5_edges_f2(const F2* u, const F2* w, const F2* wm, const F2* wp, F2& yl, F2& yr) {
   const F2 E = f2(WenoEps<float>::eps);
-  const F2 rl = lanes(w[2] + E, wm[0] + E, [](float a, float b) { return __fdividef(a, b); });
-  const F2 rr = lanes(w[0] + E, wp[2] + E, [](float a, float b) { return __fdividef(a, b); });
+  const F2 rl = (w[2] + E) * rcp2(wm[0] + E);  // the weight ratios: a fast reciprocal per lane
+  const F2 rr = (w[0] + E) * rcp2(wp[2] + E);
   const F2 ratio = lanes(rl, rr, [](float a, float b) { return fminf(a, b); });
   const F2 f = lanes((ratio - f2(1.3f)) * f2(1.0f / (1.6f - 1.3f)), [](float a) { return fmaxf(0.0f, fminf(a, 1.0f)); });
   F2 wl[3] = {w[0] * f2(1.f / 16.f), w[1] * f2(5.f / 8.f), w[2] * f2(5.f / 16.f)};
