@@ -349,8 +349,16 @@ __device__ __forceinline__ double face_hll(const Dims& d, const Phys& ph, const 
   return dtij;
 }
 
+// HARM_FLUXT_MINB: resident blocks per SM the tiled flux kernel is compiled for (the mixed
+// path's FP32 tiles: 3, at most 85 registers with every staging load in flight); unset, the
+// compiler's choice (the FP64 tiles need ~160 registers)
+#ifdef HARM_FLUXT_MINB
+#define HARM_FLUXT_LB __launch_bounds__(256, HARM_FLUXT_MINB)
+#else
+#define HARM_FLUXT_LB __launch_bounds__(256)
+#endif
 template <int DIR, int LIM, typename T, typename GT>
-__global__ void __launch_bounds__(256) k_fluxt(Dims d, Phys ph, FaceBox fb, const double* __restrict__ P,
+__global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double* __restrict__ P,
                                                const GT* __restrict__ geom, T* __restrict__ F,
                                                unsigned long long* __restrict__ dtslot) {
   using TL = FluxTile<LIM, T>;
@@ -409,8 +417,9 @@ __global__ void __launch_bounds__(256) k_fluxt(Dims d, Phys ph, FaceBox fb, cons
   for (int p0 = 0; p0 < NPR; p0 += VB) {
     if (p0 > 0) __syncthreads();
     // stage VB primitives (the tile's cells and the halo along DIR; cells past the grid's
-    // edge are clamped: they only feed faces outside the face box)
-#pragma unroll 4
+    // edge are clamped: they only feed faces outside the face box).  Fully unrolled, so
+    // that all of a thread's loads are in flight together.
+#pragma unroll
     for (int idx = tid; idx < VB * PL; idx += 256) {
       int v, cl, ct;
       split(idx, 0, NL, v, cl, ct);

@@ -2,6 +2,8 @@
 // flux-CT; FP64 conserved update, sources and inversion (compiled with FMA contraction).
 // the inversion of this path shares reciprocals between its FP64 divisions (harm_invert.cuh)
 #define HARM_INVERT_FAST_DIV 1
+// FP32 flux tiles at 3 resident blocks per SM (harm_common.cuh)
+#define HARM_FLUXT_MINB 3
 #include <algorithm>
 #include <cudaTypedefs.h>
 #include <mutex>
