@@ -1011,7 +1011,10 @@ __global__ void __launch_bounds__(256, HARM_INVERT_BLOCKS) k_invert(Dims d, Phys
 // memory once per block.  Kept apart from the Newton iteration so that each kernel runs at
 // its own occupancy (this one needs few registers, the FP64 iteration many).
 template <int PATH>
-__global__ void __launch_bounds__(256, 3) k_mlp_guess(Dims d, const double* __restrict__ U,
+#ifndef HARM_MLP_GUESS_BLOCKS
+#define HARM_MLP_GUESS_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(256, HARM_MLP_GUESS_BLOCKS) k_mlp_guess(Dims d, const double* __restrict__ U,
                                                       const double* __restrict__ geom, double* __restrict__ wpg,
                                                       const MlpPacked* __restrict__ mlp, CellTile ct) {
   __shared__ MlpPacked sm;

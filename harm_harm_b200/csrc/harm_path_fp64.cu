@@ -321,7 +321,7 @@ int hp_update_fp64(harm_ctx* c, const StepCoef& sc, const double* pi, const doub
     if (c->mlp_tc == 1) {
       if (int rc = launch_mlp_guess_tc<0>(c, d)) return rc;
     } else {
-      k_mlp_guess<0><<<3 * 148, 256, 0, c->stream>>>(d, c->d_U, c->d_geom, c->d_wpg,
+      k_mlp_guess<0><<<HARM_MLP_GUESS_BLOCKS * c->num_sms, 256, 0, c->stream>>>(d, c->d_U, c->d_geom, c->d_wpg,
                                                       reinterpret_cast<const MlpPacked*>(c->d_mlp), ct);
       c->launches++;
     }
