@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from helpers import make_torus, rel_err
-from harm_harm_b200 import HARM_GUESS_MLP, HARM_GUESS_PREV, HARM_PREC_MIXED, Harm
+from harm_harm_b200 import HARM_GUESS_MLP, HARM_GUESS_PREV, HARM_PREC_FP64, HARM_PREC_MIXED, Harm
 from oracle import oracle as O
 from test_gpu_mlp import _synth, _torus_pairs, _train
 
@@ -92,9 +92,10 @@ def test_tensor_core_learned_steps_match_plain_and_mma_sync_steps(engines):
         assert abs(runs[name] - runs["mma.sync"]) < 0.05 * runs["mma.sync"]
 
 
-@pytest.mark.parametrize("engine", ["tc", "tc-fused"])
-def test_tensor_core_learned_steps_3d(cuda, engine):
-    """3-D tiles (16 i x 8 k at one j) with a ragged edge in i and k."""
+@pytest.mark.parametrize("engine,precision", [("tc", HARM_PREC_MIXED), ("tc-fused", HARM_PREC_MIXED),
+                                              ("tc", HARM_PREC_FP64), ("tc-fused", HARM_PREC_FP64)])
+def test_tensor_core_learned_steps_3d(cuda, engine, precision):
+    """3-D tiles (16 i x 8 k at one j) with a ragged edge in i and k, on both arithmetic paths."""
     torch = cuda
     g, geom, conn, aux, P0 = make_torus(40, 24, 12)
     dev = _harm(g, geom, conn, aux, engine)
@@ -105,8 +106,8 @@ def test_tensor_core_learned_steps_3d(cuda, engine):
         Pa = torch.from_numpy(P0).cuda()
         dev.bound_prim(Pa)
         Pb = Pa.clone()
-        _, sta = dev.step_ch(Pa, 1e-3, precision=HARM_PREC_MIXED, guess=HARM_GUESS_PREV, nsteps=2)
-        _, stb = dev.step_ch(Pb, 1e-3, precision=HARM_PREC_MIXED, guess=HARM_GUESS_MLP, nsteps=2)
+        _, sta = dev.step_ch(Pa, 1e-3, precision=precision, guess=HARM_GUESS_PREV, nsteps=2)
+        _, stb = dev.step_ch(Pb, 1e-3, precision=precision, guess=HARM_GUESS_MLP, nsteps=2)
         a, b = Pa.cpu().numpy(), Pb.cpu().numpy()
         for pl in range(8):
             assert rel_err(a[pl], b[pl], 1e-8) < 1e-9, (pl, rel_err(a[pl], b[pl], 1e-8))
