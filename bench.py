@@ -68,8 +68,8 @@ def flux_bytes_per_cell(n3: int, precision: int) -> float:
 
 
 # DRAM traffic of the flux stage (three k_fluxt launches; ncu dram__bytes_read.sum +
-# dram__bytes_write.sum) per active cell, measured on the 192x96x64 torus (profiles/
-# k_fluxt_weno5_f32_torus3d_192x96x64.md) and scaled to a workload by its cell count
+# dram__bytes_write.sum) per active cell, measured on the 192x96x64 torus and scaled to a
+# workload by its cell count
 FLUX_TRAFFIC_PER_CELL = {("weno5", "mixed"): 293.6}
 
 
@@ -386,11 +386,16 @@ def run_ours(args, ws, rank, local):
                          "traffic": (FLUX_TRAFFIC_PER_CELL[(LIMNAME[lim], args.precision)] * zones
                                      if (LIMNAME[lim], args.precision) in FLUX_TRAFFIC_PER_CELL else None),
                          "unit_of_launch": "one flux stage (three k_fluxt launches, all directions)",
-                         "algorithmic_bytes_per_cell": flux_bytes_per_cell(n3, prec)},
-            "roofline_update_invert": {"bound": "hbm", "kernel": "k_conserved + k_invert(_mlp) + k_invert_rare",
+                         "algorithmic_bytes_per_cell": flux_bytes_per_cell(n3, prec),
+                         "limiter": "instruction issue, not HBM: 76 % of issue slots, FMA 56 %, ALU 50 % "
+                                    "(ncu, WENO5 FP32 tile kernel, 192x96x64)"},
+            "roofline_update_invert": {"bound": "hbm",
+                                       "kernel": "conserved update + learned start + k_invert + k_invert_rare",
                                        "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                                        "frac": ach / peaks["hbm_gbs"],
-                                       "algorithmic_bytes_per_cell": update_kernel_bytes_per_cell(n3, prec)},
+                                       "algorithmic_bytes_per_cell": update_kernel_bytes_per_cell(n3, prec),
+                                       "limiter": "FP64 pipe (55 %) and the dependent divisions of the Newton "
+                                                  "chain in k_invert; load latency in the conserved passes (ncu)"},
             "step_roofline": {"bytes_per_zone_update": bytes_per_zone_update(n3),
                               "achieved_gbs": value / ws * bytes_per_zone_update(n3) / 1e9,
                               "frac": value / ws * bytes_per_zone_update(n3) / 1e9 / peaks["hbm_gbs"]},

@@ -3,7 +3,7 @@
   C1  3-D 192x96x64, WENO5, FP64: device and oracle after 2 RK2 steps, 1e-10 relative
       (plus div B at round-off on the device after the steps);
   C2  3-D 256x128x64, WENO5, mixed precision against the FP64 device path after 20 steps:
-      L1 relative density error <= 1e-6, the north-star accuracy bound;
+      L1 relative density error <= 1e-6, the accuracy bound of the mixed path;
   C4  3-D 384x192x128, WENO5, mixed precision with the learned start (the benchmark's
       configuration) against the FP64 device path after 10 steps: the same bound, div B at
       round-off, at most 1% fallbacks from the learned start and no failed inversion.
