@@ -8,7 +8,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIBDIR = os.environ.get("HARM_B200_LIBDIR") or os.path.join(HERE, "lib")
 
 HARM_NPR = 8
-HARM_LIM_MC, HARM_LIM_PARA, HARM_LIM_WENO5 = 0, 1, 2
+HARM_LIM_MC, HARM_LIM_PARA, HARM_LIM_WENO5, HARM_LIM_PARALINE = 0, 1, 2, 3
 HARM_PREC_FP64, HARM_PREC_MIXED = 0, 1
 HARM_GUESS_PREV, HARM_GUESS_MLP = 0, 1
 HARM_LOC_CENT, HARM_LOC_FACE1, HARM_LOC_FACE2, HARM_LOC_CORN3 = 0, 1, 2, 3

@@ -34,9 +34,10 @@ extern "C" const char* harm_b200_last_error(void) { return g_errbuf; }
 // the context of grid g on `device` with every buffer allocated; the tables are filled by
 // the caller (upload or device build)
 static int create_ctx(const harm_grid* g, int device, harm_ctx** out) {
-  if (g->lim != HARM_LIM_MC && g->lim != HARM_LIM_PARA && g->lim != HARM_LIM_WENO5)
+  if (g->lim != HARM_LIM_MC && g->lim != HARM_LIM_PARA && g->lim != HARM_LIM_WENO5 && g->lim != HARM_LIM_PARALINE)
     return seterr_msg("unknown reconstruction", 2);
   if (g->lim == HARM_LIM_WENO5 && g->ng < 6) return seterr_msg("WENO5 needs ng >= 6", 2);
+  if (g->lim == HARM_LIM_PARALINE && g->ng < 4) return seterr_msg("PARALINE needs ng >= 4", 2);
   harm_ctx* c = new harm_ctx();
   memset((void*)c, 0, sizeof(*c));
   c->g = *g;

@@ -274,8 +274,10 @@ __global__ void __launch_bounds__(256) k_flux(Dims d, Phys ph, FaceBox fb, const
 // One block of 256 threads = a tile of A = 32 faces of direction DIR times NT = 8 transverse
 // lines, consecutive threads along i so that every global load is coalesced.  VB primitives
 // at a time (all 8 in FP32, 4 in FP64) are staged in shared memory with the stencil halo along
-// DIR; the block then computes every cell's reconstruction once (MC slope, para4, or the WENO5
-// weights and then the edge values), three barriers per group instead of three per primitive.
+// DIR; the block then computes every cell's reconstruction once (MC slope, para4, the WENO5
+// weights and then the edge values, or PARALINE's edges after a pass that computes each
+// staged cell's V and total pressure and each edge cell's flattening coefficient), three
+// barriers per group instead of three per primitive.
 // Each thread keeps the two states of its own face and evaluates states, fluxes, wave speeds
 // and the HLL flux of that face.
 template <int LIM>
@@ -292,6 +294,10 @@ template <>
 struct ReconGeom<HARM_LIM_WENO5> {
   static constexpr int H = 5, X = 4;
 };
+template <>
+struct ReconGeom<HARM_LIM_PARALINE> {
+  static constexpr int H = 4, X = 3;  // para edges need cells -2..2, the flattener -3..3
+};
 
 template <int LIM, typename T>
 struct FluxTile {
@@ -304,7 +310,8 @@ struct FluxTile {
   static constexpr int PLANE = NL * NT;               // staged values of one primitive
   static constexpr int PE = (A + 1) * NT;              // edge values: cells H-1 .. H+A-1
   static constexpr int PW = (NL - 4) * NT;             // WENO5 weights: cells 2 .. NL-3
-  static constexpr size_t smem = (size_t)VB * (PLANE + 2 * PE + NW * PW) * sizeof(T);
+  static constexpr int NF = (LIM == HARM_LIM_PARALINE) ? 1 : 0;  // PARALINE: V, P, Fi planes
+  static constexpr size_t smem = ((size_t)VB * (PLANE + 2 * PE + NW * PW) + (size_t)NF * (2 * PLANE + PE)) * sizeof(T);
 };
 
 // The face physics of k_fluxt: B^DIR continuity, limit_gamma, states, fluxes, wave speeds and
@@ -368,6 +375,9 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
   T* s_el = s_y + VB * PL;                    // left edge of each cell, [VB][PE]
   T* s_er = s_el + VB * PE;                   // right edge of each cell, [VB][PE]
   T* s_w = s_er + VB * PE;                    // WENO5 unoptimised weights, [VB][PW][3]
+  T* s_V = s_w + VB * PW * TL::NW;            // PARALINE: sqrt(-g) rho u^DIR, [plane]
+  T* s_P = s_V + PL;                          // PARALINE: p + b^2/2, [plane]
+  T* s_F = s_P + PL;                          // PARALINE: flattening coefficient, [PE]
   // a plane is [NT][NL] for DIR 1 and [NL][NT] otherwise: the index along i is contiguous
   auto sx = [](int c, int t) -> int { return (DIR == 1) ? t * NL + c : c * NT + t; };
   // edge planes hold cells H-1 .. H+A-1, weight planes cells 2 .. NL-3, in the same layout
@@ -412,6 +422,43 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
     if (DIR == 2) return cidx(d, text, lext, o + d.ng3);
     return cidx(d, text, o + d.ng, lext);
   };
+  if constexpr (LIM == HARM_LIM_PARALINE) {
+    // get_V_and_P (interpline.c:2964) of every staged cell from all its primitives and the
+    // cell-centre metric, then the flattening coefficient of each edge cell; the first
+    // staging group's barrier orders the s_F writes before the edge loop reads them
+    const T gam = (T)ph.gam;
+    for (int idx = tid; idx < PL; idx += 256) {
+      int v, cl, ct;
+      split(idx, 0, NL, v, cl, ct);
+      const int lext = min(max(l0 - H + cl + ngL, 0), nLe - 1);
+      const int text = min(max(t0 + ct + d.ng, 0), nTe - 1);
+      const size_t cid = cell_index(lext, text);
+      T pc[NPR];
+#pragma unroll
+      for (int p = 0; p < NPR; p++) pc[p] = (T)__ldg(P + (size_t)p * d.cells + cid);
+      const int ii = (DIR == 1) ? lext : text, jj = (DIR == 1) ? text : (DIR == 2) ? lext : o + d.ng;
+      Geo<T> g;
+      load_geo<T, GT>(geom + (size_t)HARM_LOC_CENT * HARM_NGF * d.plane, d.plane, (size_t)jj * d.n1e + ii, g);
+      State<T> q;
+      get_state<T>(pc, g, gam, q);
+      s_V[sx(cl, ct)] = g.gdet * pc[HARM_RHO] * q.ucon[DIR];
+      T pt = q.pressure;
+      pt += T(0.5) * q.bsq;
+      s_P[sx(cl, ct)] = pt;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < (A + 1) * NT; idx += 256) {
+      int v, c, t;
+      split(idx, H - 1, A + 1, v, c, t);
+      T vv[7], pp[7];
+#pragma unroll
+      for (int q = 0; q < 7; q++) {
+        vv[q] = s_V[sx(c - 3 + q, t)];
+        pp[q] = s_P[sx(c - 3 + q, t)];
+      }
+      s_F[ex(c, t)] = paraline_fi<T>(vv, pp);
+    }
+  }
   T pl[NPR], pr[NPR];
 #pragma unroll
   for (int p0 = 0; p0 < NPR; p0 += VB) {
@@ -528,6 +575,17 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
         T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
         T yl, yr;
         para4_cell<T>(u5 + 2, yl, yr);
+        s_el[v * PE + ex(c, t)] = yl;
+        s_er[v * PE + ex(c, t)] = yr;
+      }
+    } else if (LIM == HARM_LIM_PARALINE) {
+      for (int idx = tid; idx < VB * (A + 1) * NT; idx += 256) {
+        int v, c, t;
+        split(idx, H - 1, A + 1, v, c, t);
+        const T* y = s_y + v * PL;
+        T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
+        T yl, yr;
+        paraline_cell<T>(u5 + 2, s_F[ex(c, t)], yl, yr);
         s_el[v * PE + ex(c, t)] = yl;
         s_er[v * PE + ex(c, t)] = yr;
       }

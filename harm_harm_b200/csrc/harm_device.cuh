@@ -233,6 +233,21 @@ __device__ __forceinline__ T minmod2(T a, T b) {
   return (a * b <= T(0)) ? T(0) : ((fabs(a) < fabs(b)) ? a : b);
 }
 
+// checkparamonotonicity (interppoint.para.c:1069) with smooth = 0, PARAGENDQALLOWEXTREMUM = 0,
+// NONMONOLIM = 0 and the a6 coefficient of point values (4)
+template <typename T>
+__device__ __forceinline__ void para_monotonicity(T y0, T& l, T& r) {
+  const T a6 = T(4);
+  T qa = (r - y0) * (y0 - l), qd = (r - l), qe = a6 * (y0 - T(0.5) * (l + r));
+  if (qa <= T(0)) {
+    l = y0;
+    r = y0;
+  } else {
+    if (qd * (qd - qe) < T(0)) l = (-(T(2) + a6) * r + T(2) * a6 * y0) / (a6 - T(2));
+    else if (qd * (qd + qe) < T(0)) r = (-(T(2) + a6) * l + T(2) * a6 * y0) / (a6 - T(2));
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ void para4_cell(const T* y, T& lout, T& rout) {
   T dq[3];
@@ -245,15 +260,77 @@ __device__ __forceinline__ void para4_cell(const T* y, T& lout, T& rout) {
   T ddql = dq[1] - dq[0], ddqr = dq[2] - dq[1];
   T l = T(0.5) * (y[0] + y[-1]) - ddql * T(1.0 / 8.0);
   T r = T(0.5) * (y[1] + y[0]) - ddqr * T(1.0 / 8.0);
-  const T a6 = T(4);
-  T qa = (r - y[0]) * (y[0] - l), qd = (r - l), qe = a6 * (y[0] - T(0.5) * (l + r));
-  if (qa <= T(0)) {
-    l = y[0];
-    r = y[0];
-  } else {
-    if (qd * (qd - qe) < T(0)) l = (-(T(2) + a6) * r + T(2) * a6 * y[0]) / (a6 - T(2));
-    else if (qd * (qd + qe) < T(0)) r = (-(T(2) + a6) * l + T(2) * a6 * y[0]) / (a6 - T(2));
-  }
+  para_monotonicity<T>(y[0], l, r);
+  lout = l;
+  rout = r;
+}
+
+// ---------------------------------------------------------------- line PPM (PARALINE)
+// pass_1d_line_multipl_paraline (interpline.para.c:8) with DOPPMREDUCE=1 and the other
+// switches of para_and_paraenohybrid.h at their defaults: MC slopes that keep the extremum
+// (get_limit_slopes_paraline :165, PARALINE2EXTREME=1), continuous face values (paracont
+// interppoint.para.c:958), both edges pulled towards the cell value by the flattening
+// coefficient Fi (paraflatten :1305), then checkparamonotonicity (:1069).  Fi is FLASH's
+// flattener (Ficalc :1356, ftilde :1316, SP0 = 0.75) of V = sqrt(-g) rho u^dir and the total
+// pressure P = p + b^2/2 of the cells -3..3 (get_V_and_P interpline.c:2964).  The reference's
+// max/min (phys.tools.c:2356) are a > b ? a : b and a > b ? b : a, kept as written.
+template <typename T>
+struct ParalineConst;
+template <>
+struct ParalineConst<double> {
+  static constexpr double small = 1.e-300;               // SMALL of a double build
+  static constexpr double third = 0x1.5555555555556p-2;  // least double >= the long double 1/3
+};
+template <>
+struct ParalineConst<float> {
+  static constexpr float small = 1.e-35f;                // SMALL of a float build
+  static constexpr float third = 0x1.555556p-2f;         // least float >= 1/3
+};
+
+// ftilde of one cell from V at its neighbours -1, +1 and P at -2..2
+template <typename T>
+__device__ __forceinline__ T paraline_ftilde(T vm1, T vp1, T pm2, T pm1, T pp1, T pp2) {
+  using K = ParalineConst<T>;
+  const T P2diff = pp2 - pm2;
+  const T Pbottom = copysign(T(1), P2diff) / (fabs(P2diff) + K::small);
+  const T Sp = (pp1 - pm1) * Pbottom;
+  const T m = T(10) * (Sp - T(0.75));
+  const T mn = (T(1) > m) ? m : T(1);
+  T Ft = (T(0) > mn) ? T(0) : mn;
+  const T a = fabs(pp1), b = fabs(pm1);
+  const T Ft1 = fabs(pp1 - pm1) / (((a > b) ? b : a) + K::small);
+  Ft *= (Ft1 >= K::third) ? T(1) : T(0);
+  Ft *= (vp1 - vm1 <= T(0)) ? T(1) : T(0);
+  return Ft;
+}
+
+// Fi of the cell at v[3], p[3] (v, p: cells -3..3): the larger of its own ftilde and that of
+// its neighbour on the side of lower pressure (shift -sign(P[1] - P[-1]), ties to +1)
+template <typename T>
+__device__ __forceinline__ T paraline_fi(const T* v, const T* p) {
+  const T f0 = paraline_ftilde<T>(v[2], v[4], p[1], p[2], p[4], p[5]);
+  const T f1 = (p[4] - p[2] > T(0)) ? paraline_ftilde<T>(v[1], v[3], p[0], p[1], p[3], p[4])
+                                    : paraline_ftilde<T>(v[3], v[5], p[2], p[3], p[5], p[6]);
+  return (f0 > f1) ? f0 : f1;
+}
+
+template <typename T>
+__device__ __forceinline__ T paraline_dq(T ym, T y0, T yp) {
+  const T Dqm = T(2) * (y0 - ym), Dqp = T(2) * (yp - y0), Dqc = T(0.5) * (yp - ym);
+  const T m1 = (fabs(Dqm) < fabs(Dqp)) ? Dqm : Dqp;
+  return (fabs(Dqc) < fabs(m1)) ? Dqc : m1;
+}
+
+// edges of the cell at y[0] (uses y[-2..2]) with flattening coefficient fi
+template <typename T>
+__device__ __forceinline__ void paraline_cell(const T* y, T fi, T& lout, T& rout) {
+  const T dqm = paraline_dq<T>(y[-2], y[-1], y[0]), dq0 = paraline_dq<T>(y[-1], y[0], y[1]);
+  const T dqp = paraline_dq<T>(y[0], y[1], y[2]);
+  T l = T(0.5) * (y[0] + y[-1]) - (dq0 - dqm) * T(1.0 / 8.0);
+  T r = T(0.5) * (y[1] + y[0]) - (dqp - dq0) * T(1.0 / 8.0);
+  l = fi * y[0] + (T(1) - fi) * l;
+  r = fi * y[0] + (T(1) - fi) * r;
+  para_monotonicity<T>(y[0], l, r);
   lout = l;
   rout = r;
 }

@@ -293,6 +293,7 @@ int hp_fluxes_fp64(harm_ctx* c, const double* pb, double* F1, double* F2, double
   Phys ph = phys_of(c->g);
   if (c->g.lim == HARM_LIM_WENO5) { int rc = flux_dirs_double<HARM_LIM_WENO5>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
   else if (c->g.lim == HARM_LIM_PARA) { int rc = flux_dirs_double<HARM_LIM_PARA>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
+  else if (c->g.lim == HARM_LIM_PARALINE) { int rc = flux_dirs_double<HARM_LIM_PARALINE>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
   else { int rc = flux_dirs_double<HARM_LIM_MC>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
   long long nc = (long long)(d.n1 + 1) * (d.n2 + 1) * (d.n3 > 1 ? d.n3 + 1 : 1);
   k_emf<double, double><<<nblk(nc), 256, 0, c->stream>>>(d, F1, F2, F3, c->d_geom, emf);

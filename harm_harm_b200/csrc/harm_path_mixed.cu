@@ -72,15 +72,18 @@ template <int LIM>
 static int flux_dirs_float(harm_ctx* c, const Dims& d, const Phys& ph, const double* pb, float* F1, float* F2, float* F3,
                          unsigned long long* slots) {
   FaceBox b1 = face_box(d, 1), b2 = face_box(d, 2), b3 = face_box(d, 3);
-  if (tma_usable(c, pb)) {
-    if (int rc = launch_fluxt_tma<1, LIM>(c, d, ph, b1, pb, F1, slots + 0)) return rc;
-    if (int rc = launch_fluxt_tma<2, LIM>(c, d, ph, b2, pb, F2, slots + 1)) return rc;
-    c->launches += 2;
-    if (d.n3 > 1) {
-      if (int rc = launch_fluxt_tma<3, LIM>(c, d, ph, b3, pb, F3, slots + 2)) return rc;
-      c->launches++;
+  // the TMA-staged variant covers MC, PARA and WENO5; PARALINE always takes k_fluxt
+  if constexpr (LIM != HARM_LIM_PARALINE) {
+    if (tma_usable(c, pb)) {
+      if (int rc = launch_fluxt_tma<1, LIM>(c, d, ph, b1, pb, F1, slots + 0)) return rc;
+      if (int rc = launch_fluxt_tma<2, LIM>(c, d, ph, b2, pb, F2, slots + 1)) return rc;
+      c->launches += 2;
+      if (d.n3 > 1) {
+        if (int rc = launch_fluxt_tma<3, LIM>(c, d, ph, b3, pb, F3, slots + 2)) return rc;
+        c->launches++;
+      }
+      return 0;
     }
-    return 0;
   }
   CK((launch_fluxt<1, LIM, float, float>(d, ph, b1, pb, c->d_geomf, F1, slots + 0, c->stream)));
   CK((launch_fluxt<2, LIM, float, float>(d, ph, b2, pb, c->d_geomf, F2, slots + 1, c->stream)));
@@ -98,6 +101,7 @@ int hp_fluxes_mixed(harm_ctx* c, const double* pb, float* F1, float* F2, float* 
   Phys ph = phys_of(c->g);
   if (c->g.lim == HARM_LIM_WENO5) { int rc = flux_dirs_float<HARM_LIM_WENO5>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
   else if (c->g.lim == HARM_LIM_PARA) { int rc = flux_dirs_float<HARM_LIM_PARA>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
+  else if (c->g.lim == HARM_LIM_PARALINE) { int rc = flux_dirs_float<HARM_LIM_PARALINE>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
   else { int rc = flux_dirs_float<HARM_LIM_MC>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
   long long nc = (long long)(d.n1 + 1) * (d.n2 + 1) * (d.n3 > 1 ? d.n3 + 1 : 1);
   k_emf<float, float><<<nblk(nc), 256, 0, c->stream>>>(d, F1, F2, F3, c->d_geomf, emf);

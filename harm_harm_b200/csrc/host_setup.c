@@ -30,11 +30,11 @@ static inline int sym_index(int m, int n) {
 int harm_grid_setup(harm_grid *g, int n1, int n2, int n3, int lim, double a,
                     double hslope, double Rout, double cour) {
   if (!g || n1 < 2 || n2 < 2 || n3 < 1) return 1;
-  if (lim != HARM_LIM_MC && lim != HARM_LIM_PARA && lim != HARM_LIM_WENO5) return 1;
+  if (lim != HARM_LIM_MC && lim != HARM_LIM_PARA && lim != HARM_LIM_WENO5 && lim != HARM_LIM_PARALINE) return 1;
   memset(g, 0, sizeof(*g));
   g->n1 = n1; g->n2 = n2; g->n3 = n3;
   g->lim = lim;
-  /* MAXBND: 4 for MC/PARA, 6 for WENO5BND (initboundcode/init.fishmon.h) */
+  /* MAXBND: 4 for MC/PARA/PARALINE, 6 for WENO5BND (initboundcode/init.fishmon.h) */
   g->ng = (lim == HARM_LIM_WENO5) ? 6 : 4;
   g->ng3 = (n3 > 1) ? g->ng : 0;
   g->n1e = n1 + 2 * g->ng;

@@ -47,8 +47,10 @@ extern "C" {
 enum { HARM_RHO = 0, HARM_UU = 1, HARM_U1 = 2, HARM_U2 = 3, HARM_U3 = 4,
        HARM_B1 = 5, HARM_B2 = 6, HARM_B3 = 7 };
 
-/* reconstruction choices (HARM lim[]: MC, PARA, WENO5BND; init.tools.c:128) */
-enum { HARM_LIM_MC = 0, HARM_LIM_PARA = 1, HARM_LIM_WENO5 = 2 };
+/* reconstruction choices (HARM lim[]: MC, PARA, WENO5BND, PARALINE; init.tools.c:128).
+   PARALINE is the line PPM of interpline.para.c: extremum-preserving MC slopes and FLASH
+   shock flattening from the cell's total pressure and sqrt(-g) rho u^dir; it needs ng >= 4. */
+enum { HARM_LIM_MC = 0, HARM_LIM_PARA = 1, HARM_LIM_WENO5 = 2, HARM_LIM_PARALINE = 3 };
 
 /* arithmetic of the flux path: FP64 everywhere, or FP32 reconstruction/HLL/CT with the
    conserved update, inversion and metric kept in FP64 */

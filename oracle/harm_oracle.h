@@ -51,8 +51,16 @@ int orc_advance(orc *o, int timeorder, int numtimeorders, const double *pi, cons
 int orc_post_fixup(orc *o, double *pf, int8_t *pflag);
 int orc_step(orc *o, double *P, double *dt, harm_stats *st);
 
-/* reconstruction of one line (tests): y[n] -> left/right face states of faces 3..n-3 */
+/* reconstruction of one line (tests): y[n] -> left/right edge values of each cell whose
+   stencil fits (lim = PARALINE here without flattening) */
 void orc_reconstruct_line(int lim, int n, const double *y, double *pl, double *pr);
+/* PARALINE with the flattening of V[n] (sqrt(-g) rho u^dir) and P[n] (total pressure) */
+void orc_paraline_flattener(int n, const double *V, const double *P, double *Fi);
+void orc_reconstruct_line_paraline(int n, const double *y, const double *V, const double *P, double *pl,
+                                   double *pr);
+/* the PARALINE flattening coefficients fluxcalc uses on the line along dir through the
+   transverse active-relative indices (a, b); Fi has the line's extended length */
+void orc_paraline_line_fi(const orc *o, const double *pb, int dir, int a, int b, double *Fi);
 
 /* the 52 columns of one row of the main dump file (dump_content, dump.c:449) for active cell
    (i, j, k); U may be NULL (primtoU of P) */

@@ -60,6 +60,9 @@ def lib() -> C.CDLL:
             "orc_post_fixup": (I, [C.POINTER(orc), P, P]),
             "orc_step": (I, [C.POINTER(orc), P, C.POINTER(D), C.POINTER(N.harm_stats)]),
             "orc_reconstruct_line": (None, [I, I, P, P, P]),
+            "orc_paraline_flattener": (None, [I, P, P, P]),
+            "orc_reconstruct_line_paraline": (None, [I, P, P, P, P, P]),
+            "orc_paraline_line_fi": (None, [C.POINTER(orc), P, I, I, I, P]),
             "orc_mlp_nparams": (I, []),
             "orc_mlp_features": (None, [C.POINTER(N.harm_grid), P, P, P, P, P]),
             "orc_mlp_loss_grad": (D, [I, P, P, P, P, P, P]),
@@ -120,6 +123,16 @@ class Oracle:
             out[n] = row
         return out
 
+    def paraline_line_fi(self, P, d, a, b):
+        """PARALINE flattening coefficients fluxcalc uses on the line along direction d through
+        the transverse active-relative indices (a, b); length = the line's extended size"""
+        Pc = np.ascontiguousarray(P, dtype=np.float64)
+        gg = self.grid.g
+        n = {1: gg.n1e, 2: gg.n2e, 3: gg.n3e}[d]
+        Fi = np.zeros(n)
+        lib().orc_paraline_line_fi(C.byref(self.o), _p(Pc), int(d), int(a), int(b), _p(Fi))
+        return Fi
+
     def step_ch(self, P, dt):
         d = C.c_double(dt)
         st = N.harm_stats()
@@ -160,6 +173,23 @@ def reconstruct_line(lim, y):
     yl = np.zeros_like(y)
     yr = np.zeros_like(y)
     lib().orc_reconstruct_line(lim, len(y), _p(y), _p(yl), _p(yr))
+    return yl, yr
+
+
+def paraline_flattener(V, P):
+    """PARALINE flattening coefficient of each cell of a line (0 where the +-3 stencil does not fit)"""
+    V, P = _c(V), _c(P)
+    Fi = np.zeros_like(V)
+    lib().orc_paraline_flattener(len(V), _p(V), _p(P), _p(Fi))
+    return Fi
+
+
+def reconstruct_line_paraline(y, V, P):
+    """PARALINE edges of a line with the flattening of V = sqrt(-g) rho u^dir and P = p + b^2/2"""
+    y, V, P = _c(y), _c(V), _c(P)
+    yl = np.zeros_like(y)
+    yr = np.zeros_like(y)
+    lib().orc_reconstruct_line_paraline(len(y), _p(y), _p(V), _p(P), _p(yl), _p(yr))
     return yl, yr
 
 

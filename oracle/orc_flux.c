@@ -2,7 +2,7 @@
  * orc_flux.c -- TEST INFRASTRUCTURE ONLY (CPU oracle; see harm_oracle.h).
  *
  * fluxcalc (flux.c:38) restated: per direction, line reconstruction of the primitives
- * (orc_recon.c), face states with B^dir made continuous (getplpr flux.c:1952, BDIRCONT=1)
+ * (orc_recon.c; for PARALINE with the flattening coefficients of the line), face states with B^dir made continuous (getplpr flux.c:1952, BDIRCONT=1)
  * and limit_gamma on each side (check_plpr flux.c:2041, EVOLVECHECKS=1), fluid state and
  * fluxes of both sides (p2SFUevolve fluxcompute.c:122), vchar wave speeds and
  * cminmax_calc (wavespeeds.c:12, :397, ROEAVERAGEDWAVESPEED=0), the HLL flux with the
@@ -62,6 +62,39 @@ static void face_flux(const orc *o, int dir, const ogeom *g, double *pl, double 
   }
 }
 
+/* PARALINE flattening coefficients of the line along dir through the transverse
+   active-relative indices (a, b) (dir 1: (j, k), dir 2: (i, k), dir 3: (i, j)):
+   get_V_and_P (interpline.c:2964) gives V = sqrt(-g) rho u^dir and P = p + b^2/2 of every cell
+   of the line at the cell centre, then o_paraline_flattener */
+static void paraline_line_fi(const orc *o, const double *pb, int dir, int a, int b, double *Fi) {
+  const harm_grid *g = &o->g;
+  const int ng = g->ng, ng3 = g->ng3;
+  const int nline = (dir == 1) ? g->n1e : (dir == 2) ? g->n2e : g->n3e;
+  double *V = (double *)malloc(sizeof(double) * nline), *Pt = (double *)malloc(sizeof(double) * nline);
+  for (int s = 0; s < nline; s++) {
+    int ii, jj, kk;
+    if (dir == 1) { ii = s; jj = a + ng; kk = b + ng3; }
+    else if (dir == 2) { ii = a + ng; jj = s; kk = b + ng3; }
+    else { ii = a + ng; jj = b + ng; kk = s; }
+    double pr[HARM_NPR];
+    for (int p = 0; p < HARM_NPR; p++) pr[p] = pb[(size_t)p * o->cells + oidx(o, ii, jj, kk)];
+    ogeom gc;
+    og_load(o, HARM_LOC_CENT, ii, jj, &gc);
+    ostate q;
+    o_get_state(pr, &gc, g->gam, &q);
+    V[s] = gc.gdet * pr[HARM_RHO] * q.ucon[dir];
+    Pt[s] = q.pressure;
+    Pt[s] += 0.5 * q.bsq;
+  }
+  o_paraline_flattener(nline, V, Pt, Fi);
+  free(V);
+  free(Pt);
+}
+
+void orc_paraline_line_fi(const orc *o, const double *pb, int dir, int a, int b, double *Fi) {
+  paraline_line_fi(o, pb, dir, a, b, Fi);
+}
+
 int orc_fluxcalc(orc *o, const double *pb, double *F1, double *F2, double *F3, double ndt[3]) {
   const harm_grid *g = &o->g;
   const size_t cells = o->cells;
@@ -86,6 +119,11 @@ int orc_fluxcalc(orc *o, const double *pb, double *F1, double *F2, double *F3, d
         double *yr = (double *)malloc(sizeof(double) * nline * HARM_NPR);
         /* extended transverse indices */
         int e[3];
+        double *Fi = NULL;
+        if (g->lim == HARM_LIM_PARALINE) {
+          Fi = (double *)malloc(sizeof(double) * nline);
+          paraline_line_fi(o, pb, dir, a, b, Fi);
+        }
         for (int p = 0; p < HARM_NPR; p++) {
           for (int s = 0; s < nline; s++) {
             int ii, jj, kk;
@@ -94,8 +132,10 @@ int orc_fluxcalc(orc *o, const double *pb, double *F1, double *F2, double *F3, d
             else { ii = a + ng; jj = b + ng; kk = s; }
             y[s] = pb[(size_t)p * cells + oidx(o, ii, jj, kk)];
           }
-          o_recon_line(g->lim, nline, y, yl + (size_t)p * nline, yr + (size_t)p * nline);
+          if (Fi) o_recon_line_paraline(nline, y, Fi, yl + (size_t)p * nline, yr + (size_t)p * nline);
+          else o_recon_line(g->lim, nline, y, yl + (size_t)p * nline, yr + (size_t)p * nline);
         }
+        free(Fi);
         int off = (dir == 3) ? ng3 : ng;
         for (int f = lo[dir - 1]; f <= hi[dir - 1]; f++) {
           int s = f + off; /* extended index of the cell above the face */

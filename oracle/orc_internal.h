@@ -33,6 +33,10 @@ int o_fixup1zone(double *pr, const ogeom *g, double rhofl, double ufl, double ga
 
 /* reconstruction of a 1-D line of n values at n-? faces; see orc_recon.c */
 void o_recon_line(int lim, int n, const double *y, double *yl, double *yr);
+/* PARALINE: flattening coefficients of cells 3..n-4 from V, P (others 0), and the edges of a
+   line with given coefficients (Fi NULL: none); see orc_recon_hi.c */
+void o_paraline_flattener(int n, const double *V, const double *P, double *Fi);
+void o_recon_line_paraline(int n, const double *y, const double *Fi, double *yl, double *yr);
 
 static inline size_t oidx(const orc *o, int ii, int jj, int kk) {
   return ((size_t)kk * o->g.n2e + jj) * o->g.n1e + ii;

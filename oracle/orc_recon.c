@@ -8,6 +8,8 @@
  *
  *   MC   : slope_lim_3points + get_limit_slopes (interppoint.c:753, :769):
  *          dq = MINMOD(dq2, MINMOD(2 dq1l, 2 dq1r)), edges y -/+ dq/2.
+ *   PARA, WENO5, PARALINE: orc_recon_hi.c (PARALINE's flattening needs the whole primitive
+ *          state of each cell and is applied by the flux loop, orc_flux.c).
  */
 #include <math.h>
 #include <string.h>
@@ -36,6 +38,8 @@ void o_recon_line(int lim, int n, const double *y, double *yl, double *yr) {
     }
   } else if (lim == HARM_LIM_PARA) {
     o_recon_line_para(n, y, yl, yr);
+  } else if (lim == HARM_LIM_PARALINE) {
+    o_recon_line_paraline(n, y, NULL, yl, yr);
   } else {
     o_recon_line_weno5(n, y, yl, yr);
   }

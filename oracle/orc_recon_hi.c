@@ -31,6 +31,24 @@
  * PARAGENDQALLOWEXTREMUM=0, AVGINPUT=0: MC-limited slopes dq of the cells -1,0,1, face values
  * from paracont (:958, 4th-order average minus ddq/8), then checkparamonotonicity (:1069,
  * NONMONOLIM=0, a6 coefficient 4).
+ *
+ * Line PPM (lim = PARALINE): pass_1d_line_multipl_paraline (interpline.para.c:8) with the
+ * switches of para_and_paraenohybrid.h and definit.h (DOPPMREDUCE=1, DOPPMCONTACTSTEEP=0,
+ * JONPARASMOOTH=0, PARALINEUSESMONO=0, NONMONOLIM=0):
+ *   - slopes dq[i] = MINMODB(dq2, MINMODB(2 dq1l, 2 dq1r)), the MC limiter with the extremum
+ *     allowed (compute_df_line_paraline interpline.c:3463, get_limit_slopes_paraline
+ *     interpline.para.c:165 with PARALINE2LIM=MC, PARALINE2EXTREME=1, MINMODGEN
+ *     global.nondepnmemonics.h:641);
+ *   - continuous face values facecont[i] = (y[i]+y[i-1])/2 - (dq[i]-dq[i-1])/8 (paracont
+ *     interppoint.para.c:958, DF2OFMONO);
+ *   - cell i: l = facecont[i], r = facecont[i+1], pulled towards y[i] by the flattening
+ *     coefficient Fi[i] (paraflatten :1305), then the same checkparamonotonicity as PARA4;
+ *   - Fi from the cell's V = sqrt(-g) rho u^dir and total pressure P = p + b^2/2
+ *     (get_V_and_P interpline.c:2964, VLINEWITHGDETRHO=1, PLINEWITHFIELD=1) through Ficalc
+ *     (interppoint.para.c:1356) and ftilde (:1316), FLASH's flattener with SP0 = 0.75
+ *     (get_shock_indicator interpline.c:3114).  The reference's max/min are the functions of
+ *     phys.tools.c:2356 (a > b ? a : b and a > b ? b : a), its sign() is copysign(1, a), and
+ *     the 1/3 threshold is the long double THIRD (global.nondepnmemonics.h:746).
  */
 #include <float.h>
 #include <math.h>
@@ -172,6 +190,8 @@ void o_recon_line_weno5(int n, const double *y, double *yl, double *yr) {
 #define MINMODB(a, b) ((fabs(a) < fabs(b)) ? (a) : (b))
 #define MINMOD(a, b) (((a) * (b) <= 0) ? 0.0 : MINMODB(a, b))
 
+static void para_monotonicity(const double *y, double *lio, double *rio);
+
 /* para4 of the cell at y[0] (uses y[-2..2]) */
 static void para4(const double *y, double *lout, double *rout) {
   double dq1[4], dq2[3], dq[3];
@@ -187,7 +207,15 @@ static void para4(const double *y, double *lout, double *rout) {
   double ddql = (dq[1] - dq[0]), ddqr = (dq[2] - dq[1]);
   double l = 0.5 * (y[0] + y[-1]) - ddql * (1.0 / 8.0);
   double r = 0.5 * (y[1] + y[0]) - ddqr * (1.0 / 8.0);
-  /* checkparamonotonicity */
+  para_monotonicity(y, &l, &r);
+  *lout = l;
+  *rout = r;
+}
+
+/* checkparamonotonicity (interppoint.para.c:1069) with smooth = 0 and
+   PARAGENDQALLOWEXTREMUM = 0 */
+static void para_monotonicity(const double *y, double *lio, double *rio) {
+  double l = *lio, r = *rio;
   double a6 = 4.0;
   double qa = (r - y[0]) * (y[0] - l), qd = (r - l), qe = a6 * (y[0] - 0.5 * (l + r));
   if (qa <= 0.0) {
@@ -197,11 +225,76 @@ static void para4(const double *y, double *lout, double *rout) {
     if (qd * (qd - qe) < 0.0) l = (-(2.0 + a6) * r + 2.0 * a6 * y[0]) / (a6 - 2.0);
     else if (qd * (qd + qe) < 0.0) r = (-(2.0 + a6) * l + 2.0 * a6 * y[0]) / (a6 - 2.0);
   }
-  *lout = l;
-  *rout = r;
+  *lio = l;
+  *rio = r;
 }
 
 void o_recon_line_para(int n, const double *y, double *yl, double *yr) {
   for (int c = 0; c < n; c++) yl[c] = yr[c] = y[c];
   for (int c = 2; c < n - 2; c++) para4(y + c, &yl[c], &yr[c]);
+}
+
+/* ftilde (interppoint.para.c:1316) of the cell at V[0], P[0]: uses P[-2..2], V[-1], V[1] */
+static double paraline_ftilde(const double *V, const double *P) {
+  double P2diff = P[2] - P[-2];
+  double Pbottom = copysign(1.0, P2diff) / (fabs(P2diff) + O_SMALL);
+  double Sp = (P[1] - P[-1]) * Pbottom;
+  double m = 10.0 * (Sp - 0.75);          /* SP0 */
+  double mn = (1.0 > m) ? m : 1.0;        /* min(1.0, m) */
+  double Ft = (0.0 > mn) ? 0.0 : mn;      /* max(0, mn) */
+  double a = fabs(P[1]), b = fabs(P[-1]);
+  double Ft1 = fabs(P[1] - P[-1]) / (((a > b) ? b : a) + O_SMALL);
+  Ft *= (double)((long double)Ft1 >= 0.3333333333333333333333333333333333L);
+  double Ft2 = V[1] - V[-1];
+  Ft *= (double)(Ft2 <= 0.0);
+  return Ft;
+}
+
+/* Ficalc (interppoint.para.c:1356): uses V[-3..3], P[-3..3] */
+static double paraline_fi(const double *V, const double *P) {
+  int signdP = (P[1] - P[-1] > 0) * 2 - 1;
+  double f0 = paraline_ftilde(V, P), f1 = paraline_ftilde(V - signdP, P - signdP);
+  return (f0 > f1) ? f0 : f1;
+}
+
+void o_paraline_flattener(int n, const double *V, const double *P, double *Fi) {
+  for (int s = 0; s < n; s++) Fi[s] = 0.0;
+  for (int s = 3; s < n - 3; s++) Fi[s] = paraline_fi(V + s, P + s);
+}
+
+/* slope of the cell at y[0]: MC with the extremum allowed */
+static double paraline_dq(const double *y) {
+  double dq1l = y[0] - y[-1], dq1r = y[1] - y[0], dq2 = 0.5 * (y[1] - y[-1]);
+  double Dqm = 2.0 * dq1l, Dqp = 2.0 * dq1r, Dqc = dq2;
+  return MINMODB(Dqc, MINMODB(Dqm, Dqp));
+}
+
+void o_recon_line_paraline(int n, const double *y, const double *Fi, double *yl, double *yr) {
+  for (int c = 0; c < n; c++) yl[c] = yr[c] = y[c];
+  if (n < 5) return;
+  double *dq = (double *)calloc((size_t)n, sizeof(double));
+  for (int c = 1; c < n - 1; c++) dq[c] = paraline_dq(y + c);
+  for (int c = 2; c < n - 2; c++) {
+    double l = 0.5 * (y[c] + y[c - 1]) - (dq[c] - dq[c - 1]) * (1.0 / 8.0);
+    double r = 0.5 * (y[c + 1] + y[c]) - (dq[c + 1] - dq[c]) * (1.0 / 8.0);
+    double f = Fi ? Fi[c] : 0.0;
+    l = f * y[c] + (1.0 - f) * l;
+    r = f * y[c] + (1.0 - f) * r;
+    para_monotonicity(y + c, &l, &r);
+    yl[c] = l;
+    yr[c] = r;
+  }
+  free(dq);
+}
+
+void orc_paraline_flattener(int n, const double *V, const double *P, double *Fi) {
+  o_paraline_flattener(n, V, P, Fi);
+}
+
+void orc_reconstruct_line_paraline(int n, const double *y, const double *V, const double *P, double *pl,
+                                   double *pr) {
+  double *Fi = (double *)calloc((size_t)n, sizeof(double));
+  o_paraline_flattener(n, V, P, Fi);
+  o_recon_line_paraline(n, y, Fi, pl, pr);
+  free(Fi);
 }

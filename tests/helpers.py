@@ -13,6 +13,29 @@ def make_torus(n1=64, n2=64, n3=1, lim=0, seed=12345, beta=100.0):
     return g, geom, conn, aux, P
 
 
+def plant_compression(grid, P, amp=10.0, v=(0.1, 0.02, 0.05), width=3, dense_frac=0.2):
+    """A strong, converging pressure jump inside the torus (in place, ghosts included): where
+    rho exceeds dense_frac of its maximum, the internal energy is multiplied by amp in the
+    block i >= n1/2, j >= n2/2, k >= n3/2, and within `width` cells of the block's faces the
+    velocity primitives get +-v pointing at those faces, so that the PARALINE flattener
+    switches on along every direction while every inversion still succeeds."""
+    g = grid.g
+    k_, j_, i_ = np.meshgrid(np.arange(g.n3e) - g.ng3, np.arange(g.n2e) - g.ng, np.arange(g.n1e) - g.ng,
+                             indexing="ij")
+    i0, j0, k0 = g.n1 // 2, g.n2 // 2, g.n3 // 2
+    dense = P[0] > dense_frac * P[0].max()
+    P[1][(i_ >= i0) & (j_ >= j0) & (k_ >= k0) & dense] *= amp
+
+    def towards(x, x0):
+        return np.where(x >= x0, -1.0, 1.0) * (np.abs(x - x0 + 0.5) < width) * dense
+
+    P[2] += v[0] * towards(i_, i0)
+    P[3] += v[1] * towards(j_, j0)
+    if g.n3 > 1:
+        P[4] += v[2] * towards(k_, k0)
+    return P
+
+
 def rel_err(a, b, floor_frac=1e-12):
     """max |a-b| / (|a|+|b| + floor), floor = floor_frac * max(|a|) (per array)"""
     a = np.asarray(a, dtype=np.float64)

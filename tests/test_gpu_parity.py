@@ -7,20 +7,25 @@ reconstruction/HLL/CT with FP64 update and inversion, compared with the FP64 pat
 import numpy as np
 import pytest
 
-from helpers import divb_corner, make_torus, rel_err
+from helpers import divb_corner, make_torus, plant_compression, rel_err
 from harm_harm_b200 import HARM_PREC_FP64, HARM_PREC_MIXED, Harm
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-CASES = {"2d_mc": (64, 64, 1, 0), "3d_mc": (32, 24, 8, 0), "3d_ppm": (32, 24, 8, 1),
-         "3d_weno5": (32, 24, 8, 2), "2d_weno5": (48, 48, 1, 2)}
+# (n1, n2, n3, lim, planted converging pressure jump); the PARALINE cases carry the planted
+# jump so that its shock flattener is active along every direction
+CASES = {"2d_mc": (64, 64, 1, 0, False), "3d_mc": (32, 24, 8, 0, False), "3d_ppm": (32, 24, 8, 1, False),
+         "3d_weno5": (32, 24, 8, 2, False), "2d_weno5": (48, 48, 1, 2, False),
+         "3d_paraline": (32, 24, 8, 3, True), "2d_paraline": (48, 48, 1, 3, True)}
 
 
 @pytest.fixture(scope="module", params=list(CASES))
 def setup(request, cuda):
-    n1, n2, n3, lim = CASES[request.param]
+    n1, n2, n3, lim, plant = CASES[request.param]
     g, geom, conn, aux, P = make_torus(n1, n2, n3, lim=lim)
+    if plant:
+        plant_compression(g, P)
     orc = O.Oracle(g, geom, conn, aux)
     orc.bound_prim(P)
     dev = Harm(g, geom, conn, aux)
