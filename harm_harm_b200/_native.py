@@ -9,6 +9,7 @@ LIBDIR = os.environ.get("HARM_B200_LIBDIR") or os.path.join(HERE, "lib")
 
 HARM_NPR = 8
 HARM_LIM_MC, HARM_LIM_PARA, HARM_LIM_WENO5, HARM_LIM_PARALINE = 0, 1, 2, 3
+HARM_FLUX_HLL, HARM_FLUX_LAXF = 0, 1
 HARM_PREC_FP64, HARM_PREC_MIXED = 0, 1
 HARM_GUESS_PREV, HARM_GUESS_MLP = 0, 1
 HARM_LOC_CENT, HARM_LOC_FACE1, HARM_LOC_FACE2, HARM_LOC_CORN3 = 0, 1, 2, 3
@@ -26,7 +27,7 @@ class harm_grid(C.Structure):
     _fields_ = [
         ("n1", C.c_int), ("n2", C.c_int), ("n3", C.c_int), ("ng", C.c_int),
         ("n1e", C.c_int), ("n2e", C.c_int), ("n3e", C.c_int), ("ng3", C.c_int),
-        ("lim", C.c_int), ("pad0", C.c_int),
+        ("lim", C.c_int), ("fluxmethod", C.c_int),
         ("startx", C.c_double * 4), ("dx", C.c_double * 4),
         ("a", C.c_double), ("hslope", C.c_double), ("R0", C.c_double), ("Rin", C.c_double),
         ("Rout", C.c_double), ("Rhor", C.c_double), ("gam", C.c_double), ("cour", C.c_double),

@@ -38,6 +38,7 @@ static int create_ctx(const harm_grid* g, int device, harm_ctx** out) {
     return seterr_msg("unknown reconstruction", 2);
   if (g->lim == HARM_LIM_WENO5 && g->ng < 6) return seterr_msg("WENO5 needs ng >= 6", 2);
   if (g->lim == HARM_LIM_PARALINE && g->ng < 4) return seterr_msg("PARALINE needs ng >= 4", 2);
+  if (g->fluxmethod != HARM_FLUX_HLL && g->fluxmethod != HARM_FLUX_LAXF) return seterr_msg("unknown fluxmethod", 2);
   harm_ctx* c = new harm_ctx();
   memset((void*)c, 0, sizeof(*c));
   c->g = *g;

@@ -50,6 +50,7 @@ __device__ __forceinline__ size_t cidx(const Dims& d, int ii, int jj, int kk) {
 struct Phys {
   double gam, cour, gammamax, gammafail, defcon, safe;
   double dx1, dx2, dx3;
+  int laxf;  // fluxmethod LAXF instead of HLL
 };
 
 static inline Phys phys_of(const harm_grid& g) {
@@ -57,6 +58,7 @@ static inline Phys phys_of(const harm_grid& g) {
   p.gam = g.gam; p.cour = g.cour; p.gammamax = g.gammamax; p.gammafail = g.gammafail;
   p.defcon = g.defcon; p.safe = g.safe;
   p.dx1 = g.dx[1]; p.dx2 = g.dx[2]; p.dx3 = g.dx[3];
+  p.laxf = (g.fluxmethod == HARM_FLUX_LAXF);
   return p;
 }
 
@@ -254,7 +256,7 @@ __global__ void __launch_bounds__(256) k_flux(Dims d, Phys ph, FaceBox fb, const
     lmin = fabs(fmax(T(0), -lmin));
     lmax = fabs(fmax(T(0), lmax));
     const T cmin = lmin, cmax = lmax, ctop = fmax(lmax, lmin);
-    if (cmax + cmin != T(0)) {
+    if (!ph.laxf && cmax + cmin != T(0)) {
       const T inv = cmax + cmin;
 #pragma unroll
       for (int p = 0; p < NPR; p++) F[(size_t)p * d.cells + id] = ((cmax * Fl[p] + cmin * Fr[p]) - (cmax * cmin) * (Ur[p] - Ul[p])) / inv;
@@ -315,7 +317,8 @@ struct FluxTile {
 };
 
 // The face physics of k_fluxt: B^DIR continuity, limit_gamma, states, fluxes, wave speeds and
-// the HLL flux of one face (flux.c:852, vchar.c:34) into F at `id`; returns cour*dx/ctop.
+// the HLL flux of one face (flux.c:852, vchar.c:34; LAXF where both speeds vanish or where
+// fluxmethod is LAXF, fluxcompute.c:243) into F at `id`; returns cour*dx/ctop.
 template <int DIR, typename T, typename GT>
 __device__ __forceinline__ double face_hll(const Dims& d, const Phys& ph, const GT* __restrict__ geom,
                                            T* __restrict__ F, size_t id, int ii, int jj, T* pl, T* pr) {
@@ -342,7 +345,7 @@ __device__ __forceinline__ double face_hll(const Dims& d, const Phys& ph, const 
   lmin = fabs(fmax(T(0), -lmin));
   lmax = fabs(fmax(T(0), lmax));
   const T cmin = lmin, cmax = lmax, ctop = fmax(lmax, lmin);
-  if (cmax + cmin != T(0)) {
+  if (!ph.laxf && cmax + cmin != T(0)) {
     const T inv = cmax + cmin;
 #pragma unroll
     for (int p = 0; p < NPR; p++) F[(size_t)p * d.cells + id] = ((cmax * Fl[p] + cmin * Fr[p]) - (cmax * cmin) * (Ur[p] - Ul[p])) / inv;

@@ -48,11 +48,13 @@ class Grid:
 
     @classmethod
     def torus(cls, n1: int, n2: int, n3: int, lim: int = N.HARM_LIM_MC, a: float = 0.9375,
-              hslope: float = 0.3, Rout: float = 40.0, cour: float = 0.8) -> "Grid":
+              hslope: float = 0.3, Rout: float = 40.0, cour: float = 0.8,
+              fluxmethod: int = N.HARM_FLUX_HLL) -> "Grid":
         g = N.harm_grid()
         rc = N.host_lib().harm_grid_setup(C.byref(g), n1, n2, n3, lim, a, hslope, Rout, cour)
         if rc:
             raise RuntimeError(f"harm_grid_setup failed ({rc})")
+        g.fluxmethod = fluxmethod
         return cls(g)
 
     @property

@@ -52,6 +52,10 @@ enum { HARM_RHO = 0, HARM_UU = 1, HARM_U1 = 2, HARM_U2 = 3, HARM_U3 = 4,
    shock flattening from the cell's total pressure and sqrt(-g) rho u^dir; it needs ng >= 4. */
 enum { HARM_LIM_MC = 0, HARM_LIM_PARA = 1, HARM_LIM_WENO5 = 2, HARM_LIM_PARALINE = 3 };
 
+/* flux formula at a face (HARM fluxmethod, fluxcompute.c:243): HLL with the LAXF fallback
+   where both wave speeds vanish, or LAXF (Rusanov) everywhere */
+enum { HARM_FLUX_HLL = 0, HARM_FLUX_LAXF = 1 };
+
 /* arithmetic of the flux path: FP64 everywhere, or FP32 reconstruction/HLL/CT with the
    conserved update, inversion and metric kept in FP64 */
 enum { HARM_PREC_FP64 = 0, HARM_PREC_MIXED = 1 };
@@ -102,7 +106,7 @@ typedef struct harm_grid {
   int n1e, n2e, n3e;       /* extended sizes */
   int ng3;                 /* ghost cells in x3: ng if n3>1 else 0 */
   int lim;                 /* HARM_LIM_* */
-  int pad0;
+  int fluxmethod;          /* HARM_FLUX_*; harm_grid_setup sets HARM_FLUX_HLL */
   double startx[4], dx[4]; /* x^mu of the lower corner of active cell (0,0,0), spacings */
   double a;                /* black-hole spin */
   double hslope, R0, Rin, Rout, Rhor;

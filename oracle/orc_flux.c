@@ -6,7 +6,8 @@
  * and limit_gamma on each side (check_plpr flux.c:2041, EVOLVECHECKS=1), fluid state and
  * fluxes of both sides (p2SFUevolve fluxcompute.c:122), vchar wave speeds and
  * cminmax_calc (wavespeeds.c:12, :397, ROEAVERAGEDWAVESPEED=0), the HLL flux with the
- * LAXF fallback (hllflux_compute fluxcompute.c:329), the CFL dt = cour dx/ctop
+ * LAXF fallback (hllflux_compute fluxcompute.c:329) or, for fluxmethod LAXF, the LAXF flux
+ * (fluxcompute.c:243), the CFL dt = cour dx/ctop
  * (flux.c:1106), then Toth's flux-CT (flux_ct fluxct.c:186, CORNGDETVERSION=1).
  *
  * Faces computed per direction d: the faces bounding active cells in d and one layer of
@@ -29,7 +30,8 @@ static void face_loop_bounds(const orc *o, int dir, int lo[3], int hi[3]) {
   }
 }
 
-/* HLL / LAXF flux of one face (flux_compute fluxcompute.c:212 with fluxmethod=HLLFLUX) */
+/* flux of one face (flux_compute fluxcompute.c:212): fluxmethod HLLFLUX (HLLCOMPUTE :179, the
+   LAXF formula where cmax + cmin = 0, hllflux_compute :329) or LAXFFLUX (LAXFCOMPUTE :182) */
 static void face_flux(const orc *o, int dir, const ogeom *g, double *pl, double *pr, double *F, double *ctop) {
   const harm_grid *hg = &o->g;
   /* getplpr: B^dir continuous */
@@ -54,7 +56,7 @@ static void face_flux(const orc *o, int dir, const ogeom *g, double *pl, double 
   lmax = fabs(fmax(0., lmax));
   double cmin = lmin, cmax = lmax;
   *ctop = fmax(lmax, lmin);
-  if (cmax + cmin != 0.0) {
+  if (hg->fluxmethod != HARM_FLUX_LAXF && cmax + cmin != 0.0) {
     for (int p = 0; p < HARM_NPR; p++)
       F[p] = ((cmax * Fl[p] + cmin * Fr[p]) - (cmax * cmin) * (Ur[p] - Ul[p])) / (cmax + cmin);
   } else {

@@ -6,8 +6,8 @@ import numpy as np
 from harm_harm_b200 import Grid
 
 
-def make_torus(n1=64, n2=64, n3=1, lim=0, seed=12345, beta=100.0):
-    g = Grid.torus(n1, n2, n3, lim=lim)
+def make_torus(n1=64, n2=64, n3=1, lim=0, seed=12345, beta=100.0, fluxmethod=0):
+    g = Grid.torus(n1, n2, n3, lim=lim, fluxmethod=fluxmethod)
     geom, conn, aux = g.geometry()
     P = g.torus_init(geom, aux, beta_min=beta, seed=seed)
     return g, geom, conn, aux, P

@@ -13,17 +13,19 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-# (n1, n2, n3, lim, planted converging pressure jump); the PARALINE cases carry the planted
-# jump so that its shock flattener is active along every direction
-CASES = {"2d_mc": (64, 64, 1, 0, False), "3d_mc": (32, 24, 8, 0, False), "3d_ppm": (32, 24, 8, 1, False),
-         "3d_weno5": (32, 24, 8, 2, False), "2d_weno5": (48, 48, 1, 2, False),
-         "3d_paraline": (32, 24, 8, 3, True), "2d_paraline": (48, 48, 1, 3, True)}
+# (n1, n2, n3, lim, planted converging pressure jump, fluxmethod); the PARALINE cases carry
+# the planted jump so that its shock flattener is active along every direction; the last case
+# is the reference's own torus choice of reconstruction and flux (PARALINE, LAXF)
+CASES = {"2d_mc": (64, 64, 1, 0, False, 0), "3d_mc": (32, 24, 8, 0, False, 0), "3d_ppm": (32, 24, 8, 1, False, 0),
+         "3d_weno5": (32, 24, 8, 2, False, 0), "2d_weno5": (48, 48, 1, 2, False, 0),
+         "3d_paraline": (32, 24, 8, 3, True, 0), "2d_paraline": (48, 48, 1, 3, True, 0),
+         "3d_paraline_laxf": (32, 24, 8, 3, True, 1)}
 
 
 @pytest.fixture(scope="module", params=list(CASES))
 def setup(request, cuda):
-    n1, n2, n3, lim, plant = CASES[request.param]
-    g, geom, conn, aux, P = make_torus(n1, n2, n3, lim=lim)
+    n1, n2, n3, lim, plant, flux = CASES[request.param]
+    g, geom, conn, aux, P = make_torus(n1, n2, n3, lim=lim, fluxmethod=flux)
     if plant:
         plant_compression(g, P)
     orc = O.Oracle(g, geom, conn, aux)
