@@ -37,8 +37,9 @@ CONFIGS = {
     "torus3d_192x96x64": (192, 96, 64, 2),
     "torus2d_128x128": (128, 128, 1, 0),
 }
-LIMNAME = {0: "mc", 1: "ppm", 2: "weno5"}
-LIMS = {"mc": 0, "ppm": 1, "weno5": 2}
+LIMNAME = {0: "mc", 1: "ppm", 2: "weno5", 3: "paraline"}
+LIMS = {"mc": 0, "ppm": 1, "weno5": 2, "paraline": 3}
+FLUXES = {"hll": 0, "laxf": 1}
 METRIC = "zone-updates/s on 3D torus: learned+mixed vs plain FP64 GPU at L1 err≤1e-6"
 
 
@@ -165,7 +166,7 @@ def run_reference(args, ws, rank):
     n1, n2, n3, lim = CONFIGS[args.config]
     lim = LIMS.get(args.lim, lim)
     sn3 = min(n3, args.cpu_sample_n3)
-    g = Grid.torus(n1, n2, sn3, lim=lim)
+    g = Grid.torus(n1, n2, sn3, lim=lim, fluxmethod=FLUXES[args.flux])
     geom, conn, aux = g.geometry()
     P = g.torus_init(geom, aux, seed=args.seed)
     cores = os.cpu_count() or 1
@@ -187,7 +188,7 @@ def run_reference(args, ws, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded Fishbone-Moncrief torus, host-built)",
-        "config": {"workload": args.config + f"_{LIMNAME[lim]}_hll_fluxct", "sample_n3": sn3},
+        "config": {"workload": args.config + f"_{LIMNAME[lim]}_{args.flux}_fluxct", "sample_n3": sn3},
         "cpu_baseline": {"value": value, "unit": "zone-updates/s", "cores": cores, "kind": "port",
                          "sample": f"{n1}x{n2}x{sn3} zones of the same torus, full RK2 steps, FP64"},
         "e2e": {"value": value, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -201,7 +202,7 @@ def cpu_baseline_sample(args, lim) -> dict:
     from oracle import oracle as O
     n1, n2, n3, _ = CONFIGS[args.config]
     sn3 = min(n3, args.cpu_sample_n3)
-    g = Grid.torus(n1, n2, sn3, lim=lim)
+    g = Grid.torus(n1, n2, sn3, lim=lim, fluxmethod=FLUXES[args.flux])
     geom, conn, aux = g.geometry()
     P = g.torus_init(geom, aux, seed=args.seed)
     cores = os.cpu_count() or 1
@@ -261,7 +262,7 @@ def run_ours(args, ws, rank, local):
     torch.cuda.set_device(local)
     n1, n2, n3, lim = CONFIGS[args.config]
     lim = LIMS.get(args.lim, lim)
-    g = Grid.torus(n1, n2, n3, lim=lim)
+    g = Grid.torus(n1, n2, n3, lim=lim, fluxmethod=FLUXES[args.flux])
     geom, conn, aux = g.geometry()
     P0 = g.torus_init(geom, aux, seed=args.seed + rank)
     dev = Harm(g, geom, conn, aux, device=local)
@@ -365,8 +366,8 @@ def run_ours(args, ws, rank, local):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 flux / f64 update+inversion" if prec == HARM_PREC_MIXED else "f64",
             "data": "synthetic (seeded Fishbone-Moncrief torus, host-built)",
-            "config": {"workload": f"{args.config}_{LIMNAME[lim]}_hll_fluxct_{args.precision}_{args.guess}",
-                       "grid": [n1, n2, n3], "reconstruction": LIMNAME[lim], "riemann": "hll", "ct": "toth",
+            "config": {"workload": f"{args.config}_{LIMNAME[lim]}_{args.flux}_fluxct_{args.precision}_{args.guess}",
+                       "grid": [n1, n2, n3], "reconstruction": LIMNAME[lim], "riemann": args.flux, "ct": "toth",
                        "precision": args.precision, "guess": args.guess,
                        "l2": "inputs larger than L2 (P is %.0f MB)" % (pbytes / 1e6),
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
@@ -417,7 +418,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="torus3d_384x192x128", choices=list(CONFIGS))
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
-    ap.add_argument("--lim", default="config", choices=["config", "mc", "ppm", "weno5"])
+    ap.add_argument("--lim", default="config", choices=["config", "mc", "ppm", "weno5", "paraline"])
+    ap.add_argument("--flux", default="hll", choices=list(FLUXES), help="face flux formula (fluxmethod)")
     ap.add_argument("--guess", default="mlp", choices=["prev", "mlp"])
     ap.add_argument("--train-steps", type=int, default=4, help="plain steps whose (U,P) pairs train the guess")
     ap.add_argument("--train-pairs", type=int, default=2000000, help="pairs dumped over those steps")
