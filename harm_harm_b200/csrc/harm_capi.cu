@@ -139,6 +139,12 @@ extern "C" int harm_b200_destroy(harm_ctx* c) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->h_scal) cudaFreeHost(c->h_scal);
+  if (c->copy_stream) {
+    cudaStreamSynchronize(c->copy_stream);
+    cudaStreamDestroy(c->copy_stream);
+    cudaEventDestroy(c->entry_ev);
+    for (int s = 0; s < HARM_H2D_SLABS; s++) cudaEventDestroy(c->slab_ev[s]);
+  }
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return 0;
@@ -180,7 +186,7 @@ static int check_guess(harm_ctx* c, int guess) {
 // one substep on the device; dt from d_dt, dt minima of this substep into slots
 static int substep(harm_ctx* c, int precision, int guess, int timeorder, int numtimeorders, const double* d_pi,
                    const double* d_pb, double* d_pf, int8_t* d_pflag, const double* CUf, const double* Cunew,
-                   unsigned long long* slots, bool with_stats) {
+                   unsigned long long* slots, bool with_stats, const SlabWait* sw = nullptr) {
   if (int rc = check_guess(c, guess)) return rc;
   StepCoef sc;
   sc.CUf0 = CUf[0]; sc.CUf2 = CUf[2];
@@ -189,10 +195,10 @@ static int substep(harm_ctx* c, int precision, int guess, int timeorder, int num
   sc.guess = guess;
   double* st = with_stats ? c->d_stats : nullptr;
   if (precision == HARM_PREC_FP64) {
-    if (hp_fluxes_fp64(c, d_pb, c->d_F[0], c->d_F[1], c->d_F[2], c->d_emf, slots)) return 1;
+    if (hp_fluxes_fp64(c, d_pb, c->d_F[0], c->d_F[1], c->d_F[2], c->d_emf, slots, sw)) return 1;
     return hp_update_fp64(c, sc, d_pi, d_pb, d_pf, d_pflag, st);
   }
-  if (hp_fluxes_mixed(c, d_pb, c->d_Ff[0], c->d_Ff[1], c->d_Ff[2], c->d_emff, slots)) return 1;
+  if (hp_fluxes_mixed(c, d_pb, c->d_Ff[0], c->d_Ff[1], c->d_Ff[2], c->d_emff, slots, sw)) return 1;
   return hp_update_mixed(c, sc, d_pi, d_pb, d_pf, d_pflag, st);
 }
 
@@ -240,10 +246,13 @@ extern "C" int harm_b200_advance(harm_ctx* c, int precision, int guess, int time
 extern "C" int harm_b200_post_fixup(harm_ctx* c, double* d_pf, int8_t* d_pflag) { return hp_fixup(c, d_pf, d_pflag); }
 
 // enqueue one full RK2 step with dt in d_dt (no host synchronisation)
-static int enqueue_step(harm_ctx* c, int precision, int guess, double* d_P, bool with_stats) {
+// sw: d_P is still arriving in k-slabs (the first substep's flux launches wait for them)
+static int enqueue_step(harm_ctx* c, int precision, int guess, double* d_P, bool with_stats,
+                        const SlabWait* sw = nullptr) {
   static const double CUf[2][4] = {{1.0, 0.0, 0.5, 0.0}, {1.0, 0.0, 1.0, 0.0}};
   static const double Cun[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 1.0, 0.5}};
-  if (substep(c, precision, guess, 0, 2, d_P, d_P, c->d_pk, c->d_pflag, CUf[0], Cun[0], c->d_dtslots, with_stats)) return 1;
+  if (substep(c, precision, guess, 0, 2, d_P, d_P, c->d_pk, c->d_pflag, CUf[0], Cun[0], c->d_dtslots, with_stats, sw))
+    return 1;
   // bound_prim of p_f and of the flags in one pass (neither depends on the other), post_fixup,
   // bound_prim (post_advance step_ch.c:288-330)
   if (hp_bound(c, c->d_pk, c->d_pflag)) return 1;
@@ -278,13 +287,55 @@ extern "C" int harm_b200_step(harm_ctx* c, int precision, int guess, double* d_P
   return harm_b200_step_n(c, precision, guess, d_P, 1, dt, stats);
 }
 
+// H2D of the state in at most HARM_H2D_SLABS slabs of k-planes (one cudaMemcpyAsync per
+// primitive and slab, each slab followed by an event) on the copy stream, after the context
+// stream's earlier work
+static int h2d_slabs(harm_ctx* c, const double* h_P, SlabWait* sw) {
+  if (!c->copy_stream) {
+    CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->entry_ev, cudaEventDisableTiming));
+    for (int s = 0; s < HARM_H2D_SLABS; s++) CK(cudaEventCreateWithFlags(&c->slab_ev[s], cudaEventDisableTiming));
+  }
+  const int n3e = c->g.n3e;
+  const int planes = (n3e + HARM_H2D_SLABS - 1) / HARM_H2D_SLABS;
+  const int nslab = (n3e + planes - 1) / planes;
+  CK(cudaEventRecord(c->entry_ev, c->stream));
+  CK(cudaStreamWaitEvent(c->copy_stream, c->entry_ev, 0));
+  for (int s = 0; s < nslab; s++) {
+    const int z0 = s * planes, z1 = (z0 + planes < n3e) ? z0 + planes : n3e;
+    const size_t off = (size_t)z0 * c->plane, bytes = (size_t)(z1 - z0) * c->plane * sizeof(double);
+    for (int p = 0; p < NPR; p++)
+      CK(cudaMemcpyAsync(c->d_Pdev + (size_t)p * c->cells + off, h_P + (size_t)p * c->cells + off, bytes,
+                         cudaMemcpyHostToDevice, c->copy_stream));
+    CK(cudaEventRecord(c->slab_ev[s], c->copy_stream));
+  }
+  sw->ev = c->slab_ev;
+  sw->nslab = nslab;
+  sw->planes = planes;
+  return 0;
+}
+
+// One full step over a host array: the state goes to the device in k-slabs while the first
+// substep's flux tiles of the slabs already resident run, then the rest of the step, then the
+// state comes back.  Results are those of harm_b200_step on the same state.
 extern "C" int harm_b200_step_host(harm_ctx* c, int precision, int guess, double* h_P, double* dt, harm_stats* stats) {
-  size_t bytes = NPR * c->cells * sizeof(double);
+  if (int rc = check_guess(c, guess)) return rc;
+  Dims d = dims_of(c->g);
+  const size_t bytes = NPR * c->cells * sizeof(double);
   if (!c->d_Pdev) CK(cudaMalloc(&c->d_Pdev, bytes));
-  CK(cudaMemcpyAsync(c->d_Pdev, h_P, bytes, cudaMemcpyHostToDevice, c->stream));
-  if (harm_b200_step_n(c, precision, guess, c->d_Pdev, 1, dt, stats)) return 1;
+  c->h_scal[0] = *dt;
+  CK(cudaMemcpyAsync(c->d_dt, c->h_scal, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (stats) CK(cudaMemsetAsync(c->d_stats, 0, 5 * sizeof(double), c->stream));
+  SlabWait sw;
+  if (int rc = h2d_slabs(c, h_P, &sw)) return rc;
+  if (enqueue_step(c, precision, guess, c->d_Pdev, stats != nullptr, &sw)) return 1;
   CK(cudaMemcpyAsync(h_P, c->d_Pdev, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(c->h_scal, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (stats) CK(cudaMemcpyAsync(c->h_scal + 8, c->d_stats, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  if (int rc = check_status(c)) return rc;
+  *dt = c->h_scal[0];
+  add_stats(c, stats, 2.0 * (double)d.n1 * d.n2 * d.n3);
   return 0;
 }
 

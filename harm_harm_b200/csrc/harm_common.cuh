@@ -642,6 +642,20 @@ static inline dim3 fluxt_grid(const FaceBox& fb) {
   return dim3((fb.cnt[0] + NT - 1) / NT, (fb.cnt[2] + A - 1) / A, fb.cnt[1]);
 }
 
+// the face box restricted to active-relative k indices [klo, khi] (index 2: k for every
+// direction, the face index along k for DIR 3); false when nothing is left
+static inline bool face_box_k(FaceBox b, int klo, int khi, FaceBox* out) {
+  klo = (klo > b.lo[2]) ? klo : b.lo[2];
+  khi = (khi < b.hi[2]) ? khi : b.hi[2];
+  if (klo > khi) return false;
+  b.lo[2] = klo;
+  b.hi[2] = khi;
+  b.cnt[2] = khi - klo + 1;
+  b.n = (long long)b.cnt[0] * b.cnt[1] * b.cnt[2];
+  *out = b;
+  return true;
+}
+
 // launch k_fluxt<DIR, LIM, T, GT>; the first launch of an instantiation on a device raises
 // its dynamic shared-memory limit where the tile needs more than 48 KB (FP32 WENO5: 63 KB)
 template <int DIR, int LIM, typename T, typename GT>
@@ -662,6 +676,46 @@ static inline cudaError_t launch_fluxt(const Dims& d, const Phys& ph, const Face
   }
   k_fluxt<DIR, LIM, T, GT><<<fluxt_grid<DIR, LIM>(fb), 256, smem, st>>>(d, ph, fb, P, geom, F, dtslot);
   return cudaGetLastError();
+}
+
+// The three flux directions of one substep while the state is still arriving in k-slabs
+// (SlabWait): after each slab's copy, the x1 and x2 faces of its planes (their stencils stay in
+// the plane) and every row of x3 tiles (A faces along k) whose staged planes have all arrived.
+// Same kernels and results as the whole-grid launches.
+template <int LIM, typename T, typename GT>
+static inline cudaError_t launch_flux_slabs(const Dims& d, const Phys& ph, const double* pb, const GT* geom, T* F1,
+                                            T* F2, T* F3, unsigned long long* slots, cudaStream_t st,
+                                            const SlabWait& sw, unsigned long long& launches) {
+  constexpr int A = FluxTile<LIM, T>::A, X = ReconGeom<LIM>::X;
+  const FaceBox b1 = face_box(d, 1), b2 = face_box(d, 2), b3 = face_box(d, 3);
+  int f3 = b3.lo[2];  // first x3 face not launched yet
+  cudaError_t e;
+  for (int s = 0; s < sw.nslab; s++) {
+    if ((e = cudaStreamWaitEvent(st, sw.ev[s], 0)) != cudaSuccess) return e;
+    const int resident = (s + 1) * sw.planes;  // planes [0, resident) are on the device
+    const int klo = s * sw.planes - d.ng3, khi = resident - 1 - d.ng3;
+    FaceBox sb;
+    if (face_box_k(b1, klo, khi, &sb)) {
+      if ((e = launch_fluxt<1, LIM, T, GT>(d, ph, sb, pb, geom, F1, slots + 0, st)) != cudaSuccess) return e;
+      launches++;
+    }
+    if (face_box_k(b2, klo, khi, &sb)) {
+      if ((e = launch_fluxt<2, LIM, T, GT>(d, ph, sb, pb, geom, F2, slots + 1, st)) != cudaSuccess) return e;
+      launches++;
+    }
+    // x3 tile rows: a row from face f0 stages planes up to f0 + ng3 + A + X - 1 (clamped)
+    while (d.n3 > 1 && f3 <= b3.hi[2]) {
+      int top = f3 + d.ng3 + A + X - 1;
+      if (top > d.n3e - 1) top = d.n3e - 1;
+      if (top >= resident && s + 1 < sw.nslab) break;
+      if (face_box_k(b3, f3, f3 + A - 1, &sb)) {
+        if ((e = launch_fluxt<3, LIM, T, GT>(d, ph, sb, pb, geom, F3, slots + 2, st)) != cudaSuccess) return e;
+        launches++;
+      }
+      f3 += A;
+    }
+  }
+  return cudaSuccess;
 }
 
 // ------------------------------------------------------------------ EMF kernel

@@ -4,10 +4,24 @@
 #include <stdint.h>
 #include "harm_b200.h"
 
+// the host-buffer entry point copies the state in k-slabs: at most this many, each followed by
+// an event the first substep's flux launches of that slab wait for
+#define HARM_H2D_SLABS 8
+
+// which copy event each k-plane's flux launches wait for (planes [s*planes, (s+1)*planes) of
+// the extended grid arrive with ev[s])
+struct SlabWait {
+  const cudaEvent_t* ev;
+  int nslab, planes;
+};
+
 struct harm_ctx {
   harm_grid g;
   int device;
   cudaStream_t stream;
+  cudaStream_t copy_stream;             // host-buffer entry point: H2D of the state
+  cudaEvent_t slab_ev[HARM_H2D_SLABS];  // recorded on copy_stream after each slab
+  cudaEvent_t entry_ev;                 // recorded on stream before the copies start
   size_t plane, cells;
   // metric tables (FP64, plus an FP32 copy for the mixed-precision flux path)
   double* d_geom;

@@ -275,7 +275,11 @@ __global__ void __launch_bounds__(256, 2) k_utoprim_points_mlp(size_t n, Phys ph
 
 template <int LIM>
 static int flux_dirs_double(harm_ctx* c, const Dims& d, const Phys& ph, const double* pb, double* F1, double* F2, double* F3,
-                         unsigned long long* slots) {
+                         unsigned long long* slots, const SlabWait* sw) {
+  if (sw) {
+    CK((launch_flux_slabs<LIM, double, double>(d, ph, pb, c->d_geom, F1, F2, F3, slots, c->stream, *sw, c->launches)));
+    return 0;
+  }
   FaceBox b1 = face_box(d, 1), b2 = face_box(d, 2), b3 = face_box(d, 3);
   CK((launch_fluxt<1, LIM, double, double>(d, ph, b1, pb, c->d_geom, F1, slots + 0, c->stream)));
   CK((launch_fluxt<2, LIM, double, double>(d, ph, b2, pb, c->d_geom, F2, slots + 1, c->stream)));
@@ -288,13 +292,13 @@ static int flux_dirs_double(harm_ctx* c, const Dims& d, const Phys& ph, const do
 }
 
 int hp_fluxes_fp64(harm_ctx* c, const double* pb, double* F1, double* F2, double* F3, double* emf,
-                   unsigned long long* slots) {
+                   unsigned long long* slots, const SlabWait* sw) {
   Dims d = dims_of(c->g);
   Phys ph = phys_of(c->g);
-  if (c->g.lim == HARM_LIM_WENO5) { int rc = flux_dirs_double<HARM_LIM_WENO5>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
-  else if (c->g.lim == HARM_LIM_PARA) { int rc = flux_dirs_double<HARM_LIM_PARA>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
-  else if (c->g.lim == HARM_LIM_PARALINE) { int rc = flux_dirs_double<HARM_LIM_PARALINE>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
-  else { int rc = flux_dirs_double<HARM_LIM_MC>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
+  if (c->g.lim == HARM_LIM_WENO5) { int rc = flux_dirs_double<HARM_LIM_WENO5>(c, d, ph, pb, F1, F2, F3, slots, sw); if (rc) return rc; }
+  else if (c->g.lim == HARM_LIM_PARA) { int rc = flux_dirs_double<HARM_LIM_PARA>(c, d, ph, pb, F1, F2, F3, slots, sw); if (rc) return rc; }
+  else if (c->g.lim == HARM_LIM_PARALINE) { int rc = flux_dirs_double<HARM_LIM_PARALINE>(c, d, ph, pb, F1, F2, F3, slots, sw); if (rc) return rc; }
+  else { int rc = flux_dirs_double<HARM_LIM_MC>(c, d, ph, pb, F1, F2, F3, slots, sw); if (rc) return rc; }
   long long nc = (long long)(d.n1 + 1) * (d.n2 + 1) * (d.n3 > 1 ? d.n3 + 1 : 1);
   k_emf<double, double><<<nblk(nc), 256, 0, c->stream>>>(d, F1, F2, F3, c->d_geom, emf);
   c->launches++;

@@ -70,7 +70,11 @@ static int launch_fluxt_tma(harm_ctx* c, const Dims& d, const Phys& ph, const Fa
 
 template <int LIM>
 static int flux_dirs_float(harm_ctx* c, const Dims& d, const Phys& ph, const double* pb, float* F1, float* F2, float* F3,
-                         unsigned long long* slots) {
+                         unsigned long long* slots, const SlabWait* sw) {
+  if (sw) {  // state arriving in slabs: plain-load tiles, launched slab by slab
+    CK((launch_flux_slabs<LIM, float, float>(d, ph, pb, c->d_geomf, F1, F2, F3, slots, c->stream, *sw, c->launches)));
+    return 0;
+  }
   FaceBox b1 = face_box(d, 1), b2 = face_box(d, 2), b3 = face_box(d, 3);
   // the TMA-staged variant covers MC, PARA and WENO5; PARALINE always takes k_fluxt
   if constexpr (LIM != HARM_LIM_PARALINE) {
@@ -96,13 +100,13 @@ static int flux_dirs_float(harm_ctx* c, const Dims& d, const Phys& ph, const dou
 }
 
 int hp_fluxes_mixed(harm_ctx* c, const double* pb, float* F1, float* F2, float* F3, float* emf,
-                   unsigned long long* slots) {
+                   unsigned long long* slots, const SlabWait* sw) {
   Dims d = dims_of(c->g);
   Phys ph = phys_of(c->g);
-  if (c->g.lim == HARM_LIM_WENO5) { int rc = flux_dirs_float<HARM_LIM_WENO5>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
-  else if (c->g.lim == HARM_LIM_PARA) { int rc = flux_dirs_float<HARM_LIM_PARA>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
-  else if (c->g.lim == HARM_LIM_PARALINE) { int rc = flux_dirs_float<HARM_LIM_PARALINE>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
-  else { int rc = flux_dirs_float<HARM_LIM_MC>(c, d, ph, pb, F1, F2, F3, slots); if (rc) return rc; }
+  if (c->g.lim == HARM_LIM_WENO5) { int rc = flux_dirs_float<HARM_LIM_WENO5>(c, d, ph, pb, F1, F2, F3, slots, sw); if (rc) return rc; }
+  else if (c->g.lim == HARM_LIM_PARA) { int rc = flux_dirs_float<HARM_LIM_PARA>(c, d, ph, pb, F1, F2, F3, slots, sw); if (rc) return rc; }
+  else if (c->g.lim == HARM_LIM_PARALINE) { int rc = flux_dirs_float<HARM_LIM_PARALINE>(c, d, ph, pb, F1, F2, F3, slots, sw); if (rc) return rc; }
+  else { int rc = flux_dirs_float<HARM_LIM_MC>(c, d, ph, pb, F1, F2, F3, slots, sw); if (rc) return rc; }
   long long nc = (long long)(d.n1 + 1) * (d.n2 + 1) * (d.n3 > 1 ? d.n3 + 1 : 1);
   k_emf<float, float><<<nblk(nc), 256, 0, c->stream>>>(d, F1, F2, F3, c->d_geomf, emf);
   c->launches++;

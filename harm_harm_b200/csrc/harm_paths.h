@@ -5,10 +5,12 @@
 
 struct StepCoef;
 
+// fluxes and EMFs of one substep; sw: the state is still arriving in k-slabs (launches wait
+// for each slab's copy event)
 int hp_fluxes_fp64(harm_ctx* c, const double* pb, double* F1, double* F2, double* F3, double* emf,
-                   unsigned long long* slots);
+                   unsigned long long* slots, const SlabWait* sw = nullptr);
 int hp_fluxes_mixed(harm_ctx* c, const double* pb, float* F1, float* F2, float* F3, float* emf,
-                    unsigned long long* slots);
+                    unsigned long long* slots, const SlabWait* sw = nullptr);
 int hp_update_fp64(harm_ctx* c, const StepCoef& sc, const double* pi, const double* pb, double* pf, int8_t* pflag,
                    double* stats);
 int hp_update_mixed(harm_ctx* c, const StepCoef& sc, const double* pi, const double* pb, double* pf, int8_t* pflag,

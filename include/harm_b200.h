@@ -222,7 +222,9 @@ int harm_b200_step(harm_ctx *ctx, int precision, int guess, double *d_P, double 
 int harm_b200_step_n(harm_ctx *ctx, int precision, int guess, double *d_P, int nsteps,
                      double *dt, harm_stats *stats);
 
-/* Same step over a HOST primitive array: copies h_P in, steps, copies it back. */
+/* Same step over a HOST primitive array: copies h_P in (in slabs of k-planes, the first
+   substep's flux kernels of each slab starting as soon as it is resident), steps, copies it
+   back.  Results are those of harm_b200_step. */
 int harm_b200_step_host(harm_ctx *ctx, int precision, int guess, double *h_P, double *dt,
                         harm_stats *stats);
 
