@@ -163,114 +163,6 @@ static inline FaceBox face_box(const Dims& d, int dir) {
   return b;
 }
 
-template <typename T>
-__device__ __forceinline__ void recon_face_mc(const double* __restrict__ P, size_t cells, size_t c0, long long stride,
-                                              T* pl, T* pr) {
-#pragma unroll
-  for (int p = 0; p < NPR; p++) {
-    const double* base = P + (size_t)p * cells + c0;
-    T ym2 = (T)__ldg(base - 2 * stride), ym1 = (T)__ldg(base - stride), y0 = (T)__ldg(base), yp1 = (T)__ldg(base + stride);
-    T dqm = mc_slope(ym2, ym1, y0), dq0 = mc_slope(ym1, y0, yp1);
-    pl[p] = ym1 + T(0.5) * dqm;
-    pr[p] = y0 - T(0.5) * dq0;
-  }
-}
-
-// PPM: cells i-3..i+2 around the face below cell i (para4 of cells i-1 and i)
-template <typename T>
-__device__ __forceinline__ void recon_face_para(const double* __restrict__ P, size_t cells, size_t c0, long long stride,
-                                                T* pl, T* pr) {
-#pragma unroll 1
-  for (int p = 0; p < NPR; p++) {
-    const double* base = P + (size_t)p * cells + c0;
-    T y[6];
-#pragma unroll
-    for (int q = 0; q < 6; q++) y[q] = (T)__ldg(base + (long long)(q - 3) * stride);
-    T la, ra, lb, rb;
-    para4_cell<T>(y + 2, la, ra);
-    para4_cell<T>(y + 3, lb, rb);
-    pl[p] = ra;
-    pr[p] = lb;
-  }
-}
-
-// WENO5: cells i-5..i+4; unoptimised weights of cells i-3..i+2, edges of cells i-1 and i
-template <typename T>
-__device__ __forceinline__ void recon_face_weno5(const double* __restrict__ P, size_t cells, size_t c0,
-                                                 long long stride, T* pl, T* pr) {
-#pragma unroll 1
-  for (int p = 0; p < NPR; p++) {
-    const double* base = P + (size_t)p * cells + c0;
-    T y[10];
-#pragma unroll
-    for (int q = 0; q < 10; q++) y[q] = (T)__ldg(base + (long long)(q - 5) * stride);
-    T w[6][3];
-#pragma unroll
-    for (int q = 0; q < 6; q++) weno5_unopt<T>(y + 2 + q, w[q]);
-    T la, ra, lb, rb;
-    weno5_edges<T>(y + 4, w[2], w[0], w[4], la, ra);
-    weno5_edges<T>(y + 5, w[3], w[1], w[5], lb, rb);
-    pl[p] = ra;
-    pr[p] = lb;
-  }
-}
-
-template <int DIR, typename T, typename GT, int LIM = HARM_LIM_MC>
-__global__ void __launch_bounds__(256) k_flux(Dims d, Phys ph, FaceBox fb, const double* __restrict__ P,
-                                              const GT* __restrict__ geom, T* __restrict__ F,
-                                              unsigned long long* __restrict__ dtslot) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  double dtij = 1.e300;
-  if (t < fb.n) {
-    int a = (int)(t % fb.cnt[0]);
-    long long r = t / fb.cnt[0];
-    int b = (int)(r % fb.cnt[1]);
-    int c = (int)(r / fb.cnt[1]);
-    int ii = a + fb.lo[0] + d.ng, jj = b + fb.lo[1] + d.ng, kk = c + fb.lo[2] + d.ng3;
-    size_t id = cidx(d, ii, jj, kk);
-    long long stride = (DIR == 1) ? 1 : (DIR == 2) ? (long long)d.n1e : (long long)d.plane;
-    T pl[NPR], pr[NPR];
-    if (LIM == HARM_LIM_WENO5) recon_face_weno5<T>(P, d.cells, id, stride, pl, pr);
-    else if (LIM == HARM_LIM_PARA) recon_face_para<T>(P, d.cells, id, stride, pl, pr);
-    else recon_face_mc<T>(P, d.cells, id, stride, pl, pr);
-    constexpr int loc = (DIR == 1) ? HARM_LOC_FACE1 : (DIR == 2) ? HARM_LOC_FACE2 : HARM_LOC_CENT;
-    Geo<T> g;
-    load_geo<T, GT>(geom + (size_t)loc * HARM_NGF * d.plane, d.plane, (size_t)jj * d.n1e + ii, g);
-    const int bp = HARM_B1 + DIR - 1;
-    pl[bp] = pr[bp] = T(0.5) * (pl[bp] + pr[bp]);
-    const T gam = (T)ph.gam, gmax = (T)ph.gammamax;
-    limit_gamma<T>(gmax, pl, g);
-    limit_gamma<T>(gmax, pr, g);
-    State<T> ql, qr;
-    get_state<T>(pl, g, gam, ql);
-    get_state<T>(pr, g, gam, qr);
-    T Fl[NPR], Fr[NPR], Ul[NPR], Ur[NPR];
-    primtoflux<T>(pl, ql, DIR, g, g.gdet, Fl);
-    primtoflux<T>(pl, ql, 0, g, g.gdet, Ul);
-    primtoflux<T>(pr, qr, DIR, g, g.gdet, Fr);
-    primtoflux<T>(pr, qr, 0, g, g.gdet, Ur);
-    T cmaxl, cminl, cmaxr, cminr;
-    vchar<T>(pl, ql, DIR, g, gam, cmaxl, cminl);
-    vchar<T>(pr, qr, DIR, g, gam, cmaxr, cminr);
-    T lmin = fmin(cminl, cminr), lmax = fmax(cmaxl, cmaxr);
-    lmin = fabs(fmax(T(0), -lmin));
-    lmax = fabs(fmax(T(0), lmax));
-    const T cmin = lmin, cmax = lmax, ctop = fmax(lmax, lmin);
-    if (!ph.laxf && cmax + cmin != T(0)) {
-      const T inv = cmax + cmin;
-#pragma unroll
-      for (int p = 0; p < NPR; p++) F[(size_t)p * d.cells + id] = ((cmax * Fl[p] + cmin * Fr[p]) - (cmax * cmin) * (Ur[p] - Ul[p])) / inv;
-    } else {
-#pragma unroll
-      for (int p = 0; p < NPR; p++) F[(size_t)p * d.cells + id] = T(0.5) * ((Fl[p] + Fr[p]) - ctop * (Ur[p] - Ul[p]));
-    }
-    const double dxd = (DIR == 1) ? ph.dx1 : (DIR == 2) ? ph.dx2 : ph.dx3;
-    dtij = ph.cour * dxd / (double)ctop;
-    if (!(dtij > 0.0)) dtij = 1.e300;
-  }
-  block_min_atomic(dtij, dtslot);
-}
-
 // ------------------------------------------------------------------ tiled flux kernel
 //
 // One block of 256 threads = a tile of A = 32 faces of direction DIR times NT = 8 transverse

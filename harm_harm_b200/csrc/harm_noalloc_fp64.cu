@@ -62,10 +62,23 @@ static int noalloc_scratch(double** emf, unsigned long long** dtmin) {
   return 0;
 }
 
+// the three directions with the FP64 path's tile kernel (the first launch of an instantiation
+// on a device raises its shared-memory limit where the tile needs more than 48 KB)
+template <int LIM>
+static cudaError_t noalloc_dirs(const Dims& d, const Phys& ph, const double* geom, const double* pb, double* F1,
+                                double* F2, double* F3, unsigned long long* dtmin, cudaStream_t st) {
+  cudaError_t e = launch_fluxt<1, LIM, double, double>(d, ph, face_box(d, 1), pb, geom, F1, dtmin + 0, st);
+  if (e == cudaSuccess) e = launch_fluxt<2, LIM, double, double>(d, ph, face_box(d, 2), pb, geom, F2, dtmin + 1, st);
+  if (e == cudaSuccess && d.n3 > 1) e = launch_fluxt<3, LIM, double, double>(d, ph, face_box(d, 3), pb, geom, F3, dtmin + 2, st);
+  return e;
+}
+
 extern "C" int harm_b200_fluxcalc_noalloc(const harm_grid* g, const double* d_geom, const double* d_pb, double* d_F1,
                                           double* d_F2, double* d_F3, double ndt[3], void* stream) {
   if (!g || !d_geom || !d_pb || !d_F1 || !d_F2 || !d_F3 || !ndt) return noalloc_fail("null argument");
-  if (g->lim != HARM_LIM_MC) return noalloc_fail("reconstruction not available on this entry point");
+  if (g->lim != HARM_LIM_MC && g->lim != HARM_LIM_PARA && g->lim != HARM_LIM_WENO5 && g->lim != HARM_LIM_PARALINE)
+    return noalloc_fail("unknown reconstruction");
+  if ((g->lim == HARM_LIM_WENO5 && g->ng < 6) || g->ng < 4) return noalloc_fail("too few ghost zones for the reconstruction");
   const size_t cells = (size_t)g->n1e * g->n2e * g->n3e;
   if (cells > (size_t)HARM_NOALLOC_MAX_CELLS) {
     char buf[256];
@@ -82,14 +95,16 @@ extern "C" int harm_b200_fluxcalc_noalloc(const harm_grid* g, const double* d_ge
   // the CFL minima start from the identity of the min reduction
   if (cudaMemsetAsync(dtmin, 0xFF, 3 * sizeof(unsigned long long), st) != cudaSuccess)
     return noalloc_fail("cudaMemsetAsync failed");
-  FaceBox b1 = face_box(d, 1), b2 = face_box(d, 2), b3 = face_box(d, 3);
-  k_flux<1, double, double><<<nblk(b1.n), 256, 0, st>>>(d, ph, b1, d_pb, d_geom, d_F1, dtmin + 0);
-  k_flux<2, double, double><<<nblk(b2.n), 256, 0, st>>>(d, ph, b2, d_pb, d_geom, d_F2, dtmin + 1);
-  if (d.n3 > 1) k_flux<3, double, double><<<nblk(b3.n), 256, 0, st>>>(d, ph, b3, d_pb, d_geom, d_F3, dtmin + 2);
+  cudaError_t e;
+  if (g->lim == HARM_LIM_WENO5) e = noalloc_dirs<HARM_LIM_WENO5>(d, ph, d_geom, d_pb, d_F1, d_F2, d_F3, dtmin, st);
+  else if (g->lim == HARM_LIM_PARA) e = noalloc_dirs<HARM_LIM_PARA>(d, ph, d_geom, d_pb, d_F1, d_F2, d_F3, dtmin, st);
+  else if (g->lim == HARM_LIM_PARALINE) e = noalloc_dirs<HARM_LIM_PARALINE>(d, ph, d_geom, d_pb, d_F1, d_F2, d_F3, dtmin, st);
+  else e = noalloc_dirs<HARM_LIM_MC>(d, ph, d_geom, d_pb, d_F1, d_F2, d_F3, dtmin, st);
+  if (e != cudaSuccess) return noalloc_fail(cudaGetErrorString(e));
   long long nc = (long long)(d.n1 + 1) * (d.n2 + 1) * (d.n3 > 1 ? d.n3 + 1 : 1);
   k_emf<double, double><<<nblk(nc), 256, 0, st>>>(d, d_F1, d_F2, d_F3, d_geom, emf);
   k_emf_to_flux<double><<<nblk(nc), 256, 0, st>>>(d, emf, d_F1, d_F2, d_F3);
-  cudaError_t e = cudaGetLastError();
+  e = cudaGetLastError();
   if (e != cudaSuccess) return noalloc_fail(cudaGetErrorString(e));
   unsigned long long hb[3];
   if (cudaMemcpyAsync(hb, dtmin, sizeof(hb), cudaMemcpyDeviceToHost, st) != cudaSuccess)

@@ -338,8 +338,8 @@ int harm_b200_dump(harm_ctx *ctx, const double *d_P, const double *d_U, double t
 
 /* No counterpart in the reference.  fluxcalc for callers that cannot allocate device
    memory (a caller working inside a memory pool it does not own, or a host that forbids
-   allocation once its time loop runs): same FP64 fluxes and ndt[3] as harm_b200_fluxcalc,
-   from caller-provided d_geom (the device copy of the geom table), d_pb and d_F1..d_F3, on
+   allocation once its time loop runs): same FP64 fluxes and ndt[3] as harm_b200_fluxcalc
+   (every reconstruction and flux method of harm_grid), from caller-provided d_geom (the device copy of the geom table), d_pb and d_F1..d_F3, on
    `stream` (cudaStream_t, NULL for the default stream).  It allocates nothing: the EMF and
    CFL scratch is a file-scope device array that every GPU loading the library holds until
    exit.  Grids above HARM_NOALLOC_MAX_CELLS are rejected (return 2).  All calls share the

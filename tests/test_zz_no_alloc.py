@@ -28,9 +28,10 @@ def _faces(g, d):
     return (slice(None), k, j, i)
 
 
-def test_noalloc_fluxes_equal_fluxcalc_on_two_calls(cuda):
+@pytest.mark.parametrize("lim,flux", [(0, 0), (1, 0), (2, 0), (3, 1)])
+def test_noalloc_fluxes_equal_fluxcalc_on_two_calls(cuda, lim, flux):
     torch = cuda
-    g, geom, conn, aux, P = make_torus(40, 32, 16)
+    g, geom, conn, aux, P = make_torus(40, 32, 16, lim=lim, fluxmethod=flux)
     assert g.cells <= N.HARM_NOALLOC_MAX_CELLS
     dev = Harm(g, geom, conn, aux)
     lib = N.device_lib()
