@@ -256,6 +256,37 @@ def train_guess(dev, Pd, dt0, prec, args):
             "loss_first": float(hist[0]), "loss_last100": float(hist[-100:].mean()), "start_bias": args.start_bias}
 
 
+def divb_max(g, geom_cent_gdet, P):
+    """max over active corners of Toth's corner divergence of sqrt(-g) B (the quantity flux-CT
+    keeps at round-off), absolute and relative to max |sqrt(-g) B| / min(dx); P on the device"""
+    import torch
+    gg = g.g
+    U = P[5:8] * geom_cent_gdet[None, None]
+    ng, ng3, n1, n2, n3 = gg.ng, gg.ng3, gg.n1, gg.n2, gg.n3
+    dx = gg.dx
+
+    def sl(a, dk, dj, di):
+        return a[ng3 + dk:ng3 + dk + n3 + 1, ng + dj:ng + dj + n2 + 1, ng + di:ng + di + n1 + 1]
+
+    if n3 == 1:
+        u1, u2 = U[0, 0], U[1, 0]
+        s2 = (lambda a, dj, di: a[ng + dj:ng + dj + n2 + 1, ng + di:ng + di + n1 + 1])
+        div = (0.5 * (s2(u1, 0, 0) + s2(u1, -1, 0) - s2(u1, 0, -1) - s2(u1, -1, -1)) / dx[1]
+               + 0.5 * (s2(u2, 0, 0) + s2(u2, 0, -1) - s2(u2, -1, 0) - s2(u2, -1, -1)) / dx[2])
+        scale = float(U[:2].abs().max()) / min(dx[1], dx[2])
+    else:
+        u1, u2, u3 = U[0], U[1], U[2]
+        div = (0.25 * (sl(u1, 0, 0, 0) + sl(u1, 0, -1, 0) + sl(u1, -1, 0, 0) + sl(u1, -1, -1, 0)
+                       - sl(u1, 0, 0, -1) - sl(u1, 0, -1, -1) - sl(u1, -1, 0, -1) - sl(u1, -1, -1, -1)) / dx[1]
+               + 0.25 * (sl(u2, 0, 0, 0) + sl(u2, 0, 0, -1) + sl(u2, -1, 0, 0) + sl(u2, -1, 0, -1)
+                         - sl(u2, 0, -1, 0) - sl(u2, 0, -1, -1) - sl(u2, -1, -1, 0) - sl(u2, -1, -1, -1)) / dx[2]
+               + 0.25 * (sl(u3, 0, 0, 0) + sl(u3, 0, 0, -1) + sl(u3, 0, -1, 0) + sl(u3, 0, -1, -1)
+                         - sl(u3, -1, 0, 0) - sl(u3, -1, 0, -1) - sl(u3, -1, -1, 0) - sl(u3, -1, -1, -1)) / dx[3])
+        scale = float(U.abs().max()) / min(dx[1], dx[2], dx[3])
+    m = float(torch.abs(div).max())
+    return m, m / max(scale, 1e-300)
+
+
 def run_ours(args, ws, rank, local):
     import torch
     from harm_harm_b200 import HARM_GUESS_MLP, HARM_GUESS_PREV, HARM_PREC_FP64, HARM_PREC_MIXED, Grid, Harm
@@ -320,6 +351,8 @@ def run_ours(args, ws, rank, local):
     if guess == HARM_GUESS_MLP:
         msp = max_over_ranks(msp, ws)
         value_prev = ws * zones * args.steps / (msp * 1e-3)
+    # div B of the headline path's state after its warm-up and timed steps
+    divb_abs, divb_rel = divb_max(g, torch.from_numpy(np.ascontiguousarray(geom[0, 26])).to(Pm.device), Pm)
     # accuracy of the headline path against the FP64 path after the same steps
     Pa, Pb = Pd.clone(), Pd.clone()
     dev.step_ch(Pa, dt0, precision=HARM_PREC_FP64, nsteps=args.err_steps, stats=False)
@@ -374,6 +407,8 @@ def run_ours(args, ws, rank, local):
             "fp64_value": value64, "speedup_vs_fp64": value / value64,
             "plain_guess_value": value_prev if guess == HARM_GUESS_MLP else value,
             "l1_rel_err_vs_fp64": l1, "linf_rel_err_vs_fp64": linf, "err_steps": args.err_steps,
+            "divb_max": {"abs": divb_abs, "rel": divb_rel,
+                         "of": "Toth corner divergence of sqrt(-g) B after the timed steps, rel to max|sqrt(-g) B|/min dx"},
             "newton_iters_per_cell": st["newton_iters"] / ninv,
             "newton_iters_per_cell_plain_guess": (stp if guess == HARM_GUESS_MLP else st)["newton_iters"]
             / max((stp if guess == HARM_GUESS_MLP else st)["cells_inverted"], 1.0),
