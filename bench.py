@@ -359,10 +359,9 @@ def run_ours(args, ws, rank, local):
     dev.step_ch(Pb, dt0, precision=prec, guess=guess, nsteps=args.err_steps, stats=False)
     act = (slice(None),) + g.active
     a, b = Pa.cpu().numpy()[act], Pb.cpu().numpy()[act]
-    l1 = {nm: float(np.abs(a[pl] - b[pl]).mean() / max(np.abs(a[pl]).mean(), 1e-300))
-          for nm, pl in (("rho", 0), ("u", 1), ("B1", 5), ("B2", 6), ("B3", 7))}
-    linf = {nm: float(np.abs(a[pl] - b[pl]).max() / max(np.abs(a[pl]).max(), 1e-300))
-            for nm, pl in (("rho", 0), ("u", 1), ("B1", 5), ("B2", 6), ("B3", 7))}
+    fields = (("rho", 0), ("u", 1), ("U1", 2), ("U2", 3), ("U3", 4), ("B1", 5), ("B2", 6), ("B3", 7))
+    l1 = {nm: float(np.abs(a[pl] - b[pl]).mean() / max(np.abs(a[pl]).mean(), 1e-300)) for nm, pl in fields}
+    linf = {nm: float(np.abs(a[pl] - b[pl]).max() / max(np.abs(a[pl]).max(), 1e-300)) for nm, pl in fields}
     del Pa, Pb
     # stage times and roofline of the dominant kernels
     stages = dev.time_stages(Pm, dt0, precision=prec, guess=guess, reps=3)
