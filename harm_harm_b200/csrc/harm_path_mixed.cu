@@ -3,7 +3,9 @@
 // the inversion of this path shares reciprocals between its FP64 divisions (harm_invert.cuh)
 #define HARM_INVERT_FAST_DIV 1
 // FP32 flux tiles at 3 resident blocks per SM (harm_common.cuh)
+#ifndef HARM_FLUXT_MINB
 #define HARM_FLUXT_MINB 3
+#endif
 #include <algorithm>
 #include <cudaTypedefs.h>
 #include <mutex>
