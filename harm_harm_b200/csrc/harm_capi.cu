@@ -81,13 +81,13 @@ static int create_ctx(const harm_grid* g, int device, harm_ctx** out) {
     // its tile loop, halving the warps that hide the face physics' latency), so it is opt-in.
     const char* e = getenv("HARM_B200_FLUX_STAGING");
     c->flux_tma = (e && strcmp(e, "tma") == 0);
-    // learned start: the mma.sync network as a kernel ahead of the inversion (default), the
-    // tcgen05 network as a kernel ahead of it ("tc") or inside the inversion kernel
-    // ("tc-fused").  The network's arithmetic is the same; on B200 the mma.sync kernel measured
-    // fastest (its activations stay in registers; the tcgen05 kernels stage each layer's
-    // activations through shared memory and synchronise a warpgroup per layer).
+    // learned start: the mma.sync network as a kernel ahead of the inversion (default) or
+    // inside the inversion kernel ("mma-fused"), the tcgen05 network as a kernel ahead of it
+    // ("tc") or inside the inversion kernel ("tc-fused").  The network's arithmetic is the
+    // same in all four.
     const char* m = getenv("HARM_B200_MLP_ENGINE");
-    c->mlp_tc = (m && strcmp(m, "tc") == 0) ? 1 : (m && strcmp(m, "tc-fused") == 0) ? 2 : 0;
+    c->mlp_tc = (m && strcmp(m, "tc") == 0) ? 1 : (m && strcmp(m, "tc-fused") == 0) ? 2
+              : (m && strcmp(m, "mma-fused") == 0) ? 3 : 0;
     CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
   }
   CK(cudaMemset(c->d_dtslots, 0xFF, 6 * sizeof(unsigned long long)));

@@ -63,7 +63,8 @@ struct harm_ctx {
   int mlp_tc;              // learned start: 0 mma.sync network kernel ahead of the inversion
                            // (default), 1 tcgen05 network kernel ahead of it
                            // (HARM_B200_MLP_ENGINE=tc), 2 tcgen05 inside the inversion
-                           // kernel (=tc-fused)
+                           // kernel (=tc-fused), 3 mma.sync inside the inversion kernel
+                           // (=mma-fused)
   int num_sms;
   unsigned long long launches;  // kernels launched by this context
 };

@@ -386,6 +386,67 @@ __global__ void __launch_bounds__(256, HARM_MLP_TC_BLOCKS) k_mlp_guess_tc(Dims d
   mlp_tc_end(B, st);
 }
 
+// The learned start inside the inversion kernel with the warp-level mma.sync network: a
+// persistent grid walks the cell tiles (k_invert's CellTile order); for each tile every warp
+// evaluates the network for its 32 cells (BF16 tensor cores, FP32 accumulation, no block
+// barrier), then each thread runs the Newton inversion of its cell from that start.  The
+// warps of an SM interleave network phases (tensor and special-function pipes) with Newton
+// phases (FP64 pipe), and neither U nor the start makes an extra trip through HBM.
+#ifndef HARM_INVERT_MMA_BLOCKS
+#define HARM_INVERT_MMA_BLOCKS HARM_INVERT_BLOCKS
+#endif
+template <int PATH>
+__global__ void __launch_bounds__(256, HARM_INVERT_MMA_BLOCKS) k_invert_mma(Dims d, Phys ph, const double* __restrict__ U,
+                                                        const double* __restrict__ pb, double* __restrict__ pf,
+                                                        int8_t* __restrict__ pflag, const double* __restrict__ geom,
+                                                        const double* __restrict__ aux, unsigned int* __restrict__ rare,
+                                                        unsigned int* __restrict__ nrare, double* __restrict__ stats,
+                                                        CellTile ct, const MlpPacked* __restrict__ mlp) {
+  __shared__ MlpPacked sm;
+  __shared__ MlpWarpScratch wsc[8];
+  mlp_load_packed(sm, mlp);
+  __syncthreads();
+  const dim3 gg = cell_grid_dev(d, ct);
+  const int gx = (int)gg.x;
+  const long long ntiles = (long long)gg.x * gg.y * gg.z;
+  double iters_d = 0.0, fb_d = 0.0;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    int i, j, k;
+    const long long rest = tile / gx;
+    const bool valid = tile_cell(d.n1, d.n2, d.n3, ct, (int)(tile % gx), (int)(rest % gg.y), (int)(rest / gg.y), i, j, k);
+    float f[MLP_IN];
+    double D = 0.0;
+    if (valid) mlp_cell_features(d, U, geom, i, j, k, f, D);
+    float y[MLP_OUT];
+    mlp_warp_eval(sm, wsc[threadIdx.x >> 5], f, valid, y);
+    if (valid) {
+      double w = D * exp((double)y[0] + (double)sm.start_bias);
+      w = (w > 0.0 && isfinite(w)) ? w : -1.0;
+      invert_cell<true>(d, ph, U, pb, pf, pflag, geom, aux, rare, nrare, i, j, k, w, iters_d, fb_d);
+    }
+  }
+  if (stats) {
+    warp_add_atomic(iters_d, stats + 0);
+    warp_add_atomic(fb_d, stats + 2);
+  }
+}
+
+// k_invert_mma over every active cell: one persistent grid of HARM_INVERT_MMA_BLOCKS blocks
+// per SM (fewer when there are fewer tiles)
+template <int PATH>
+static int launch_invert_mma(harm_ctx* c, const Dims& d, const Phys& ph, const CellTile& ct, const double* pb,
+                             double* pf, int8_t* pflag, double* stats) {
+  const dim3 g = cell_grid(d.n1, d.n2, d.n3, ct);
+  const long long ntiles = (long long)g.x * g.y * g.z;
+  const long long cap = (long long)HARM_INVERT_MMA_BLOCKS * c->num_sms;
+  const unsigned grid = (unsigned)(ntiles < cap ? ntiles : cap);
+  k_invert_mma<PATH><<<grid, 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
+                                                   c->d_nrare, stats, ct, reinterpret_cast<const MlpPacked*>(c->d_mlp));
+  c->launches++;
+  CK(cudaGetLastError());
+  return 0;
+}
+
 // The tensor-core record follows the mma.sync record in the context's network buffer.
 static inline const MlpTc* mlp_tc_of(const harm_ctx* c) {
   return reinterpret_cast<const MlpTc*>(reinterpret_cast<const char*>(c->d_mlp) + sizeof(MlpPacked));

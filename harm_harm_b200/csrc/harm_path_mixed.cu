@@ -135,6 +135,8 @@ int hp_update_mixed(harm_ctx* c, const StepCoef& sc, const double* pi, const dou
   CK(cudaMemsetAsync(c->d_nrare, 0, sizeof(unsigned int), c->stream));
   if (sc.guess == HARM_GUESS_MLP && c->mlp_tc == 2) {
     if (int rc = launch_invert_tc<1>(c, d, ph, pb, pf, pflag, stats)) return rc;
+  } else if (sc.guess == HARM_GUESS_MLP && c->mlp_tc == 3) {
+    if (int rc = launch_invert_mma<1>(c, d, ph, ct, pb, pf, pflag, stats)) return rc;
   } else if (sc.guess == HARM_GUESS_MLP) {
     if (c->mlp_tc == 1) {
       if (int rc = launch_mlp_guess_tc<1>(c, d)) return rc;

@@ -1,7 +1,8 @@
 """GPU tests of the learned start on the tcgen05 tensor cores (harm_mlp_tc.cuh), through the
 C ABI.  HARM_B200_MLP_ENGINE selects the engine of a context: the mma.sync network in a kernel
-ahead of the inversion (default, "mma"), the tcgen05 network in a kernel ahead of it ("tc"),
-or the tcgen05 network inside the inversion kernel ("tc-fused").  The engines compute the same
+ahead of the inversion (default, "mma"), the mma.sync network inside the inversion kernel
+("mma-fused"), the tcgen05 network in a kernel ahead of it ("tc"), or the tcgen05 network
+inside the inversion kernel ("tc-fused").  The engines compute the same
 BF16 products with FP32 accumulation in different orders, so their outputs agree to the BF16
 rounding of the activations; both are checked against the oracle's double-precision forward
 pass.  Steps with every engine match the plain steps within the Newton tolerance."""
@@ -33,14 +34,14 @@ def _harm(g, geom, conn, aux, engine):
 @pytest.fixture(scope="module")
 def engines(cuda):
     g, geom, conn, aux, P = make_torus(64, 64, 1)
-    tc, mma, fused = (_harm(g, geom, conn, aux, e) for e in ("tc", "mma", "tc-fused"))
-    yield cuda, g, geom, conn, aux, P, tc, mma, fused
-    for dev in (tc, mma, fused):
+    tc, mma, fused, mfused = (_harm(g, geom, conn, aux, e) for e in ("tc", "mma", "tc-fused", "mma-fused"))
+    yield cuda, g, geom, conn, aux, P, tc, mma, fused, mfused
+    for dev in (tc, mma, fused, mfused):
         dev.close()
 
 
 def test_tensor_core_network_matches_mma_sync_and_oracle(engines):
-    torch, g, geom, conn, aux, P0, tc, mma, _ = engines
+    torch, g, geom, conn, aux, P0, tc, mma, _, _ = engines
     f, t, *_ = _synth(torch, tc, 80000, 11)
     norm, params, _ = _train(torch, tc, f, t, steps=3000)
     tc.mlp_set(params, norm)
@@ -65,10 +66,10 @@ def test_tensor_core_network_matches_mma_sync_and_oracle(engines):
 
 
 def test_tensor_core_learned_steps_match_plain_and_mma_sync_steps(engines):
-    torch, g, geom, conn, aux, P0, tc, mma, fused = engines
+    torch, g, geom, conn, aux, P0, tc, mma, fused, mfused = engines
     _, f, t, _ = _torus_pairs(torch, tc, P0)
     norm, params, _ = _train(torch, tc, f, t, steps=3000)
-    for dev in (tc, mma, fused):
+    for dev in (tc, mma, fused, mfused):
         dev.mlp_set(params, norm)
     P = torch.from_numpy(P0).cuda()
     tc.bound_prim(P)
@@ -76,7 +77,7 @@ def test_tensor_core_learned_steps_match_plain_and_mma_sync_steps(engines):
     dta, sta = tc.step_ch(Pa, 1e-3, precision=HARM_PREC_MIXED, guess=HARM_GUESS_PREV, nsteps=3)
     a = Pa.cpu().numpy()
     runs = {}
-    for name, dev in (("mma.sync", mma), ("tcgen05", tc), ("tcgen05 fused", fused)):
+    for name, dev in (("mma.sync", mma), ("mma.sync fused", mfused), ("tcgen05", tc), ("tcgen05 fused", fused)):
         Pb = P.clone()
         dtb, stb = dev.step_ch(Pb, 1e-3, precision=HARM_PREC_MIXED, guess=HARM_GUESS_MLP, nsteps=3)
         b = Pb.cpu().numpy()
@@ -90,10 +91,13 @@ def test_tensor_core_learned_steps_match_plain_and_mma_sync_steps(engines):
           " ".join("%s %.3f" % kv for kv in runs.items()))
     for name in ("tcgen05", "tcgen05 fused"):
         assert abs(runs[name] - runs["mma.sync"]) < 0.05 * runs["mma.sync"]
+    # the fused mma.sync kernel evaluates the same network with the same arithmetic
+    assert runs["mma.sync fused"] == runs["mma.sync"]
 
 
 @pytest.mark.parametrize("engine,precision", [("tc", HARM_PREC_MIXED), ("tc-fused", HARM_PREC_MIXED),
-                                              ("tc", HARM_PREC_FP64), ("tc-fused", HARM_PREC_FP64)])
+                                              ("tc", HARM_PREC_FP64), ("tc-fused", HARM_PREC_FP64),
+                                              ("mma-fused", HARM_PREC_MIXED), ("mma-fused", HARM_PREC_FP64)])
 def test_tensor_core_learned_steps_3d(cuda, engine, precision):
     """3-D tiles (16 i x 8 k at one j) with a ragged edge in i and k, on both arithmetic paths."""
     torch = cuda
