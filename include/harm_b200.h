@@ -163,6 +163,7 @@ typedef struct harm_ctx harm_ctx;
      HARM_B200_MLP_ENGINE=tc      learned start on tcgen05 tensor cores, in a kernel ahead
                                   of the inversion
      HARM_B200_MLP_ENGINE=tc-fused  the same inside the inversion kernel
+     HARM_B200_MLP_ENGINE=mma-fused the mma.sync network inside the inversion kernel
                                   (default: mma.sync tensor cores, in a kernel ahead of the
                                   inversion; same network, same results to the BF16
                                   rounding of its activations) */
