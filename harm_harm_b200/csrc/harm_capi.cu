@@ -226,6 +226,16 @@ static void add_stats(harm_ctx* c, harm_stats* stats, double inverted) {
 extern "C" int harm_b200_advance(harm_ctx* c, int precision, int guess, int timeorder, int numtimeorders,
                                  const double* d_pi, const double* d_pb, double* d_pf, int8_t* d_pflag, double dt,
                                  const double CUf[4], const double Cunew[4], double* ndt, harm_stats* stats) {
+  // The conserved state of a substep is formed from U_i and dU alone: U_f = CUf0 U_i +
+  // CUf2 dt dU (UFSET global.stepch.h:1 without the CUf1 U_f term) and, on the final
+  // substep, ucum = Cunew0 U_i + Cunew1 dt dU + Cunew2 U_f (UCUMUPDATE :10 into an empty
+  // ucum).  That is exact for setup_rktimestep's TIMEORDER 1 and its RK2 midpoint; sets that
+  // carry U_f or ucum across substeps (TVD RK2, RK3, RK4) are refused.
+  if (timeorder < 0 || numtimeorders < 1 || timeorder >= numtimeorders)
+    return seterr_msg("timeorder must lie in [0, numtimeorders)", 2);
+  if (CUf[1] != 0.0 || (timeorder < numtimeorders - 1 && (Cunew[0] != 0.0 || Cunew[1] != 0.0 || Cunew[2] != 0.0)))
+    return seterr_msg("RK coefficients that carry U_f or ucum across substeps are not supported (CUf[1] must be 0 "
+                      "and Cunew[0..2] 0 before the final substep)", 2);
   Dims d = dims_of(c->g);
   c->h_scal[0] = dt;
   CK(cudaMemcpyAsync(c->d_dt, c->h_scal, sizeof(double), cudaMemcpyHostToDevice, c->stream));

@@ -164,9 +164,10 @@ class Harm:
         return tuple(ndt)
 
     def advance(self, timeorder: int, pi, pb, pf, pflag, dt: float, precision: int = N.HARM_PREC_FP64,
-                guess: int = N.HARM_GUESS_PREV, numtimeorders: int = 2):
-        CUf = (C.c_double * 4)(*RK2_CUF[timeorder])
-        Cun = (C.c_double * 4)(*RK2_CUNEW[timeorder])
+                guess: int = N.HARM_GUESS_PREV, numtimeorders: int = 2, CUf=None, Cunew=None):
+        """one RK substep; CUf/Cunew default to the RK2 midpoint's coefficients of this substep"""
+        CUf = (C.c_double * 4)(*(RK2_CUF[timeorder] if CUf is None else CUf))
+        Cun = (C.c_double * 4)(*(RK2_CUNEW[timeorder] if Cunew is None else Cunew))
         ndt = C.c_double()
         st = N.harm_stats()
         self._check(self.lib.harm_b200_advance(self._ctx, precision, guess, timeorder, numtimeorders, _ptr(pi), _ptr(pb),

@@ -201,7 +201,10 @@ int harm_b200_fluxcalc(harm_ctx *ctx, int precision, const double *d_pb,
    fluxes of d_pb, U_i = primtoU(d_pi), source(d_pb), U_f = CUf0 U_i + CUf1 U_f +
    CUf2 dt dU, ucum, then Utoprimgen (utoprimgen.c:32) into d_pf with d_pb as guess,
    then fixup1zone (fixup.c:561).  ndt = defcon*wavedt (prepare_globaldt advance.c:1558).
-   d_pflag[k][j][i] (active and ghost layout of P) receives the inversion codes. */
+   d_pflag[k][j][i] (active and ghost layout of P) receives the inversion codes.
+   Coefficients: U_f and ucum are formed from U_i and dU of this substep only, which is exact
+   for setup_rktimestep's TIMEORDER 1 and RK2 midpoint (CUf[1] = 0; Cunew[0..2] = 0 before
+   the final substep); other sets (TVD RK2, RK3, RK4) return 2. */
 int harm_b200_advance(harm_ctx *ctx, int precision, int guess, int timeorder,
                       int numtimeorders, const double *d_pi, const double *d_pb,
                       double *d_pf, int8_t *d_pflag, double dt, const double CUf[4],

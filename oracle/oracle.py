@@ -99,14 +99,14 @@ class Oracle:
         lib().orc_fluxcalc(C.byref(self.o), _p(pb), _p(F1), _p(F2), _p(F3), ndt)
         return tuple(ndt)
 
-    def advance(self, timeorder, pi, pb, pf, pflag, dt):
+    def advance(self, timeorder, pi, pb, pf, pflag, dt, numtimeorders=2, CUf=None, Cunew=None):
         from harm_harm_b200.harm import RK2_CUF, RK2_CUNEW
-        CUf = np.array(RK2_CUF[timeorder])
-        Cun = np.array(RK2_CUNEW[timeorder])
+        CUf = np.array(RK2_CUF[timeorder] if CUf is None else CUf, dtype=np.float64)
+        Cun = np.array(RK2_CUNEW[timeorder] if Cunew is None else Cunew, dtype=np.float64)
         ndt = C.c_double()
         st = N.harm_stats()
-        lib().orc_advance(C.byref(self.o), timeorder, 2, _p(pi), _p(pb), _p(pf), _p(pflag), dt, _p(CUf), _p(Cun),
-                          C.byref(ndt), C.byref(st))
+        lib().orc_advance(C.byref(self.o), timeorder, numtimeorders, _p(pi), _p(pb), _p(pf), _p(pflag), dt, _p(CUf),
+                          _p(Cun), C.byref(ndt), C.byref(st))
         return ndt.value, st.as_dict()
 
     def post_fixup(self, pf, pflag):
