@@ -27,7 +27,7 @@ using hbasync::smem_u32;
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
-// 4-D tiled load into this CTA's shared memory (no multicast)
+// 4-D tiled load into this CTA's own shared memory
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z,
                                             int w) {
   asm volatile(
