@@ -1,0 +1,168 @@
+"""The CPU oracle (oracle/*.c) pinned to the reference HARM code itself.
+
+Two sources of reference output:
+  - the golden fixtures of tests/golden/ (made by tests/golden/make_golden.py from the
+    reference binaries): a 2-D torus step with both substeps' advance()/fluxcalc() records,
+    and Utoprimgen() of physical and unphysical conserved states;
+  - the reference binaries of oracle/_ref/ run live (built by oracle/ref/build.sh from the
+    reference's sources where those are present), for 2-D and 3-D grids and every
+    reconstruction whose parity holds.
+The oracle gets the reference's own inputs (its metric, connection and floor tables and its
+bounded substep input), so what is compared is the algorithm of each entry point.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from harm_harm_b200 import Grid
+from oracle import oracle as O
+from oracle import ref as R
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def rel(a, b, floor_frac=1e-12):
+    """max |a-b| / (|a| + |b| + floor), floor = floor_frac * max|b|"""
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    floor = floor_frac * max(np.abs(b).max(), 1e-300)
+    return float((np.abs(a - b) / (np.abs(a) + np.abs(b) + floor)).max())
+
+
+def normwise(a, b):
+    """max |a-b| / max |b|"""
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(b).max(), 1e-300))
+
+
+def active_faces(g, d):
+    gg = g.g
+    k = slice(gg.ng3, gg.ng3 + gg.n3 + (1 if d == 3 else 0))
+    j = slice(gg.ng, gg.ng + gg.n2 + (1 if d == 2 else 0))
+    i = slice(gg.ng, gg.ng + gg.n1 + (1 if d == 1 else 0))
+    return (slice(None), k, j, i)
+
+
+# ------------------------------------------------------------------ golden fixtures
+
+@pytest.fixture(scope="module")
+def torus32():
+    d = np.load(os.path.join(GOLDEN, "ref_2d_mc_32x32.npz"))
+    g = Grid.torus(32, 32, 1, lim=0)
+    assert abs(g.g.startx[1] - d["grid"][5]) < 1e-15 and abs(g.g.dx[1] - d["grid"][9]) < 1e-15
+    orc = O.Oracle(g, d["geom"], d["conn"], d["aux"])
+    return g, d, orc
+
+
+@pytest.mark.parametrize("to", [0, 1])
+def test_golden_fluxcalc(torus32, to):
+    g, d, orc = torus32
+    pb = np.ascontiguousarray(d[f"s{to}_pb"])
+    F = [np.zeros_like(pb) for _ in range(3)]
+    ndt = orc.fluxcalc(pb.copy(), *F)
+    for dd in (1, 2):
+        a = F[dd - 1][active_faces(g, dd)]
+        for pl in range(8):
+            assert rel(a[pl], d[f"s{to}_F{dd}"][pl]) < 1e-12, (dd, pl)
+        assert abs(ndt[dd - 1] - d[f"s{to}_ndtdir"][dd - 1]) <= 1e-13 * ndt[dd - 1]
+
+
+@pytest.mark.parametrize("to", [0, 1])
+def test_golden_advance(torus32, to):
+    """advance() of one substep from the reference's bounded input: flux, conserved update
+    with sources, inversion and fixup1zone, and the next dt"""
+    g, d, orc = torus32
+    pb = np.ascontiguousarray(d[f"s{to}_pb"])
+    pi = np.ascontiguousarray(d["s0_pb"])  # RK2 midpoint: both substeps start from P^n
+    args = d[f"s{to}_args"]
+    pf = pb.copy()
+    flag = np.zeros(pb.shape[1:], dtype=np.int8)
+    ndt, st = orc.advance(to, pi.copy(), pb.copy(), pf, flag, float(args[0]), CUf=args[4:8], Cunew=args[8:12])
+    act = (slice(None),) + g.active
+    for pl in range(8):
+        assert rel(pf[act][pl], d[f"s{to}_pf"][pl]) < 1e-12, pl
+    assert (flag[g.active] == d[f"s{to}_pflag"]).all()
+    assert abs(ndt - d[f"s{to}_ndt"][0]) <= 1e-13 * ndt
+
+
+PHYSICAL_AND_FAILING = ["physical", "physical_far_guess", "momentum_beyond_light_cone", "negative_density",
+                        "energy_low", "energy_high", "nan_energy"]
+
+
+@pytest.mark.parametrize("kind", PHYSICAL_AND_FAILING)
+def test_golden_utoprimgen(kind):
+    """Utoprimgen of physical states and of states the hot inversion cannot invert: the same
+    primitives (NaN where the reference returns NaN) and failure codes"""
+    d = np.load(os.path.join(GOLDEN, "ref_utoprimgen_points.npz"))
+    g = Grid.torus(32, 32, 1, lim=0)
+    sel = np.nonzero(d["kind"] == kind)[0]
+    assert len(sel) > 0
+    iters_equal = 0
+    for p in sel:
+        P, fl, it = O.utoprimgen_point(g, d["geomrec"][:, p], d["U"][p], d["guess"][p])
+        assert fl == d["pflag"][p], (kind, p, fl, d["pflag"][p])
+        ref = d["P"][p]
+        assert (np.isnan(P) == np.isnan(ref)).all()
+        m = ~np.isnan(ref)
+        assert rel(P[m], ref[m]) < 1e-10, (kind, p)
+        iters_equal += it == d["iters"][p]
+    if kind.startswith("physical") or kind in ("negative_density", "energy_low"):
+        assert iters_equal == len(sel)
+
+
+# ------------------------------------------------------------------ live reference runs
+
+LIVE = {  # name: (n1, n2, n3, ng, lim, flux, tolerance, measure)
+    "2d_mc_64x64": (64, 64, 1, 4, 0, 0, 1e-12, "rel"),
+    # the reference stores its metric per (i,j,k), and its numerically differentiated
+    # Jacobian varies with x3 by ~1e-11 of each component; the oracle uses k=0's tables on
+    # every plane, so 3-D fluxes agree to ~1e-10 of each field's largest face value
+    "3d_mc_32x24x8": (32, 24, 8, 4, 0, 0, 2e-10, "norm"),
+    "3d_para_32x24x8": (32, 24, 8, 4, 1, 0, 2e-10, "norm"),
+}
+
+
+def live(name):
+    n1, n2, n3, ng, lim, flux, tol, how = LIVE[name]
+    if not R.available(n1, n2, n3, ng):
+        pytest.skip("reference binary not built (oracle/ref/build.sh needs the reference sources)")
+    path = R.run(n1, n2, n3, ng, lim=lim, flux=flux, nsteps=2, every=1, substeps=(1, 2))
+    g = Grid.torus(n1, n2, n3, lim=lim, fluxmethod=flux)
+    rr = R.RefRun(path, g)
+    return g, rr, tol, (rel if how == "rel" else normwise)
+
+
+@pytest.mark.parametrize("name", list(LIVE))
+def test_live_substeps(name):
+    g, rr, tol, err = live(name)
+    orc = O.Oracle(g, rr.geom, rr.conn, rr.aux)
+    act = (slice(None),) + g.active
+    nd = 3 if g.g.n3 > 1 else 2
+    for step in (1, 2):
+        for to in (0, 1):
+            pb = rr.sub(step, to, "pb")
+            F = [np.zeros_like(pb) for _ in range(3)]
+            ndt = orc.fluxcalc(pb.copy(), *F)
+            for dd in range(1, nd + 1):
+                Fr = rr.sub(step, to, f"F{dd}")
+                sl = active_faces(g, dd)
+                for pl in range(8):
+                    assert err(F[dd - 1][sl][pl], Fr[sl][pl]) < tol, (step, to, dd, pl)
+                assert abs(ndt[dd - 1] - rr.sub(step, to, "ndtdir")[dd - 1]) <= max(tol, 1e-13) * ndt[dd - 1]
+            args = rr.sub(step, to, "args")
+            pf = pb.copy()
+            flag = np.zeros(pb.shape[1:], dtype=np.int8)
+            ndt1, _ = orc.advance(to, rr.sub(step, to, "pi"), pb.copy(), pf, flag, float(args[0]), CUf=args[4:8],
+                                  Cunew=args[8:12])
+            pfr = rr.sub(step, to, "pf")
+            for pl in range(8):
+                assert err(pf[act][pl], pfr[act][pl]) < tol, (step, to, "pf", pl)
+            assert (flag[g.active] == rr.sub(step, to, "pflag")[g.active]).all()
+            assert abs(ndt1 - rr.sub(step, to, "ndt")[0]) <= max(tol, 1e-13) * ndt1
+
+
+def test_reference_metric_locations_shared():
+    """The device keeps 4 metric locations per (i,j): in the reference's tables FACE3 equals
+    CENT, CORN1 equals FACE2 and CORN2 equals FACE1 exactly"""
+    g, rr, _, _ = live("2d_mc_64x64")
+    G = rr.geom8
+    assert np.array_equal(G[3], G[0]) and np.array_equal(G[4], G[2]) and np.array_equal(G[5], G[1])
