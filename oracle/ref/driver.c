@@ -27,6 +27,7 @@
  *       steps listed in HREF_SUBSTEP_STEPS also every substep's advance() inputs and outputs
  *       (sub_<step>_<timeorder>_{pi,pb,pf,pflag,args,ndt}), its fluxcalc() fluxes
  *       (_F1,_F2,_F3,_ndtdir) and post_fixup()'s input and output (_fixin,_fixflag,_fixout),
+ *       and every per-direction boundary call's input and output (bnd_<step>_<n>_{in,out,info}),
  *       as extended arrays [k][j][i][pl] with the ghost zones
  *   harm_ref_<cfg> points <outdir> <nthreads> <infile>
  *       Utoprimgen (utoprimgen.c:32) of every record of <infile> (raw doubles: i, j, U[8],
@@ -408,8 +409,37 @@ int __wrap_post_fixup(int stageit, SFTYPE boundtime, FTYPE (*pv)[NSTORE2][NSTORE
   return r;
 }
 
+/* every bound_prim_user_dir() call (bounds.fishmon.c:15, called per direction from
+   bound_anyprim step_ch.c) of a wanted step: its input, output and arguments, numbered in
+   call order within the step */
+static int bnd_calls = 0;
+
+int __real_bound_prim_user_dir(int boundstage, SFTYPE boundtime, int whichdir, int boundvartype,
+                               FTYPE (*prim)[NSTORE2][NSTORE3][NPR]);
+
+int __wrap_bound_prim_user_dir(int boundstage, SFTYPE boundtime, int whichdir, int boundvartype,
+                               FTYPE (*prim)[NSTORE2][NSTORE3][NPR])
+{
+  int r, want = step_wanted(nstep + 1);
+  if (want) {
+    double v[4];
+    snprintf(sub_prefix, sizeof sub_prefix, "bnd_%ld_%d", nstep + 1, bnd_calls);
+    v[0] = whichdir; v[1] = boundvartype; v[2] = boundstage; v[3] = BOUNDPRIMTYPE;
+    dump_scalars("info", v, 4);
+    dump_ext("in", prim);
+  }
+  r = __real_bound_prim_user_dir(boundstage, boundtime, whichdir, boundvartype, prim);
+  if (want) {
+    snprintf(sub_prefix, sizeof sub_prefix, "bnd_%ld_%d", nstep + 1, bnd_calls);
+    dump_ext("out", prim);
+    bnd_calls++;
+  }
+  return r;
+}
+
 static void do_step(void)
 {
+  bnd_calls = 0;
   nstroke = 0;
   step_ch_full(GLOBALPOINT(pglobal), GLOBALPOINT(pstagglobal), GLOBALPOINT(unewglobal),
                GLOBALPOINT(vpotarrayglobal), GLOBALPOINT(Bhatglobal), GLOBALPOINT(gp_l),
