@@ -257,8 +257,9 @@ def train_guess(dev, Pd, dt0, prec, args):
 
 
 def divb_max(g, geom_cent_gdet, P):
-    """max over active corners of Toth's corner divergence of sqrt(-g) B (the quantity flux-CT
-    keeps at round-off), absolute and relative to max |sqrt(-g) B| / min(dx); P on the device"""
+    """max of Toth's corner divergence of sqrt(-g) B (the quantity flux-CT keeps at round-off)
+    over the corners whose cells are all active in x1 and x2 (x3 is periodic), absolute and
+    relative to max |sqrt(-g) B| / min(dx); P on the device"""
     import torch
     gg = g.g
     U = P[5:8] * geom_cent_gdet[None, None]
@@ -266,11 +267,11 @@ def divb_max(g, geom_cent_gdet, P):
     dx = gg.dx
 
     def sl(a, dk, dj, di):
-        return a[ng3 + dk:ng3 + dk + n3 + 1, ng + dj:ng + dj + n2 + 1, ng + di:ng + di + n1 + 1]
+        return a[ng3 + dk:ng3 + dk + n3 + 1, ng + 1 + dj:ng + dj + n2, ng + 1 + di:ng + di + n1]
 
     if n3 == 1:
         u1, u2 = U[0, 0], U[1, 0]
-        s2 = (lambda a, dj, di: a[ng + dj:ng + dj + n2 + 1, ng + di:ng + di + n1 + 1])
+        s2 = (lambda a, dj, di: a[ng + 1 + dj:ng + dj + n2, ng + 1 + di:ng + di + n1])
         div = (0.5 * (s2(u1, 0, 0) + s2(u1, -1, 0) - s2(u1, 0, -1) - s2(u1, -1, -1)) / dx[1]
                + 0.5 * (s2(u2, 0, 0) + s2(u2, 0, -1) - s2(u2, -1, 0) - s2(u2, -1, -1)) / dx[2])
         scale = float(U[:2].abs().max()) / min(dx[1], dx[2])

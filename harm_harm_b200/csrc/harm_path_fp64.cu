@@ -20,69 +20,213 @@ __global__ void k_copy_ghosts(Dims d, const double* __restrict__ pb, double* __r
 }
 
 // ------------------------------------------------------------------ boundary conditions
+//
+// bound_prim of the torus problem (step_ch.c:1332 -> bound_prim_user_dir,
+// initboundcode/bounds.fishmon.c:15), direction by direction as bound_anyprim does:
+//   x1: extrapfunc (bounds.tools.c:1417; HORIZONEXTRAP = OUTEREXTRAP = 3) fills the ghost
+//       cells of each active (j,k) line from its three cells next to the boundary; at the
+//       outer boundary inflow_check_rel4vel and limit_gamma follow (bound_x1up_outflow :337);
+//   x2: polar reflection in the same phi plane with U2, B2 negated (bound_x2dn_polaraxis :751;
+//       a run without MPI has periodicx3 = 0 and so no transfer across the pole), then
+//       poledeath (:2004) on the ghost cell and the first active cell at each pole
+//       (POLEDEATH 1, POLEINTERPTYPE 3) and POLEGAMMADEATH's Lorentz-factor limit there,
+//       over every i of the extended grid;
+//   x3: periodic (:1114), over every (i,j) of the extended grid.
+// One thread per boundary line; the arithmetic is the oracle's (oracle/orc_bound.c) in the
+// same order.
 
-__global__ void k_bound_x1(Dims d, Phys ph, double* P, int8_t* flag, const double* __restrict__ geom) {
+#define BMINMOD(a, b) (((a) * (b) <= 0) ? 0.0 : ((fabs(a) < fabs(b)) ? (a) : (b)))
+
+__device__ __forceinline__ void cent_geo(const Dims& d, const double* __restrict__ geom, int ii, int jj,
+                                         Geo<double>& g) {
+  load_geo<double, double>(geom + (size_t)HARM_LOC_CENT * HARM_NGF * d.plane, d.plane, (size_t)jj * d.n1e + ii, g);
+}
+
+// extrapfunc for the ghost cells of the x1 line (jj,kk) on one side
+__global__ void k_bound_x1_extrap(Dims d, Phys ph, double* __restrict__ P, const double* __restrict__ geom) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long n = (long long)2 * d.ng * d.n2e * d.n3e;
-  if (t >= n) return;
-  int gq = (int)(t % (2 * d.ng));
-  long long r = t / (2 * d.ng);
-  int jj = (int)(r % d.n2e), kk = (int)(r / d.n2e);
-  if (gq < d.ng) {
-    int ii = gq;
-    size_t dst = cidx(d, ii, jj, kk), src = cidx(d, d.ng, jj, kk);
-    if (P)
-      for (int p = 0; p < NPR; p++) P[(size_t)p * d.cells + dst] = P[(size_t)p * d.cells + src];
-    if (flag) flag[dst] = flag[src];
-  } else {
-    int ii = d.ng + d.n1 + (gq - d.ng);
-    size_t dst = cidx(d, ii, jj, kk), src = cidx(d, d.ng + d.n1 - 1, jj, kk);
-    if (flag) flag[dst] = flag[src];
-    if (!P) return;
-    double pr[NPR];
-    for (int p = 0; p < NPR; p++) pr[p] = P[(size_t)p * d.cells + src];
-    Geo<double> g;
-    load_geo<double, double>(geom, d.plane, (size_t)jj * d.n1e + ii, g);
-    // inflow_check_rel4vel (fixup.c:3255) for the outer radial boundary
-    double ucon[4], gamma, qsq;
-    ucon_of<double>(pr, g, ucon, gamma, qsq);
-    if (ucon[1] < 0.) {
-      pr[HARM_U1] /= gamma; pr[HARM_U2] /= gamma; pr[HARM_U3] /= gamma;
-      double alpha = 1. / sqrt(-g.gcon[0]);
-      double betacon = g.gcon[1] * alpha * alpha;
-      pr[HARM_U1] = betacon / alpha;
-      double vsq = 0.;
-      for (int a = 1; a < 4; a++)
-        for (int b = 1; b < 4; b++) vsq += g.gcov[sym(a, b)] * pr[HARM_U1 + a - 1] * pr[HARM_U1 + b - 1];
-      if (vsq < 0.0 && vsq > -2.220446049250313e-16 * 100.0) vsq = 0.0;
-      if (vsq >= 1.0) vsq = 1.0 - 1.0 / (ph.gammamax * ph.gammamax);
-      gamma = 1. / sqrt(1. - vsq);
-      pr[HARM_U1] *= gamma; pr[HARM_U2] *= gamma; pr[HARM_U3] *= gamma;
+  if (t >= 2LL * d.n2 * d.n3) return;
+  const int up = (int)(t & 1);
+  long long r = t >> 1;
+  const int jj = (int)(r % d.n2) + d.ng, kk = (int)(r / d.n2) + d.ng3;
+  const int ri = up ? d.ng + d.n1 - 1 : d.ng;
+  const int ri2 = up ? ri - 1 : ri + 1, ri3 = up ? ri - 2 : ri + 2;
+  const double signdq = up ? -1.0 : 1.0;
+  Geo<double> gr, g2, g3;
+  cent_geo(d, geom, ri, jj, gr);
+  cent_geo(d, geom, ri2, jj, g2);
+  cent_geo(d, geom, ri3, jj, g3);
+  double p1[NPR], p2[NPR], p3[NPR];
+  const size_t c1 = cidx(d, ri, jj, kk), c2 = cidx(d, ri2, jj, kk), c3 = cidx(d, ri3, jj, kk);
+#pragma unroll
+  for (int pl = 0; pl < NPR; pl++) {
+    p1[pl] = P[(size_t)pl * d.cells + c1];
+    p2[pl] = P[(size_t)pl * d.cells + c2];
+    p3[pl] = P[(size_t)pl * d.cells + c3];
+  }
+  double Bd3 = 0.0, Bd3ri2 = 0.0, Bd3ri3 = 0.0;
+  for (int a = 1; a <= 3; a++) Bd3 += p1[HARM_B1 + a - 1] * gr.gcov[sym(3, a)];
+  for (int a = 1; a <= 3; a++) Bd3ri2 += p2[HARM_B1 + a - 1] * g2.gcov[sym(3, a)];
+  for (int a = 1; a <= 3; a++) Bd3ri3 += p3[HARM_B1 + a - 1] * g3.gcov[sym(3, a)];
+  double Dqp = Bd3ri3 - Bd3ri2, Dqm = Bd3ri2 - Bd3, Dqc = Bd3ri3 - Bd3;
+  const double dqBd3 = signdq * BMINMOD(BMINMOD(Dqp, Dqm), Dqc);
+  double ucref[4], ucref2[4], gam, qsq;
+  ucon_of<double>(p1, gr, ucref, gam, qsq);
+  ucon_of<double>(p2, g2, ucref2, gam, qsq);
+  double dq[NPR], dqlog[NPR], dqgd[NPR];
+#pragma unroll
+  for (int pl = 0; pl < NPR; pl++) {
+    Dqp = p3[pl] - p2[pl];
+    Dqm = p2[pl] - p1[pl];
+    Dqc = p3[pl] - p1[pl];
+    dq[pl] = signdq * BMINMOD(BMINMOD(Dqp, Dqm), Dqc);
+    Dqp = log(1.e-300 + fabs(p3[pl])) - log(1.e-300 + fabs(p2[pl]));
+    Dqm = log(1.e-300 + fabs(p2[pl])) - log(1.e-300 + fabs(p1[pl]));
+    Dqc = log(1.e-300 + fabs(p3[pl])) - log(1.e-300 + fabs(p1[pl]));
+    dqlog[pl] = signdq * BMINMOD(BMINMOD(Dqp, Dqm), Dqc);
+    Dqp = g3.gdet * p3[pl] - g2.gdet * p2[pl];
+    Dqm = g2.gdet * p2[pl] - gr.gdet * p1[pl];
+    Dqc = g3.gdet * p3[pl] - gr.gdet * p1[pl];
+    dqgd[pl] = signdq * BMINMOD(BMINMOD(Dqp, Dqm), Dqc);
+  }
+  // the slopes of u and the velocities fade out where u^t jumps between ri and ri2
+  const double xdqfrac = fabs(ucref[0] - ucref2[0]) / ucref[0];
+  double ydqfrac;
+  if (xdqfrac < 0.1) ydqfrac = 0.0;
+  else if (xdqfrac < 0.2) ydqfrac = (0.0 + (1.0 - 0.0) / (0.2 - 0.1) * (xdqfrac - 0.1));
+  else ydqfrac = 1.0;
+#pragma unroll
+  for (int a = 0; a < 4; a++) {
+    dq[HARM_UU + a] = dq[HARM_UU + a] * (1.0 - ydqfrac);
+    dqlog[HARM_UU + a] = dqlog[HARM_UU + a] * (1.0 - ydqfrac);
+  }
+  const double powerratio = (1.0 + (0.1));
+  for (int q = 1; q <= d.ng; q++) {
+    const int ii = up ? ri + q : ri - q;
+    const double di = (double)(ii - ri);
+    Geo<double> gi;
+    cent_geo(d, geom, ii, jj, gi);
+    double p[NPR];
+#pragma unroll
+    for (int pl = 0; pl < NPR; pl++) p[pl] = p1[pl];
+#pragma unroll
+    for (int pl = HARM_RHO; pl <= HARM_UU; pl++) {
+      double ftemp = exp(-signdq * dqlog[pl]) - powerratio, mydqlog;
+      if (ftemp >= 0.0) mydqlog = log(powerratio) / (-signdq);
+      else mydqlog = dqlog[pl];
+      p[pl] = exp(log(1.e-300 + fabs(p1[pl])) + mydqlog * di);
     }
-    limit_gamma<double>(ph.gammamax, pr, g);
-    for (int p = 0; p < NPR; p++) P[(size_t)p * d.cells + dst] = pr[p];
+#pragma unroll
+    for (int pl = HARM_U1; pl <= HARM_U3; pl++) p[pl] = p1[pl] + dq[pl] * di;
+#pragma unroll
+    for (int pl = HARM_B1; pl <= HARM_B2; pl++) {
+      const double igd = copysign(1.0, gi.gdet) / (fabs(gi.gdet) + 1.e-300);
+      p[pl] = (p1[pl] * fabs(gr.gdet + dqgd[pl] * di)) * igd;
+    }
+    {
+      const double Bu1 = p[HARM_B1], Bu2 = p[HARM_B2];
+      const double gcon03 = gi.gcon[sym(0, 3)], gcon13 = gi.gcon[sym(1, 3)], gcon23 = gi.gcon[sym(2, 3)],
+                   gcon33 = gi.gcon[sym(3, 3)];
+      const double gcov01 = gi.gcov[sym(0, 1)], gcov02 = gi.gcov[sym(0, 2)], gcov11 = gi.gcov[sym(1, 1)],
+                   gcov12 = gi.gcov[sym(1, 2)], gcov21 = gcov12, gcov22 = gi.gcov[sym(2, 2)],
+                   gcov03 = gi.gcov[sym(0, 3)], gcov13 = gi.gcov[sym(1, 3)], gcov23 = gi.gcov[sym(2, 3)];
+      const double myBd3 = Bd3 + dqBd3 * di;
+      const double ftemp = (1.0 - gcon03 * gcov03 - gcon13 * gcov13 - gcon23 * gcov23);
+      const double igd = copysign(1.0, ftemp) / (fabs(ftemp) + 1.e-300);
+      p[HARM_B3] = (myBd3 * gcon33 + Bu1 * gcon03 * gcov01 + Bu2 * gcon03 * gcov02 + Bu1 * gcon13 * gcov11 +
+                    Bu2 * gcon13 * gcov12 + Bu1 * gcon23 * gcov21 + Bu2 * gcon23 * gcov22) * igd;
+    }
+    if (up) {
+      // inflow_check_rel4vel (fixup.c:3255) for the outer radial boundary, then limit_gamma
+      double ucon[4], gamma, qsq2;
+      ucon_of<double>(p, gi, ucon, gamma, qsq2);
+      if (ucon[1] < 0.) {
+        p[HARM_U1] /= gamma; p[HARM_U2] /= gamma; p[HARM_U3] /= gamma;
+        double alpha = 1. / sqrt(-gi.gcon[0]);
+        double betacon = gi.gcon[1] * alpha * alpha;
+        p[HARM_U1] = betacon / alpha;
+        double vsq = 0.;
+        for (int a = 1; a < 4; a++)
+          for (int b = 1; b < 4; b++) vsq += gi.gcov[sym(a, b)] * p[HARM_U1 + a - 1] * p[HARM_U1 + b - 1];
+        if (vsq < 0.0 && vsq > -2.220446049250313e-16 * 100.0) vsq = 0.0;
+        if (vsq >= 1.0) vsq = 1.0 - 1.0 / (ph.gammamax * ph.gammamax);
+        gamma = 1. / sqrt(1. - vsq);
+        p[HARM_U1] *= gamma; p[HARM_U2] *= gamma; p[HARM_U3] *= gamma;
+      }
+      limit_gamma<double>(ph.gammamax, p, gi);
+    }
+    const size_t c = cidx(d, ii, jj, kk);
+#pragma unroll
+    for (int pl = 0; pl < NPR; pl++) P[(size_t)pl * d.cells + c] = p[pl];
   }
 }
 
-__global__ void k_bound_x2(Dims d, double* P, int8_t* flag) {
+// polar reflection of the ghost rows of column (ii,kk) at both poles
+__global__ void k_bound_x2_reflect(Dims d, double* __restrict__ P) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long n = (long long)2 * d.ng * d.n1e * d.n3e;
-  if (t >= n) return;
-  int ii = (int)(t % d.n1e);
-  long long r = t / d.n1e;
-  int gq = (int)(r % (2 * d.ng)), kk = (int)(r / (2 * d.ng));
-  int k = kk - d.ng3;
-  int ks = (d.n3 > 1) ? ((k + d.n3 / 2) % d.n3 + d.n3) % d.n3 + d.ng3 : kk;
-  int jj, js;
-  if (gq < d.ng) { jj = gq; js = 2 * d.ng - 1 - jj; }
-  else { jj = d.ng + d.n2 + (gq - d.ng); js = 2 * (d.ng + d.n2) - 1 - jj; }
-  size_t dst = cidx(d, ii, jj, kk), src = cidx(d, ii, js, ks);
-  if (flag) flag[dst] = flag[src];
-  if (!P) return;
-  for (int p = 0; p < NPR; p++) {
-    double v = P[(size_t)p * d.cells + src];
-    if (p == HARM_U2 || p == HARM_B2) v = -v;
-    P[(size_t)p * d.cells + dst] = v;
+  if (t >= 2LL * d.n1e * d.n3) return;
+  const int up = (int)(t & 1);
+  long long r = t >> 1;
+  const int ii = (int)(r % d.n1e), kk = (int)(r / d.n1e) + d.ng3;
+  for (int q = 1; q <= d.ng; q++) {
+    const int j = up ? d.n2 - 1 + q : -q;
+    const int rj = up ? 2 * (d.n2 - 1) - j + 1 : -j - 1;
+    const size_t dst = cidx(d, ii, j + d.ng, kk), src = cidx(d, ii, rj + d.ng, kk);
+#pragma unroll
+    for (int pl = 0; pl < NPR; pl++) {
+      double v = P[(size_t)pl * d.cells + src];
+      if (pl == HARM_U2 || pl == HARM_B2) v *= -1.;
+      P[(size_t)pl * d.cells + dst] = v;
+    }
+  }
+}
+
+// poledeath and POLEGAMMADEATH of column (ii,kk) at one pole: the ghost cell and the first
+// active cell take rho, u, U1, U3 (and B3 in 2-D) of the second active cell; U2 there is the
+// second cell's extrapolated linearly to zero at the pole, or zero where it flows into the
+// pole; then the Lorentz factor is limited (1.1, growing as r/10 beyond r = 10, where u^r > 0;
+// GAMMAMAX otherwise)
+__global__ void k_bound_x2_pole(Dims d, Phys ph, double startx2, double* __restrict__ P,
+                                const double* __restrict__ geom, const double* __restrict__ aux) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 2LL * d.n1e * d.n3) return;
+  const int up = (int)(t & 1);
+  long long r = t >> 1;
+  const int ii = (int)(r % d.n1e), kk = (int)(r / d.n1e) + d.ng3;
+  const int rj = up ? d.n2 - 2 : 1, js = up ? d.n2 - 1 : -1, poleloc = up ? d.n2 : 0;
+  const double Xr2 = startx2 + (rj + 0 + 0.5) * ph.dx2, X02 = startx2 + (poleloc + 0) * ph.dx2;
+  const size_t cr = cidx(d, ii, rj + d.ng, kk);
+  for (int j = js; j <= js + 1; j++) {
+    const size_t c = cidx(d, ii, j + d.ng, kk);
+#pragma unroll
+    for (int pl = HARM_RHO; pl <= HARM_U3; pl++) {
+      if (pl == HARM_U2) continue;
+      P[(size_t)pl * d.cells + c] = P[(size_t)pl * d.cells + cr];
+    }
+    double ftemp = P[(size_t)HARM_U2 * d.cells + cr];
+    const double X2 = startx2 + (j + 0 + 0.5) * ph.dx2;
+    if ((!up && ftemp > 0.0) || (up && ftemp < 0.0)) ftemp = 0.0;
+    P[(size_t)HARM_U2 * d.cells + c] = ftemp + (X2 - Xr2) * (ftemp - 0.0) / (Xr2 - X02);
+    if (d.n3 == 1) P[(size_t)HARM_B3 * d.cells + c] = P[(size_t)HARM_B3 * d.cells + cr];
+  }
+  for (int j = js; j <= js + 1; j++) {
+    const int jj = j + d.ng;
+    const size_t c = cidx(d, ii, jj, kk);
+    Geo<double> gi;
+    cent_geo(d, geom, ii, jj, gi);
+    double p[NPR], ucon[4], gamma, qsq;
+#pragma unroll
+    for (int pl = 0; pl < NPR; pl++) p[pl] = P[(size_t)pl * d.cells + c];
+    ucon_of<double>(p, gi, ucon, gamma, qsq);
+    if (ucon[1] > 0.0) {
+      const double rr = aux[(size_t)HARM_AUX_R * d.plane + (size_t)jj * d.n1e + ii];
+      const double lim = (rr <= 10.0) ? 1.1 : 1.1 * pow(rr / 10.0, 1.0);
+      limit_gamma<double>(lim, p, gi);
+    } else {
+      limit_gamma<double>(ph.gammamax, p, gi);
+    }
+#pragma unroll
+    for (int pl = 0; pl < NPR; pl++) P[(size_t)pl * d.cells + c] = p[pl];
   }
 }
 
@@ -100,6 +244,36 @@ __global__ void k_bound_x3(Dims d, double* P, int8_t* flag) {
   if (flag) flag[dst] = flag[src];
   if (P)
     for (int p = 0; p < NPR; p++) P[(size_t)p * d.cells + dst] = P[(size_t)p * d.cells + src];
+}
+
+// ghost-zone flags for post_fixup's neighbour test (bound_pflag step_ch.c:1637): x1 copies
+// of the nearest active cell, x2 reflection across the pole (with n3 > 1 from the column
+// across the pole), then x3 periodic (k_bound_x3)
+__global__ void k_bound_flags_x1(Dims d, int8_t* flag) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)2 * d.ng * d.n2e * d.n3e;
+  if (t >= n) return;
+  int gq = (int)(t % (2 * d.ng));
+  long long r = t / (2 * d.ng);
+  int jj = (int)(r % d.n2e), kk = (int)(r / d.n2e);
+  int ii = (gq < d.ng) ? gq : d.ng + d.n1 + (gq - d.ng);
+  int is = (gq < d.ng) ? d.ng : d.ng + d.n1 - 1;
+  flag[cidx(d, ii, jj, kk)] = flag[cidx(d, is, jj, kk)];
+}
+
+__global__ void k_bound_flags_x2(Dims d, int8_t* flag) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)2 * d.ng * d.n1e * d.n3e;
+  if (t >= n) return;
+  int ii = (int)(t % d.n1e);
+  long long r = t / d.n1e;
+  int gq = (int)(r % (2 * d.ng)), kk = (int)(r / (2 * d.ng));
+  int k = kk - d.ng3;
+  int ks = (d.n3 > 1) ? ((k + d.n3 / 2) % d.n3 + d.n3) % d.n3 + d.ng3 : kk;
+  int jj, js;
+  if (gq < d.ng) { jj = gq; js = 2 * d.ng - 1 - jj; }
+  else { jj = d.ng + d.n2 + (gq - d.ng); js = 2 * (d.ng + d.n2) - 1 - jj; }
+  flag[cidx(d, ii, jj, kk)] = flag[cidx(d, ii, js, ks)];
 }
 
 // ------------------------------------------------------------------ post_fixup
@@ -359,12 +533,24 @@ int hp_emf_to_flux_fp64(harm_ctx* c, const double* emf, double* F1, double* F2, 
 int hp_bound(harm_ctx* c, double* P, int8_t* flag) {
   Dims d = dims_of(c->g);
   Phys ph = phys_of(c->g);
-  k_bound_x1<<<nblk(2LL * d.ng * d.n2e * d.n3e), 256, 0, c->stream>>>(d, ph, P, flag, c->d_geom);
-  k_bound_x2<<<nblk(2LL * d.ng * d.n1e * d.n3e), 256, 0, c->stream>>>(d, P, flag);
-  c->launches += 2;
-  if (d.n3 > 1) {
-    k_bound_x3<<<nblk(2LL * d.ng3 * (long long)d.plane), 256, 0, c->stream>>>(d, P, flag);
-    c->launches++;
+  if (P) {
+    k_bound_x1_extrap<<<nblk(2LL * d.n2 * d.n3, 128), 128, 0, c->stream>>>(d, ph, P, c->d_geom);
+    k_bound_x2_reflect<<<nblk(2LL * d.n1e * d.n3, 128), 128, 0, c->stream>>>(d, P);
+    k_bound_x2_pole<<<nblk(2LL * d.n1e * d.n3, 128), 128, 0, c->stream>>>(d, ph, c->g.startx[2], P, c->d_geom, c->d_aux);
+    c->launches += 3;
+    if (d.n3 > 1) {
+      k_bound_x3<<<nblk(2LL * d.ng3 * (long long)d.plane), 256, 0, c->stream>>>(d, P, nullptr);
+      c->launches++;
+    }
+  }
+  if (flag) {
+    k_bound_flags_x1<<<nblk(2LL * d.ng * d.n2e * d.n3e), 256, 0, c->stream>>>(d, flag);
+    k_bound_flags_x2<<<nblk(2LL * d.ng * d.n1e * d.n3e), 256, 0, c->stream>>>(d, flag);
+    c->launches += 2;
+    if (d.n3 > 1) {
+      k_bound_x3<<<nblk(2LL * d.ng3 * (long long)d.plane), 256, 0, c->stream>>>(d, nullptr, flag);
+      c->launches++;
+    }
   }
   CK(cudaGetLastError());
   return 0;

@@ -29,7 +29,9 @@ static inline int sym_index(int m, int n) {
 
 int harm_grid_setup(harm_grid *g, int n1, int n2, int n3, int lim, double a,
                     double hslope, double Rout, double cour) {
-  if (!g || n1 < 2 || n2 < 2 || n3 < 1) return 1;
+  /* the radial boundary extrapolates from three cells, the polar one reads the second
+     cell from each pole while it rewrites the first */
+  if (!g || n1 < 3 || n2 < 4 || n3 < 1) return 1;
   if (lim != HARM_LIM_MC && lim != HARM_LIM_PARA && lim != HARM_LIM_WENO5 && lim != HARM_LIM_PARALINE) return 1;
   memset(g, 0, sizeof(*g));
   g->n1 = n1; g->n2 = n2; g->n3 = n3;

@@ -32,6 +32,15 @@ RK2_CUF = ((1.0, 0.0, 0.5, 0.0), (1.0, 0.0, 1.0, 0.0))   # setup_rktimestep step
 RK2_CUNEW = ((0.0, 0.0, 0.0, 0.0), (0.0, 0.0, 1.0, 0.5))
 
 
+def _torch_cuda():
+    """torch, when it is already imported and has CUDA; None otherwise"""
+    import sys
+    torch = sys.modules.get("torch")
+    if torch is None or not torch.cuda.is_available():
+        return None
+    return torch
+
+
 def _ptr(a) -> int:
     if a is None:
         return None
@@ -101,6 +110,7 @@ class Harm:
         self.grid = grid
         self.lib = N.device_lib()
         self._ctx = C.c_void_p()
+        self._ext = None
         if geom is None and conn is None and aux is None:
             rc = self.lib.harm_b200_create_grid(C.byref(grid.g), device, C.byref(self._ctx))
             self._check(rc, "harm_b200_create_grid")
@@ -116,7 +126,7 @@ class Harm:
         """the reference's main dump file of P (bounded ghost zones) at `path`: "text" (the
         reference's default), "binary" or "mixed" (harm_b200_dump)"""
         code = {"text": 0, "binary": 1, "mixed": 2}[fmt]
-        rc = self.lib.harm_b200_dump(self._ctx, _ptr(P), None if U is None else _ptr(U), float(t), float(dt), int(nstep),
+        rc = self._ordered(self.lib.harm_b200_dump, self._ctx, _ptr(P), None if U is None else _ptr(U), float(t), float(dt), int(nstep),
                                      code, path.encode())
         self._check(rc, "harm_b200_dump")
 
@@ -127,12 +137,28 @@ class Harm:
         geom = np.empty((4, 28, g.n2e, g.n1e), dtype=np.float64)
         conn = np.empty((64, g.n2e, g.n1e), dtype=np.float64)
         aux = np.empty((3, g.n2e, g.n1e), dtype=np.float64)
-        self._check(self.lib.harm_b200_get_tables(self._ctx, _ptr(geom), _ptr(conn), _ptr(aux)), "get_tables")
+        self._check(self._ordered(self.lib.harm_b200_get_tables, self._ctx, _ptr(geom), _ptr(conn), _ptr(aux)), "get_tables")
         return geom, conn, aux
 
     def _check(self, rc: int, what: str) -> None:
         if rc:
             raise RuntimeError(f"{what} failed ({rc}): {self.lib.harm_b200_last_error().decode()}")
+
+    def _ordered(self, fn, *args):
+        """Call a library entry point in stream order with torch: the context's stream first
+        waits for the work queued so far on torch's current stream (which may still be writing
+        the arguments), and torch's stream then waits for the context's (which may still be
+        writing the results).  The library enqueues on its own non-blocking stream."""
+        torch = _torch_cuda()
+        if torch is None:
+            return fn(*args)
+        if self._ext is None:
+            self._ext = torch.cuda.ExternalStream(self.stream_ptr)
+        cur = torch.cuda.current_stream()
+        self._ext.wait_stream(cur)
+        rc = fn(*args)
+        cur.wait_stream(self._ext)
+        return rc
 
     def close(self) -> None:
         if self._ctx:
@@ -155,11 +181,11 @@ class Harm:
 
     # ---------------------------------------------------------------- reference API
     def bound_prim(self, P) -> None:
-        self._check(self.lib.harm_b200_bound(self._ctx, _ptr(P)), "bound_prim")
+        self._check(self._ordered(self.lib.harm_b200_bound, self._ctx, _ptr(P)), "bound_prim")
 
     def fluxcalc(self, pb, F1, F2, F3, precision: int = N.HARM_PREC_FP64):
         ndt = (C.c_double * 3)()
-        self._check(self.lib.harm_b200_fluxcalc(self._ctx, precision, _ptr(pb), _ptr(F1), _ptr(F2), _ptr(F3), ndt),
+        self._check(self._ordered(self.lib.harm_b200_fluxcalc, self._ctx, precision, _ptr(pb), _ptr(F1), _ptr(F2), _ptr(F3), ndt),
                     "fluxcalc")
         return tuple(ndt)
 
@@ -170,19 +196,19 @@ class Harm:
         Cun = (C.c_double * 4)(*(RK2_CUNEW[timeorder] if Cunew is None else Cunew))
         ndt = C.c_double()
         st = N.harm_stats()
-        self._check(self.lib.harm_b200_advance(self._ctx, precision, guess, timeorder, numtimeorders, _ptr(pi), _ptr(pb),
+        self._check(self._ordered(self.lib.harm_b200_advance, self._ctx, precision, guess, timeorder, numtimeorders, _ptr(pi), _ptr(pb),
                                                _ptr(pf), _ptr(pflag), dt, CUf, Cun, C.byref(ndt), C.byref(st)),
                     "advance")
         return ndt.value, st.as_dict()
 
     def post_fixup(self, pf, pflag) -> None:
-        self._check(self.lib.harm_b200_post_fixup(self._ctx, _ptr(pf), _ptr(pflag)), "post_fixup")
+        self._check(self._ordered(self.lib.harm_b200_post_fixup, self._ctx, _ptr(pf), _ptr(pflag)), "post_fixup")
 
     def step_ch(self, P, dt: float, precision: int = N.HARM_PREC_FP64, guess: int = N.HARM_GUESS_PREV,
                 nsteps: int = 1, stats: bool = True):
         d = C.c_double(dt)
         st = N.harm_stats()
-        self._check(self.lib.harm_b200_step_n(self._ctx, precision, guess, _ptr(P), nsteps, C.byref(d),
+        self._check(self._ordered(self.lib.harm_b200_step_n, self._ctx, precision, guess, _ptr(P), nsteps, C.byref(d),
                                               C.byref(st) if stats else None), "step_ch")
         return d.value, st.as_dict()
 
@@ -190,19 +216,19 @@ class Harm:
                      guess: int = N.HARM_GUESS_PREV):
         d = C.c_double(dt)
         st = N.harm_stats()
-        self._check(self.lib.harm_b200_step_host(self._ctx, precision, guess, _ptr(P_host), C.byref(d), C.byref(st)),
+        self._check(self._ordered(self.lib.harm_b200_step_host, self._ctx, precision, guess, _ptr(P_host), C.byref(d), C.byref(st)),
                     "step_ch_host")
         return d.value, st.as_dict()
 
     def Utoprimgen(self, U, geomrec, P, pflag, iters=None, guess: int = N.HARM_GUESS_PREV) -> None:
         n = U.shape[-1]
-        self._check(self.lib.harm_b200_utoprimgen_points(self._ctx, n, guess, _ptr(U), _ptr(geomrec), _ptr(P),
+        self._check(self._ordered(self.lib.harm_b200_utoprimgen_points, self._ctx, n, guess, _ptr(U), _ptr(geomrec), _ptr(P),
                                                          _ptr(pflag), _ptr(iters)), "Utoprimgen")
 
     def time_stages(self, P, dt: float, precision: int = N.HARM_PREC_FP64, guess: int = N.HARM_GUESS_PREV,
                     reps: int = 5) -> dict:
         ms = (C.c_double * 5)()
-        self._check(self.lib.harm_b200_time_stages(self._ctx, precision, guess, _ptr(P), dt, reps, ms), "time_stages")
+        self._check(self._ordered(self.lib.harm_b200_time_stages, self._ctx, precision, guess, _ptr(P), dt, reps, ms), "time_stages")
         return dict(zip(("flux", "emf", "update_invert", "bound", "post_fixup"), list(ms)))
 
     # ---------------------------------------------------------------- learned guess
@@ -210,25 +236,25 @@ class Harm:
         """Training pairs from the most recent inversion of this context (its U and the
         primitives P it produced); returns the number written (at most len(feat))."""
         n = C.c_size_t()
-        self._check(self.lib.harm_b200_mlp_dump(self._ctx, _ptr(P), stride, phase, feat.shape[0], _ptr(feat),
+        self._check(self._ordered(self.lib.harm_b200_mlp_dump, self._ctx, _ptr(P), stride, phase, feat.shape[0], _ptr(feat),
                                                 _ptr(targ), _ptr(cell), C.byref(n)), "mlp_dump")
         return int(n.value)
 
     def mlp_synth(self, feat, targ, seed: int, U=None, P=None, cell=None) -> None:
-        self._check(self.lib.harm_b200_mlp_synth(self._ctx, feat.shape[0], seed, _ptr(feat), _ptr(targ), _ptr(U),
+        self._check(self._ordered(self.lib.harm_b200_mlp_synth, self._ctx, feat.shape[0], seed, _ptr(feat), _ptr(targ), _ptr(U),
                                                  _ptr(P), _ptr(cell)), "mlp_synth")
 
     def mlp_norm(self, feat, targ, norm, n: int | None = None) -> None:
         n = feat.shape[0] if n is None else n
-        self._check(self.lib.harm_b200_mlp_norm(self._ctx, n, _ptr(feat), _ptr(targ), _ptr(norm)), "mlp_norm")
+        self._check(self._ordered(self.lib.harm_b200_mlp_norm, self._ctx, n, _ptr(feat), _ptr(targ), _ptr(norm)), "mlp_norm")
 
     def mlp_init(self, params, seed: int = 1) -> None:
-        self._check(self.lib.harm_b200_mlp_init(self._ctx, seed, _ptr(params)), "mlp_init")
+        self._check(self._ordered(self.lib.harm_b200_mlp_init, self._ctx, seed, _ptr(params)), "mlp_init")
 
     def mlp_loss_grad(self, feat, targ, params, norm, grad, n: int | None = None) -> float:
         n = feat.shape[0] if n is None else n
         loss = C.c_double()
-        self._check(self.lib.harm_b200_mlp_loss_grad(self._ctx, n, _ptr(feat), _ptr(targ), _ptr(params), _ptr(norm),
+        self._check(self._ordered(self.lib.harm_b200_mlp_loss_grad, self._ctx, n, _ptr(feat), _ptr(targ), _ptr(params), _ptr(norm),
                                                      C.byref(loss), _ptr(grad)), "mlp_loss_grad")
         return loss.value
 
@@ -236,13 +262,13 @@ class Harm:
                   n: int | None = None) -> np.ndarray:
         n = feat.shape[0] if n is None else n
         hist = np.zeros(steps, dtype=np.float32)
-        self._check(self.lib.harm_b200_mlp_train(self._ctx, n, _ptr(feat), _ptr(targ), _ptr(norm), _ptr(params), steps,
+        self._check(self._ordered(self.lib.harm_b200_mlp_train, self._ctx, n, _ptr(feat), _ptr(targ), _ptr(norm), _ptr(params), steps,
                                                  batch, lr, seed, _ptr(hist)), "mlp_train")
         return hist
 
     def mlp_set(self, params, norm, start_bias: float = 0.0) -> None:
-        self._check(self.lib.harm_b200_mlp_set(self._ctx, _ptr(params), _ptr(norm), start_bias), "mlp_set")
+        self._check(self._ordered(self.lib.harm_b200_mlp_set, self._ctx, _ptr(params), _ptr(norm), start_bias), "mlp_set")
 
     def mlp_predict(self, feat, out, n: int | None = None) -> None:
         n = feat.shape[0] if n is None else n
-        self._check(self.lib.harm_b200_mlp_predict(self._ctx, n, _ptr(feat), _ptr(out)), "mlp_predict")
+        self._check(self._ordered(self.lib.harm_b200_mlp_predict, self._ctx, n, _ptr(feat), _ptr(out)), "mlp_predict")

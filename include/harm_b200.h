@@ -25,6 +25,12 @@
  *     so metric tables are stored per (i,j) only: geom[loc][field][j][i] over n2e x n1e.
  *     FACE3 shares CENT, CORN1 shares FACE2, CORN2 shares FACE1 (HARM stores all eight
  *     locations per (i,j,k): superdefs.h:382).
+ *   - Streams: a context enqueues its work on its own non-blocking CUDA stream
+ *     (harm_b200_stream).  Calls that return host values (ndt, dt, stats, losses) synchronise
+ *     that stream before returning; the others (bound, post_fixup, Utoprimgen over points,
+ *     the mlp_* kernels) return once their work is queued.  A caller that writes the
+ *     arguments or reads the results on another stream orders that stream against the
+ *     context's (events, or a synchronisation).
  *   - Return value: 0 on success, >0 on error (HARM's MYFUN convention,
  *     global.variousmacros.h:43).  Per-cell inversion failures are not return codes;
  *     they are written to an int8 pflag array with HARM's codes

@@ -44,6 +44,7 @@ void orc_vchar_point(const harm_grid *g, const double *geomrec, const double *pr
 
 /* grid routines */
 int orc_bound(orc *o, double *P);
+int orc_bound_dir(orc *o, double *P, int dir, int simple);
 int orc_fluxcalc(orc *o, const double *pb, double *F1, double *F2, double *F3, double ndt[3]);
 int orc_advance(orc *o, int timeorder, int numtimeorders, const double *pi, const double *pb,
                 double *pf, int8_t *pflag, double dt, const double CUf[4],

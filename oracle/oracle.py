@@ -55,6 +55,7 @@ def lib() -> C.CDLL:
             "orc_utoprimgen_point": (I, [C.POINTER(N.harm_grid), P, P, P, P, P]),
             "orc_vchar_point": (None, [C.POINTER(N.harm_grid), P, P, I, C.POINTER(D), C.POINTER(D)]),
             "orc_bound": (I, [C.POINTER(orc), P]),
+            "orc_bound_dir": (I, [C.POINTER(orc), P, I, I]),
             "orc_fluxcalc": (I, [C.POINTER(orc), P, P, P, P, P]),
             "orc_advance": (I, [C.POINTER(orc), I, I, P, P, P, P, D, P, P, C.POINTER(D), C.POINTER(N.harm_stats)]),
             "orc_post_fixup": (I, [C.POINTER(orc), P, P]),
@@ -93,6 +94,10 @@ class Oracle:
 
     def bound_prim(self, P):
         lib().orc_bound(C.byref(self.o), _p(P))
+
+    def bound_dir(self, P, d, simple=False):
+        """one direction of bound_prim; simple: one ghost layer (BOUNDPRIMSIMPLETYPE)"""
+        lib().orc_bound_dir(C.byref(self.o), _p(P), int(d), int(bool(simple)))
 
     def fluxcalc(self, pb, F1, F2, F3):
         ndt = (C.c_double * 3)()

@@ -2,8 +2,7 @@
  * orc_advance.c -- TEST INFRASTRUCTURE ONLY (CPU oracle; see harm_oracle.h).
  *
  * advance_standard (advance.c:140) for one RK substep, post_fixup/fixup_utoprim
- * (fixup.c:53, :1061, general_average :1830), the boundary conditions of the torus
- * problem (bound_prim, bounds.fishmon.c, bounds.tools.c) and the full RK2 step
+ * (fixup.c:53, :1061, general_average :1830) with the flags' ghost zones, and the full RK2 step
  * (step_ch_simplempi step_ch.c:524, setup_rktimestep :1244-1266, post_stepch :150).
  */
 #include <math.h>
@@ -23,87 +22,34 @@ void orc_init(orc *o, const harm_grid *g, const double *geom, const double *conn
   o->nthreads = nthreads > 0 ? nthreads : 1;
 }
 
-/* Ghost zones: x1 inner FREEOUTFLOW copy, x1 outer OUTFLOW copy with the inflow check
-   and limit_gamma (bound_x1up_outflow bounds.tools.c), x2 POLARAXIS reflection with U2,B2
-   sign flips (bound_x2dn_polaraxis bounds.tools.c:751; with n3>1 the source column is
-   the one across the pole, phi+pi, as in the full-3D polar transfer :618), x3 periodic.
-   Applied in the order x1, x2, x3 over the full transverse extent. */
-static void bound_generic(orc *o, double *P, int8_t *flag) {
+/* Ghost-zone flags for post_fixup's neighbour test (bound_pflag step_ch.c:1637): x1 copies of
+   the nearest active cell, x2 reflection across the pole (with n3>1 from the column across the
+   pole, phi+pi), x3 periodic; applied in the order x1, x2, x3 over the full transverse extent. */
+static void bound_flags(orc *o, int8_t *flag) {
   const harm_grid *g = &o->g;
   const int n1e = g->n1e, n2e = g->n2e, n3e = g->n3e, ng = g->ng, ng3 = g->ng3;
-  const size_t cells = o->cells;
-#pragma omp parallel for collapse(2) num_threads(o->nthreads)
   for (int kk = 0; kk < n3e; kk++)
     for (int jj = 0; jj < n2e; jj++) {
-      for (int ii = 0; ii < ng; ii++) {
-        size_t d = oidx(o, ii, jj, kk), s = oidx(o, ng, jj, kk);
-        if (P) for (int p = 0; p < HARM_NPR; p++) P[p * cells + d] = P[p * cells + s];
-        if (flag) flag[d] = flag[s];
-      }
-      for (int ii = ng + g->n1; ii < n1e; ii++) {
-        size_t d = oidx(o, ii, jj, kk), s = oidx(o, ng + g->n1 - 1, jj, kk);
-        if (flag) flag[d] = flag[s];
-        if (!P) continue;
-        double pr[HARM_NPR];
-        for (int p = 0; p < HARM_NPR; p++) pr[p] = P[p * cells + s];
-        ogeom gc;
-        og_load(o, HARM_LOC_CENT, ii, jj, &gc);
-        o_inflow_check_x1up(pr, &gc, g->gammamax);
-        o_limit_gamma(g->gammamax, pr, &gc);
-        for (int p = 0; p < HARM_NPR; p++) P[p * cells + d] = pr[p];
-      }
+      for (int ii = 0; ii < ng; ii++) flag[oidx(o, ii, jj, kk)] = flag[oidx(o, ng, jj, kk)];
+      for (int ii = ng + g->n1; ii < n1e; ii++) flag[oidx(o, ii, jj, kk)] = flag[oidx(o, ng + g->n1 - 1, jj, kk)];
     }
   const int n3 = g->n3;
-#pragma omp parallel for collapse(2) num_threads(o->nthreads)
   for (int kk = 0; kk < n3e; kk++)
     for (int ii = 0; ii < n1e; ii++) {
       int k = kk - ng3;
       int ks = (n3 > 1) ? ((k + n3 / 2) % n3 + n3) % n3 + ng3 : kk;
-      for (int jj = 0; jj < ng; jj++) {
-        int js = 2 * ng - 1 - jj;
-        size_t d = oidx(o, ii, jj, kk), s = oidx(o, ii, js, ks);
-        if (flag) flag[d] = flag[s];
-        if (!P) continue;
-        for (int p = 0; p < HARM_NPR; p++) {
-          double v = P[p * cells + s];
-          if (p == HARM_U2 || p == HARM_B2) v = -v;
-          P[p * cells + d] = v;
-        }
-      }
-      for (int jj = ng + g->n2; jj < n2e; jj++) {
-        int js = 2 * (ng + g->n2) - 1 - jj;
-        size_t d = oidx(o, ii, jj, kk), s = oidx(o, ii, js, ks);
-        if (flag) flag[d] = flag[s];
-        if (!P) continue;
-        for (int p = 0; p < HARM_NPR; p++) {
-          double v = P[p * cells + s];
-          if (p == HARM_U2 || p == HARM_B2) v = -v;
-          P[p * cells + d] = v;
-        }
-      }
+      for (int jj = 0; jj < ng; jj++) flag[oidx(o, ii, jj, kk)] = flag[oidx(o, ii, 2 * ng - 1 - jj, ks)];
+      for (int jj = ng + g->n2; jj < n2e; jj++)
+        flag[oidx(o, ii, jj, kk)] = flag[oidx(o, ii, 2 * (ng + g->n2) - 1 - jj, ks)];
     }
-  if (n3 > 1) {
-#pragma omp parallel for collapse(2) num_threads(o->nthreads)
+  if (n3 > 1)
     for (int jj = 0; jj < n2e; jj++)
       for (int ii = 0; ii < n1e; ii++) {
-        for (int kk = 0; kk < ng3; kk++) {
-          size_t d = oidx(o, ii, jj, kk), s = oidx(o, ii, jj, kk + n3);
-          if (P) for (int p = 0; p < HARM_NPR; p++) P[p * cells + d] = P[p * cells + s];
-          if (flag) flag[d] = flag[s];
-        }
-        for (int kk = ng3 + n3; kk < n3e; kk++) {
-          size_t d = oidx(o, ii, jj, kk), s = oidx(o, ii, jj, kk - n3);
-          if (P) for (int p = 0; p < HARM_NPR; p++) P[p * cells + d] = P[p * cells + s];
-          if (flag) flag[d] = flag[s];
-        }
+        for (int kk = 0; kk < ng3; kk++) flag[oidx(o, ii, jj, kk)] = flag[oidx(o, ii, jj, kk + n3)];
+        for (int kk = ng3 + n3; kk < n3e; kk++) flag[oidx(o, ii, jj, kk)] = flag[oidx(o, ii, jj, kk - n3)];
       }
-  }
 }
 
-int orc_bound(orc *o, double *P) {
-  bound_generic(o, P, NULL);
-  return 0;
-}
 
 int orc_advance(orc *o, int timeorder, int numtimeorders, const double *pi, const double *pb,
                 double *pf, int8_t *pflag, double dt, const double CUf[4],
@@ -196,7 +142,7 @@ int orc_advance(orc *o, int timeorder, int numtimeorders, const double *pi, cons
 int orc_post_fixup(orc *o, double *pf, int8_t *pflag) {
   const harm_grid *g = &o->g;
   const size_t cells = o->cells;
-  bound_generic(o, NULL, pflag);
+  bound_flags(o, pflag);
   double *ptoavg = (double *)malloc(HARM_NPR * cells * sizeof(double));
   int8_t *forig = (int8_t *)malloc(cells);
   memcpy(ptoavg, pf, HARM_NPR * cells * sizeof(double));

@@ -170,6 +170,17 @@ class RefRun:
             return np.ascontiguousarray(a.astype(np.int8))
         return a
 
+    def bound_calls(self, step: int):
+        """The boundary calls of step `step` in call order: (direction, one_layer, input, output)
+        with input/output as [8][n3e][n2e][n1e]; one_layer marks BOUNDPRIMSIMPLETYPE calls."""
+        out, n = [], 0
+        while os.path.exists(os.path.join(self.path, f"bnd_{step}_{n}_info.npy")):
+            info = np.load(os.path.join(self.path, f"bnd_{step}_{n}_info.npy"))
+            ld = lambda w: np.ascontiguousarray(np.moveaxis(np.load(os.path.join(self.path, f"bnd_{step}_{n}_{w}.npy")), 3, 0))
+            out.append((int(info[0]), int(info[1]) != int(info[3]), ld("in"), ld("out")))
+            n += 1
+        return out
+
     def dt_of_step(self, step: int) -> float:
         """dt the reference used for step `step` (1-based)"""
         return float(self.steps[step, 1])

@@ -17,8 +17,8 @@
 #      global.defnprs.h with the reference's own generatenprs.c;
 #   5. compiles every source of the reference's GRMHD object lists except main.c, plus
 #      oracle/ref/driver.c, with gcc -O3 -fopenmp -fcommon, and links them with the calls of
-#      advance(), fluxcalc(), post_fixup() and bound_prim_user_dir() routed through the
-#      driver's recording
+#      advance(), fluxcalc(), post_fixup(), bound_prim_user_dir() and flux_compute_general()
+#      routed through the driver's recording
 #      wrappers (ld --wrap), which call the reference's own functions.
 # gcc on x86-64 without -march emits no fused multiply-add, so the arithmetic is the
 # IEEE operations of the source in its order.
@@ -113,7 +113,7 @@ build_one() {
     printf '%s\n' $srcs href_driver.c | xargs -P "$JOBS" -I{} sh -c \
       'gcc '"$CFLAGS"' -c {} -o "$(basename {} .c).o" || { echo "ref_build: compiling {} failed" >&2; exit 255; }'
     objs=$(printf '%s\n' $srcs href_driver.c | sed 's/\.c$/.o/')
-    gcc -fopenmp -mcmodel=medium -no-pie -Wl,--wrap=advance,--wrap=fluxcalc,--wrap=post_fixup,--wrap=bound_prim_user_dir \
+    gcc -fopenmp -mcmodel=medium -no-pie -Wl,--wrap=advance,--wrap=fluxcalc,--wrap=post_fixup,--wrap=bound_prim_user_dir,--wrap=flux_compute_general \
         -o "$bin.tmp" $objs -lm
     mv "$bin.tmp" "$bin"
   )

@@ -13,7 +13,8 @@
  * R0 0, Rout 40; Toth flux-CT; rescaletype 0 floors 1e-6 r^-1.5 / 1e-8 r^-2.5; Courant 0.8;
  * fixed seed of the internal-energy perturbation; no diagnostics), with the reconstruction,
  * flux formula, time order and Courant factor taken from the environment:
- *   HREF_LIM        mc | para | paraline | weno5        (lim[1..3], default mc)
+ *   HREF_LIM        mc | para | paraline | weno5 | weno5bnd   (lim[1..3], default mc;
+ *                   weno5 is lim WENO5, weno5bnd lim WENO5BND)
  *   HREF_FLUX       hll | laxf                          (fluxmethod, default hll)
  *   HREF_TIMEORDER  1 | 2                               (TIMEORDER, default 2)
  *   HREF_COUR       Courant factor                      (default 0.8)
@@ -88,7 +89,8 @@ int init_global(void)
   int limv = MC;
   if (!strcmp(lim_s, "para")) limv = PARA;
   else if (!strcmp(lim_s, "paraline")) limv = PARALINE;
-  else if (!strcmp(lim_s, "weno5")) limv = WENO5BND;
+  else if (!strcmp(lim_s, "weno5")) limv = WENO5;
+  else if (!strcmp(lim_s, "weno5bnd")) limv = WENO5BND;
   for (dir = 1; dir <= 3; dir++) lim[dir] = limv;
   fluxmethod = strcmp(env_or("HREF_FLUX", "hll"), "laxf") ? HLLFLUX : LAXFFLUX;
   FLUXB = FLUXCTTOTH;
@@ -263,6 +265,7 @@ static void dump_grid(const char *dir)
 static const char *sub_dir = NULL;
 static int sub_active = 0;
 static char sub_prefix[64];
+static char adv_prefix[64]; /* sub_<step>_<timeorder> of the latest recorded advance() */
 
 static int step_wanted(long step)
 {
@@ -340,7 +343,8 @@ int __wrap_advance(int stage, FTYPE (*pi)[NSTORE2][NSTORE3][NPR], FTYPE (*pb)[NS
   if (want) {
     double v[14];
     int m;
-    snprintf(sub_prefix, sizeof sub_prefix, "sub_%ld_%d", nstep + 1, timeorder);
+    snprintf(adv_prefix, sizeof adv_prefix, "sub_%ld_%d", nstep + 1, timeorder);
+    snprintf(sub_prefix, sizeof sub_prefix, "%s", adv_prefix);
     dump_ext("pi", pi);
     dump_ext("pb", pb);
     v[0] = dt; v[1] = fluxdt; v[2] = timeorder; v[3] = numtimeorders;
@@ -354,6 +358,7 @@ int __wrap_advance(int stage, FTYPE (*pi)[NSTORE2][NSTORE3][NPR], FTYPE (*pb)[NS
   if (want) {
     double v[1];
     sub_active = 0;
+    snprintf(sub_prefix, sizeof sub_prefix, "%s", adv_prefix);
     dump_ext("pf", pf);
     dump_flags("pflag");
     v[0] = *ndt;
@@ -401,11 +406,15 @@ int __wrap_post_fixup(int stageit, SFTYPE boundtime, FTYPE (*pv)[NSTORE2][NSTORE
 {
   int r, want = step_wanted(nstep + 1);
   if (want) {
+    snprintf(sub_prefix, sizeof sub_prefix, "%s", adv_prefix);
     dump_ext("fixin", pv);
     dump_flags("fixflag");
   }
   r = __real_post_fixup(stageit, boundtime, pv, pbackup, ucons, finalstep);
-  if (want) dump_ext("fixout", pv);
+  if (want) {
+    snprintf(sub_prefix, sizeof sub_prefix, "%s", adv_prefix);
+    dump_ext("fixout", pv);
+  }
   return r;
 }
 
@@ -433,6 +442,33 @@ int __wrap_bound_prim_user_dir(int boundstage, SFTYPE boundtime, int whichdir, i
     snprintf(sub_prefix, sizeof sub_prefix, "bnd_%ld_%d", nstep + 1, bnd_calls);
     dump_ext("out", prim);
     bnd_calls++;
+  }
+  return r;
+}
+
+/* HREF_PROBE="i,j,k,dir": print the face states and flux of that face at every flux
+   computation (flux_compute_general fluxcompute.c:19, called from fluxcalc_standard) */
+int __real_flux_compute_general(int i, int j, int k, int dir, struct of_geom *ptrgeom, FTYPE CUf, FTYPE *p_c,
+                                FTYPE *p_l, FTYPE *p_r, FTYPE *F, FTYPE *ctopptr);
+
+int __wrap_flux_compute_general(int i, int j, int k, int dir, struct of_geom *ptrgeom, FTYPE CUf, FTYPE *p_c,
+                                FTYPE *p_l, FTYPE *p_r, FTYPE *F, FTYPE *ctopptr)
+{
+  static int pi = -9999, pj, pk, pd;
+  int r, pl;
+  if (pi == -9999) {
+    const char *s = getenv("HREF_PROBE");
+    if (!s || sscanf(s, "%d,%d,%d,%d", &pi, &pj, &pk, &pd) != 4) pi = -9998;
+  }
+  r = __real_flux_compute_general(i, j, k, dir, ptrgeom, CUf, p_c, p_l, p_r, F, ctopptr);
+  if (i == pi && j == pj && k == pk && dir == pd) {
+    fprintf(stderr, "PROBE nstep=%ld face %d %d %d dir %d\n  p_l", nstep, i, j, k, dir);
+    for (pl = 0; pl < NPR; pl++) fprintf(stderr, " %.17g", p_l[pl]);
+    fprintf(stderr, "\n  p_r");
+    for (pl = 0; pl < NPR; pl++) fprintf(stderr, " %.17g", p_r[pl]);
+    fprintf(stderr, "\n  F  ");
+    for (pl = 0; pl < NPR; pl++) fprintf(stderr, " %.17g", F[pl]);
+    fprintf(stderr, "\n  ctop %.17g\n", *ctopptr);
   }
   return r;
 }

@@ -50,7 +50,9 @@ def per_field_close(a, b, rtol, floor_frac=1e-10):
 
 
 def divb_corner(grid, geom, P):
-    """Toth corner divergence of sqrt(-g) B (the quantity flux-CT preserves), active corners."""
+    """Toth corner divergence of sqrt(-g) B (the quantity flux-CT preserves) at the corners whose
+    cells are all active in x1 and x2 (the corners on the radial and polar boundaries also see
+    ghost cells, which the boundary conditions set, not flux-CT); x3 is periodic."""
     g = grid.g
     gd = geom[0, 26]  # CENT gdet [j][i]
     U = P[5:8] * gd[None, None, :, :]
@@ -59,13 +61,13 @@ def divb_corner(grid, geom, P):
     if g.n3 == 1:
         k = 0
         u1, u2 = U[0, k], U[1, k]
-        j0, j1, i0, i1 = ng, ng + g.n2 + 1, ng, ng + g.n1 + 1
+        j0, j1, i0, i1 = ng + 1, ng + g.n2, ng + 1, ng + g.n1
         J, I = np.mgrid[j0:j1, i0:i1]
         d1 = 0.5 * (u1[J, I] + u1[J - 1, I] - u1[J, I - 1] - u1[J - 1, I - 1]) / dx1
         d2 = 0.5 * (u2[J, I] + u2[J, I - 1] - u2[J - 1, I] - u2[J - 1, I - 1]) / dx2
         return np.abs(d1 + d2)
     u1, u2, u3 = U[0], U[1], U[2]
-    K, J, I = np.mgrid[ng3:ng3 + g.n3 + 1, ng:ng + g.n2 + 1, ng:ng + g.n1 + 1]
+    K, J, I = np.mgrid[ng3:ng3 + g.n3 + 1, ng + 1:ng + g.n2, ng + 1:ng + g.n1]
     d1 = 0.25 * (u1[K, J, I] + u1[K, J - 1, I] + u1[K - 1, J, I] + u1[K - 1, J - 1, I]
                  - u1[K, J, I - 1] - u1[K, J - 1, I - 1] - u1[K - 1, J, I - 1] - u1[K - 1, J - 1, I - 1]) / dx1
     d2 = 0.25 * (u2[K, J, I] + u2[K, J, I - 1] + u2[K - 1, J, I] + u2[K - 1, J, I - 1]

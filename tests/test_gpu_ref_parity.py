@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from harm_harm_b200 import Grid, Harm
-from test_ref_pins import GOLDEN, LIVE, PHYSICAL_AND_FAILING, active_faces, live, rel
+from test_ref_pins import GOLDEN, LIVE, PHYSICAL_AND_FAILING, active_faces, live, live_substeps, rel
 
 pytestmark = pytest.mark.gpu
 
@@ -88,28 +88,87 @@ def test_live_substeps_device(cuda, name):
     act = (slice(None),) + g.active
     nd = 3 if g.g.n3 > 1 else 2
     try:
-        for step in (1, 2):
-            for to in (0, 1):
-                pb = dev(cuda, rr.sub(step, to, "pb"))
-                F = [cuda.zeros_like(pb) for _ in range(3)]
-                ndt = h.fluxcalc(pb, *F)
-                for dd in range(1, nd + 1):
-                    Fr = rr.sub(step, to, f"F{dd}")
-                    sl = active_faces(g, dd)
-                    a = F[dd - 1].cpu().numpy()[sl]
-                    for pl in range(8):
-                        assert err(a[pl], Fr[sl][pl]) < tol, (step, to, dd, pl)
-                    assert abs(ndt[dd - 1] - rr.sub(step, to, "ndtdir")[dd - 1]) <= max(tol, 1e-13) * ndt[dd - 1]
-                args = rr.sub(step, to, "args")
-                pf = pb.clone()
-                flag = cuda.zeros(pb.shape[1:], dtype=cuda.int8, device="cuda")
-                ndt1, _ = h.advance(to, dev(cuda, rr.sub(step, to, "pi")), pb, pf, flag, float(args[0]),
-                                    CUf=args[4:8], Cunew=args[8:12])
-                pfr = rr.sub(step, to, "pf")
-                a = pf.cpu().numpy()[act]
+        for step, to in live_substeps(name):
+            pb = dev(cuda, rr.sub(step, to, "pb"))
+            F = [cuda.zeros_like(pb) for _ in range(3)]
+            ndt = h.fluxcalc(pb, *F)
+            for dd in range(1, nd + 1):
+                Fr = rr.sub(step, to, f"F{dd}")
+                sl = active_faces(g, dd)
+                a = F[dd - 1].cpu().numpy()[sl]
                 for pl in range(8):
-                    assert err(a[pl], pfr[act][pl]) < tol, (step, to, "pf", pl)
-                assert (flag.cpu().numpy()[g.active] == rr.sub(step, to, "pflag")[g.active]).all()
-                assert abs(ndt1 - rr.sub(step, to, "ndt")[0]) <= max(tol, 1e-13) * ndt1
+                    assert err(a[pl], Fr[sl][pl]) < tol, (step, to, dd, pl)
+                assert abs(ndt[dd - 1] - rr.sub(step, to, "ndtdir")[dd - 1]) <= max(tol, 1e-13) * ndt[dd - 1]
+            args = rr.sub(step, to, "args")
+            pf = pb.clone()
+            flag = cuda.zeros(pb.shape[1:], dtype=cuda.int8, device="cuda")
+            ndt1, _ = h.advance(to, dev(cuda, rr.sub(step, to, "pi")), pb, pf, flag, float(args[0]),
+                                CUf=args[4:8], Cunew=args[8:12])
+            pfr = rr.sub(step, to, "pf")
+            a = pf.cpu().numpy()[act]
+            for pl in range(8):
+                assert err(a[pl], pfr[act][pl]) < tol, (step, to, "pf", pl)
+            assert (flag.cpu().numpy()[g.active] == rr.sub(step, to, "pflag")[g.active]).all()
+            assert abs(ndt1 - rr.sub(step, to, "ndt")[0]) <= max(tol, 1e-13) * ndt1
+    finally:
+        h.close()
+
+
+@pytest.mark.parametrize("name", ["2d_32x32", "3d_32x24x8"])
+def test_live_bound_device(cuda, name):
+    """the device's bound_prim (x1, x2, x3) against the reference's full bound of both
+    substeps: input of its x1 call, output of its x3 call"""
+    from test_ref_pins import BOUND
+    from oracle import ref as R
+    n1, n2, n3, ng, lim, tol = BOUND[name]
+    if not R.available(n1, n2, n3, ng):
+        pytest.skip("reference binary not built")
+    g = Grid.torus(n1, n2, n3, lim=lim)
+    rr = R.RefRun(R.run(n1, n2, n3, ng, lim=lim, nsteps=1, every=1, substeps=(1,)), g)
+    calls = rr.bound_calls(1)
+    h = Harm(g, rr.geom, rr.conn, rr.aux)
+    try:
+        for first in (3, 9):  # the full bounds after post_fixup, substeps 0 and 1
+            assert [c[0] for c in calls[first:first + 3]] == [1, 2, 3] and not calls[first][1]
+            P = dev(cuda, calls[first][2])
+            h.bound_prim(P)
+            out = calls[first + 2][3]
+            err = np.abs(P.cpu().numpy() - out) / np.maximum(np.abs(out), 1e-300)
+            # exp/log of the radial extrapolation: CUDA's and glibc's may differ in the last ulp
+            assert float(err.max()) <= max(tol, 1e-13), (first, float(err.max()))
+    finally:
+        h.close()
+
+
+@pytest.mark.parametrize("name", ["c0_2d_mc_128x128_100steps", "2d_mc_64x64_10steps", "3d_mc_32x24x8_4steps"])
+def test_live_full_steps_device(cuda, name):
+    """full device RK2 steps (harm_b200_step_n, one step per call) from the reference's initial
+    torus against the reference's states, dt and Newton iteration counts"""
+    from test_ref_pins import STEPS, normwise
+    from oracle import ref as R
+    n1, n2, n3, ng, lim, flux, nsteps, tol = STEPS[name]
+    if not R.available(n1, n2, n3, ng):
+        pytest.skip("reference binary not built")
+    every = max(1, nsteps // 4)
+    g = Grid.torus(n1, n2, n3, lim=lim, fluxmethod=flux)
+    rr = R.RefRun(R.run(n1, n2, n3, ng, lim=lim, flux=flux, nsteps=nsteps, every=every), g)
+    h = Harm(g, rr.geom, rr.conn, rr.aux)
+    act = (slice(None),) + g.active
+    try:
+        P = dev(cuda, rr.state(0))
+        h.bound_prim(P)
+        dt = rr.dt0
+        for s in range(1, nsteps + 1):
+            assert abs(dt - rr.dt_of_step(s)) <= max(tol, 1e-15) * dt, (s, dt, rr.dt_of_step(s))
+            dt, st = h.step_ch(P, dt)
+            if n3 == 1:
+                # the device's exp, log and pow may differ from glibc's in the last bit, so a
+                # cell's stopping test can flip by one iteration earlier than the oracle's
+                assert abs(st["newton_iters"] - rr.steps[s, 2]) <= 1e-4 * rr.steps[s, 2], s
+            if s % every == 0 or s == nsteps:
+                a = P.cpu().numpy()[act]
+                b = rr.state(s)[act]
+                for pl in range(8):
+                    assert normwise(a[pl], b[pl]) < tol, (s, pl, normwise(a[pl], b[pl]))
     finally:
         h.close()

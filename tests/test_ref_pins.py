@@ -113,12 +113,26 @@ def test_golden_utoprimgen(kind):
 
 LIVE = {  # name: (n1, n2, n3, ng, lim, flux, tolerance, measure)
     "2d_mc_64x64": (64, 64, 1, 4, 0, 0, 1e-12, "rel"),
+    "2d_paraline_laxf_64x64": (64, 64, 1, 4, 3, 1, 1e-12, "rel"),
     # the reference stores its metric per (i,j,k), and its numerically differentiated
     # Jacobian varies with x3 by ~1e-11 of each component; the oracle uses k=0's tables on
     # every plane, so 3-D fluxes agree to ~1e-10 of each field's largest face value
     "3d_mc_32x24x8": (32, 24, 8, 4, 0, 0, 2e-10, "norm"),
     "3d_para_32x24x8": (32, 24, 8, 4, 1, 0, 2e-10, "norm"),
+    "3d_paraline_32x24x8": (32, 24, 8, 4, 3, 0, 2e-10, "norm"),
+    "3d_paraline_laxf_32x24x8": (32, 24, 8, 4, 3, 1, 2e-10, "norm"),
 }
+
+# The reference's first flux computation after init in 3-D PARALINE: its shock indicator is
+# computed from a scratch array that aliases the EMF array (shocktemparray = emf,
+# flux.c:1667), which init leaves holding other data; a few cells' flattening differs in that
+# one call.  From the second substep on the records agree.
+FIRST_SUBSTEP_SKIPPED = {"3d_paraline_32x24x8", "3d_paraline_laxf_32x24x8"}
+
+
+def live_substeps(name):
+    subs = [(1, 0), (1, 1), (2, 0), (2, 1)]
+    return subs[1:] if name in FIRST_SUBSTEP_SKIPPED else subs
 
 
 def live(name):
@@ -137,27 +151,26 @@ def test_live_substeps(name):
     orc = O.Oracle(g, rr.geom, rr.conn, rr.aux)
     act = (slice(None),) + g.active
     nd = 3 if g.g.n3 > 1 else 2
-    for step in (1, 2):
-        for to in (0, 1):
-            pb = rr.sub(step, to, "pb")
-            F = [np.zeros_like(pb) for _ in range(3)]
-            ndt = orc.fluxcalc(pb.copy(), *F)
-            for dd in range(1, nd + 1):
-                Fr = rr.sub(step, to, f"F{dd}")
-                sl = active_faces(g, dd)
-                for pl in range(8):
-                    assert err(F[dd - 1][sl][pl], Fr[sl][pl]) < tol, (step, to, dd, pl)
-                assert abs(ndt[dd - 1] - rr.sub(step, to, "ndtdir")[dd - 1]) <= max(tol, 1e-13) * ndt[dd - 1]
-            args = rr.sub(step, to, "args")
-            pf = pb.copy()
-            flag = np.zeros(pb.shape[1:], dtype=np.int8)
-            ndt1, _ = orc.advance(to, rr.sub(step, to, "pi"), pb.copy(), pf, flag, float(args[0]), CUf=args[4:8],
-                                  Cunew=args[8:12])
-            pfr = rr.sub(step, to, "pf")
+    for step, to in live_substeps(name):
+        pb = rr.sub(step, to, "pb")
+        F = [np.zeros_like(pb) for _ in range(3)]
+        ndt = orc.fluxcalc(pb.copy(), *F)
+        for dd in range(1, nd + 1):
+            Fr = rr.sub(step, to, f"F{dd}")
+            sl = active_faces(g, dd)
             for pl in range(8):
-                assert err(pf[act][pl], pfr[act][pl]) < tol, (step, to, "pf", pl)
-            assert (flag[g.active] == rr.sub(step, to, "pflag")[g.active]).all()
-            assert abs(ndt1 - rr.sub(step, to, "ndt")[0]) <= max(tol, 1e-13) * ndt1
+                assert err(F[dd - 1][sl][pl], Fr[sl][pl]) < tol, (step, to, dd, pl)
+            assert abs(ndt[dd - 1] - rr.sub(step, to, "ndtdir")[dd - 1]) <= max(tol, 1e-13) * ndt[dd - 1]
+        args = rr.sub(step, to, "args")
+        pf = pb.copy()
+        flag = np.zeros(pb.shape[1:], dtype=np.int8)
+        ndt1, _ = orc.advance(to, rr.sub(step, to, "pi"), pb.copy(), pf, flag, float(args[0]), CUf=args[4:8],
+                              Cunew=args[8:12])
+        pfr = rr.sub(step, to, "pf")
+        for pl in range(8):
+            assert err(pf[act][pl], pfr[act][pl]) < tol, (step, to, "pf", pl)
+        assert (flag[g.active] == rr.sub(step, to, "pflag")[g.active]).all()
+        assert abs(ndt1 - rr.sub(step, to, "ndt")[0]) <= max(tol, 1e-13) * ndt1
 
 
 def test_reference_metric_locations_shared():
@@ -166,3 +179,71 @@ def test_reference_metric_locations_shared():
     g, rr, _, _ = live("2d_mc_64x64")
     G = rr.geom8
     assert np.array_equal(G[3], G[0]) and np.array_equal(G[4], G[2]) and np.array_equal(G[5], G[1])
+
+
+# ------------------------------------------------------------------ boundary conditions
+
+BOUND = {  # name: (n1, n2, n3, ng, lim, relative tolerance)
+    "2d_32x32": (32, 32, 1, 4, 0, 1e-15),
+    # the reference's 3-D tables vary with x3 by ~1e-11 (see LIVE), which the inflow check and
+    # the Lorentz-factor limits of the ghost cells see
+    "3d_32x24x8": (32, 24, 8, 4, 0, 1e-9),
+}
+
+
+@pytest.mark.parametrize("name", list(BOUND))
+def test_live_boundary_calls(name):
+    """every per-direction boundary call of a step (the one-layer bound before post_fixup and
+    the full one after it, both substeps), from the reference's own input"""
+    n1, n2, n3, ng, lim, tol = BOUND[name]
+    if not R.available(n1, n2, n3, ng):
+        pytest.skip("reference binary not built (oracle/ref/build.sh needs the reference sources)")
+    g = Grid.torus(n1, n2, n3, lim=lim)
+    rr = R.RefRun(R.run(n1, n2, n3, ng, lim=lim, nsteps=1, every=1, substeps=(1,)), g)
+    orc = O.Oracle(g, rr.geom, rr.conn, rr.aux)
+    calls = rr.bound_calls(1)
+    assert len(calls) == 12
+    for n, (d, one_layer, pin, pout) in enumerate(calls):
+        x = pin.copy()
+        orc.bound_dir(x, d, simple=one_layer)
+        err = np.abs(x - pout) / np.maximum(np.abs(pout), 1e-300)
+        assert float(err.max()) <= tol, (n, d, one_layer, float(err.max()))
+
+
+STEPS = {  # name: (n1, n2, n3, ng, lim, flux, steps, normwise tolerance)
+    "c0_2d_mc_128x128_100steps": (128, 128, 1, 4, 0, 0, 100, 1e-12),
+    "2d_mc_64x64_10steps": (64, 64, 1, 4, 0, 0, 10, 1e-13),
+    "3d_mc_32x24x8_4steps": (32, 24, 8, 4, 0, 0, 4, 1e-9),
+}
+
+
+@pytest.mark.parametrize("name", list(STEPS))
+def test_live_full_steps(name):
+    """full RK2 steps (advance, bound, post_fixup, bound, twice; dt from post_stepch) from the
+    reference's initial torus: the state, the dt sequence and the Newton iteration count of
+    every step equal the reference's"""
+    n1, n2, n3, ng, lim, flux, nsteps, tol = STEPS[name]
+    if not R.available(n1, n2, n3, ng):
+        pytest.skip("reference binary not built (oracle/ref/build.sh needs the reference sources)")
+    every = max(1, nsteps // 4)
+    g = Grid.torus(n1, n2, n3, lim=lim, fluxmethod=flux)
+    rr = R.RefRun(R.run(n1, n2, n3, ng, lim=lim, flux=flux, nsteps=nsteps, every=every), g)
+    orc = O.Oracle(g, rr.geom, rr.conn, rr.aux)
+    P = rr.state(0)
+    orc.bound_prim(P)
+    dt = rr.dt0
+    act = (slice(None),) + g.active
+    for s in range(1, nsteps + 1):
+        assert abs(dt - rr.dt_of_step(s)) <= max(tol, 1e-15) * dt, (s, dt, rr.dt_of_step(s))
+        dt, st = orc.step_ch(P, dt)
+        if n3 == 1:
+            # equal counts while the states agree to round-off; later a cell's stopping test
+            # may flip by one iteration as round-off grows
+            if s <= 25:
+                assert st["newton_iters"] == rr.steps[s, 2], s
+            else:
+                assert abs(st["newton_iters"] - rr.steps[s, 2]) <= 1e-4 * rr.steps[s, 2], s
+        if s % every == 0 or s == nsteps:
+            b = rr.state(s)[act]
+            for pl in range(8):
+                assert normwise(P[act][pl], b[pl]) < tol, (s, pl)
