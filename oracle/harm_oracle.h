@@ -62,6 +62,8 @@ void orc_reconstruct_line_paraline(int n, const double *y, const double *V, cons
 /* the PARALINE flattening coefficients fluxcalc uses on the line along dir through the
    transverse active-relative indices (a, b); Fi has the line's extended length */
 void orc_paraline_line_fi(const orc *o, const double *pb, int dir, int a, int b, double *Fi);
+/* the WENO5 momentum-flux jump indicator fluxcalc uses on the same line */
+void orc_weno_line_dp(const orc *o, const double *pb, int dir, int a, int b, double *dP);
 
 /* the 52 columns of one row of the main dump file (dump_content, dump.c:449) for active cell
    (i, j, k); U may be NULL (primtoU of P) */

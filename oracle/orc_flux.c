@@ -97,6 +97,32 @@ void orc_paraline_line_fi(const orc *o, const double *pb, int dir, int a, int b,
   paraline_line_fi(o, pb, dir, a, b, Fi);
 }
 
+/* WENO5BND: the momentum-flux jump indicator dP of every cell of the line along dir through
+   (a, b) (get_df_line_gen_new interpline.c:1473 -> compute_df_line_new), from the cells'
+   primitives and centre geometry */
+static void weno_line_dp(const orc *o, const double *pb, int dir, int a, int b, double *dP) {
+  const harm_grid *g = &o->g;
+  const int ng = g->ng, ng3 = g->ng3;
+  const int nline = (dir == 1) ? g->n1e : (dir == 2) ? g->n2e : g->n3e;
+  double *pr = (double *)malloc(sizeof(double) * HARM_NPR * (size_t)nline);
+  ogeom *gc = (ogeom *)malloc(sizeof(ogeom) * (size_t)nline);
+  for (int s = 0; s < nline; s++) {
+    int ii, jj, kk;
+    if (dir == 1) { ii = s; jj = a + ng; kk = b + ng3; }
+    else if (dir == 2) { ii = a + ng; jj = s; kk = b + ng3; }
+    else { ii = a + ng; jj = b + ng; kk = s; }
+    for (int p = 0; p < HARM_NPR; p++) pr[(size_t)p * nline + s] = pb[(size_t)p * o->cells + oidx(o, ii, jj, kk)];
+    og_load(o, HARM_LOC_CENT, ii, jj, &gc[s]);
+  }
+  o_weno_dp_line(nline, dir, pr, gc, g->gam, dP);
+  free(pr);
+  free(gc);
+}
+
+void orc_weno_line_dp(const orc *o, const double *pb, int dir, int a, int b, double *dP) {
+  weno_line_dp(o, pb, dir, a, b, dP);
+}
+
 int orc_fluxcalc(orc *o, const double *pb, double *F1, double *F2, double *F3, double ndt[3]) {
   const harm_grid *g = &o->g;
   const size_t cells = o->cells;
@@ -121,10 +147,13 @@ int orc_fluxcalc(orc *o, const double *pb, double *F1, double *F2, double *F3, d
         double *yr = (double *)malloc(sizeof(double) * nline * HARM_NPR);
         /* extended transverse indices */
         int e[3];
-        double *Fi = NULL;
+        double *Fi = NULL, *dP = NULL;
         if (g->lim == HARM_LIM_PARALINE) {
           Fi = (double *)malloc(sizeof(double) * nline);
           paraline_line_fi(o, pb, dir, a, b, Fi);
+        } else if (g->lim == HARM_LIM_WENO5) {
+          dP = (double *)malloc(sizeof(double) * nline);
+          weno_line_dp(o, pb, dir, a, b, dP);
         }
         for (int p = 0; p < HARM_NPR; p++) {
           for (int s = 0; s < nline; s++) {
@@ -135,9 +164,11 @@ int orc_fluxcalc(orc *o, const double *pb, double *F1, double *F2, double *F3, d
             y[s] = pb[(size_t)p * cells + oidx(o, ii, jj, kk)];
           }
           if (Fi) o_recon_line_paraline(nline, y, Fi, yl + (size_t)p * nline, yr + (size_t)p * nline);
+          else if (dP) o_recon_line_weno5(nline, y, dP, yl + (size_t)p * nline, yr + (size_t)p * nline);
           else o_recon_line(g->lim, nline, y, yl + (size_t)p * nline, yr + (size_t)p * nline);
         }
         free(Fi);
+        free(dP);
         int off = (dir == 3) ? ng3 : ng;
         for (int f = lo[dir - 1]; f <= hi[dir - 1]; f++) {
           int s = f + off; /* extended index of the cell above the face */

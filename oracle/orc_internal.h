@@ -37,6 +37,11 @@ void o_recon_line(int lim, int n, const double *y, double *yl, double *yr);
    line with given coefficients (Fi NULL: none); see orc_recon_hi.c */
 void o_paraline_flattener(int n, const double *V, const double *P, double *Fi);
 void o_recon_line_paraline(int n, const double *y, const double *Fi, double *yl, double *yr);
+/* WENO5BND with the momentum-flux jump indicator dP[n] of the line's cells (NULL: no
+   reduction by it); see orc_recon_hi.c */
+void o_recon_line_weno5(int n, const double *y, const double *dP, double *yl, double *yr);
+/* dP of each cell of a line from the cells' primitives pr[p * n + s] and centre geometry */
+void o_weno_dp_line(int n, int dir, const double *pr, const ogeom *g, double gam, double *dP);
 
 static inline size_t oidx(const orc *o, int ii, int jj, int kk) {
   return ((size_t)kk * o->g.n2e + jj) * o->g.n1e + ii;

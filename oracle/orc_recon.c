@@ -25,7 +25,6 @@ static double mc_slope(double yl, double yc, double yr) {
   return MINMOD(Dqc, MINMOD(Dqm, Dqp));
 }
 
-void o_recon_line_weno5(int n, const double *y, double *yl, double *yr);
 void o_recon_line_para(int n, const double *y, double *yl, double *yr);
 
 void o_recon_line(int lim, int n, const double *y, double *yl, double *yr) {
@@ -41,7 +40,7 @@ void o_recon_line(int lim, int n, const double *y, double *yl, double *yr) {
   } else if (lim == HARM_LIM_PARALINE) {
     o_recon_line_paraline(n, y, NULL, yl, yr);
   } else {
-    o_recon_line_weno5(n, y, yl, yr);
+    o_recon_line_weno5(n, y, NULL, yl, yr);
   }
 }
 

@@ -16,15 +16,20 @@
  *   - the same for the 2-stencil WENO3 (compute_lower_order_stencil_weights :1300);
  *   - stencil reduction: the ratio of a stencil's weight to its neighbour's weight at
  *     distance 2 gives lower_order_fraction = clamp((min ratio - 1.3)/0.3, 0, 1)
- *     (compute_weights_ratios :2316, DO_OR_STENCIL_REDUCTION=0), and the output mixes
- *     (1-f) WENO5 + f WENO3 (choose_weno_order :2442);
+ *     (compute_weights_ratios :2311, DO_OR_STENCIL_REDUCTION=0), raised where the cell's
+ *     momentum-flux jump dP exceeds 0.25 to its neighbours' fractions
+ *     (apply_additional_reduction_to_weights :795, DO_REDUCE_POST_SHOCK/PRE_SHOCK,
+ *     REDUCE_DP_FRACTION 0.5; dP from compute_df_line_new interpline.c:3557), and the output
+ *     mixes (1-f) WENO5 + f WENO3 (choose_weno_order :2442);
+ *   - the SMONO monotonicity indicator m of the 5-point polynomial (DO_SMONO_C2E,
+ *     compute_mono_indicator_point_eno5 interpline.smono.c:517): m = 1 gives the 5-point
+ *     edge values, m in (0,1) blends the cell's WENO5 weights towards equal weights
+ *     (mono_adjust_unoptimized_weights :852) and the output towards the 5-point values;
  *   - edge values from the stencil polynomials (eno_cvt :884, c2l/c2r_array2/3 :335-349),
  *     all sums in the symmetric pairwise order of get_sum_of_elements (:2266,
  *     SYMMETRIZE_WENO=1).
- * Not restated: the SMONO monotonicity indicator (DO_SMONO_C2E, interpline.smono.c), which
- * here is taken as 0 everywhere (pure WENO output), the shock / pressure-jump reductions
- * (apply_additional_reduction_to_weights, SHOCKINDICATOR), and the GAMCHECK switch of the
- * ratio thresholds for Lorentz factors above 10.
+ * GAMCHECK (the a2c ratio thresholds for large Lorentz factors, reconstructeno.c:303) is 0 in
+ * this build (VSQ is not interpolated).
  *
  * PPM (lim = PARA, WHICHPARA=PARA4): para4 / para4gen (interppoint.para.c:568, :611) with
  * PARA2LIM=MC, JONPARASTEEP=0, JONPARASMOOTH=0, JONPARAREDUCE=0, WHICHLIMITERTOUSEFORLR=0,
@@ -83,14 +88,20 @@ static double limit_weight(int order, double w) {
 }
 
 /* weights of one cell: w[0..r-1] unoptimised, w[r..2r-1] left face, w[2r..3r-1] right face.
-   u points at the cell. */
+   u points at the cell; m is the cell's SMONO indicator. */
 typedef struct wts {
   double w5[9], w3[6];
-  double frac;
+  double frac, m;
 } wts;
 
-static void cell_weights(int r, const double *u, double *w) {
+static void cell_weights(int r, double m, const double *u, double *w) {
   double beta[3];
+  /* compute_cf_stencil_weights (reconstructeno.c:1693): a monotone cell (indicator 1) takes
+     equal weights, and its face weights are never formed (its edges are the 5-point values) */
+  if (m == 1) {
+    for (int s = 0; s < r; s++) w[s] = 1.0 / r;
+    return;
+  }
   if (r == 3) {
     double fd[3], sd[3];
     fd[0] = -(3 * u[0] + u[2]) + 4 * u[1];
@@ -118,6 +129,15 @@ static void cell_weights(int r, const double *u, double *w) {
   normalize(r, 0.0, w);
   for (int s = 0; s < r; s++) w[s] = limit_weight(r, w[s]);
   normalize(r, 0.0, w);
+  /* mono_adjust_unoptimized_weights (:446): a partly monotone cell moves its WENO5 weights
+     towards equal ones */
+  if (r == 3 && m > 0.0 && m < 1.0)
+    for (int s = 0; s < r; s++) w[s] = (1.0 - m) * w[s] + m * (1.0 / r);
+}
+
+/* face weights: the unoptimised weights times the optimal ones, normalised
+   (compute_optimized_cf_stencil_weights :1905) */
+static void face_weights(int r, double *w) {
   static const double dl3[3] = {1. / 16., 5. / 8., 5. / 16.}, dr3[3] = {5. / 16., 5. / 8., 1. / 16.};
   static const double dl2[2] = {1. / 4., 3. / 4.}, dr2[2] = {3. / 4., 1. / 4.};
   for (int s = 0; s < r; s++) {
@@ -147,28 +167,131 @@ static double cvt(int r, int right, const double *w, const double *u) {
   return symsum(r, upd);
 }
 
-void o_recon_line_weno5(int n, const double *y, double *yl, double *yr) {
+/* SMONO indicator of the 5-point polynomial through u[-2..2] (compute_mono_indicator_point_eno5
+   interpline.smono.c:517, SMONO_EPSILON = 500 DBL_EPSILON): 1 where the edge derivatives of
+   orders 1..3 agree in sign on both sides and are well above round-off, 0 at an extremum or
+   inflection, linear in between (SMONO_DO_SMOOTH_TRANSITION) */
+static double smono_indicator(const double *y) {
+  double ld[4], rd[4], md[4], minabs = 1.e+100;
+  ld[1] = (((-3 * y[-2] + y[2]) + (-10 * y[-1] - 6 * y[1])) + 18 * y[0]) / 12.;
+  ld[2] = (((11 * y[-2] - y[2]) + (-20 * y[-1] + 4 * y[1])) + 6 * y[0]) / 12.;
+  ld[3] = (((-3 * y[-2] - y[2]) + (10 * y[-1] + 6 * y[1])) - 12 * y[0]) / 2.;
+  rd[1] = (((-y[-2] + 3 * y[2]) + (6 * y[-1] + 10 * y[1])) - 18 * y[0]) / 12.;
+  rd[2] = (((-y[-2] + 11 * y[2]) + (4 * y[-1] - 20 * y[1])) + 6 * y[0]) / 12.;
+  rd[3] = (((y[-2] + 3 * y[2]) - (6 * y[-1] + 10 * y[1])) + 12 * y[0]) / 2.;
+#define SMINMODB(a, b) ((fabs(a) < fabs(b)) ? (a) : (b))
+#define SMINMOD(a, b) (((a) * (b) <= 0) ? 0.0 : SMINMODB(a, b))
+  ld[1] = SMINMOD(ld[1], y[-1] - y[-2]);
+  rd[1] = SMINMOD(rd[1], y[2] - y[1]);
+  for (int n = 1; n <= 3; n++) {
+    md[n] = SMINMOD(ld[n], rd[n]);
+    minabs = (minabs < fabs(md[n])) ? minabs : fabs(md[n]);
+  }
+  double norm = fabs(y[0]) + ((fabs(y[-1]) + fabs(y[1])) + (fabs(y[-2]) + fabs(y[2])));
+  double cutoff = norm * (500.0 * DBL_EPSILON) + DBL_MIN;
+  double v = (minabs - 0.0) / (cutoff - 0.0);
+  v = (1. < v) ? 1. : v;
+  return (0. > v) ? 0. : v;
+}
+
+/* the 5-point interpolation of the left or right edge (c2e_simple_eno reconstructeno.c:984,
+   c2l_array5 / c2r_array5 row 2 reconstructeno_staticfuncs_constvars.h:321-333) */
+static double edge5(int right, const double *y) {
+  static const double cl[5] = {-5. / 128., 15. / 32., 45. / 64., -5. / 32., 3. / 128.};
+  static const double cr[5] = {3. / 128., -5. / 32., 45. / 64., 15. / 32., -5. / 128.};
+  double d[5];
+  for (int i = -2; i <= 2; i++) d[i + 2] = (right ? cr : cl)[i + 2] * y[i];
+  return symsum(5, d);
+}
+
+/* the momentum-flux jump indicator of each cell of a line (compute_df_line_new
+   interpline.c:3557, from the cell-centre state get_stateforinterpline phys.c:76):
+   par = |(1 + u_t) u^dir|, veff = sign(sqrt(-g) rho u^dir) par / (sqrt(par) + SMALL),
+   upar = |(u + p + b^2)(|u^dir| u_t) + p + b^2/2 - b^dir b_t|, and
+   dP = (|rho (veff[+1] - veff[-1])^2| + |upar[+1] - upar[-1]|) / (|rho par| + |upar| + SMALL)
+   for the cells 1..n-2 (0 at the two ends, which no reconstruction reads) */
+void o_weno_dp_line(int n, int dir, const double *pr, const ogeom *g, double gam, double *dP) {
+  const double SMALL = 1.e-300;
+  double *par = (double *)malloc(sizeof(double) * 3 * (size_t)n), *veff = par + n, *upar = par + 2 * n;
+  for (int s = 0; s < n; s++) {
+    double p[HARM_NPR];
+    for (int q = 0; q < HARM_NPR; q++) p[q] = pr[(size_t)q * n + s];
+    ostate q;
+    o_get_state(p, &g[s], gam, &q);
+    double bcon[4], bcov[4];
+    bcon[0] = p[HARM_B1] * q.ucov[1] + p[HARM_B2] * q.ucov[2] + p[HARM_B3] * q.ucov[3];
+    for (int j = 1; j <= 3; j++) bcon[j] = (p[HARM_B1 - 1 + j] + bcon[0] * q.ucon[j]) / q.ucon[0];
+    o_lower(bcon, &g[s], bcov);
+    double pgas = q.pressure;
+    double V = g[s].gdet * p[HARM_RHO] * q.ucon[dir];
+    double btt = -bcon[dir] * bcov[0];
+    double ptot = pgas + 0.5 * q.bsq;
+    par[s] = fabs(q.plus1ud0 * q.ucon[dir]);
+    veff[s] = copysign(1.0, V) * par[s] / (sqrt(par[s]) + SMALL);
+    upar[s] = fabs((p[HARM_UU] + pgas + q.bsq) * (fabs(q.ucon[dir]) * q.ucov[0]) + ptot + btt);
+  }
+  dP[0] = dP[n - 1] = 0.0;
+  for (int s = 1; s < n - 1; s++) {
+    double rho = pr[(size_t)HARM_RHO * n + s], dv = veff[s + 1] - veff[s - 1];
+    dP[s] = (fabs(rho * dv * dv) + fabs(upar[s + 1] - upar[s - 1])) / (fabs(rho * par[s]) + fabs(upar[s]) + SMALL);
+  }
+  free(par);
+}
+
+void o_recon_line_weno5(int n, const double *y, const double *dP, double *yl, double *yr) {
   for (int c = 0; c < n; c++) yl[c] = yr[c] = y[c];
   if (n < 9) return;
   wts *W = (wts *)calloc((size_t)n, sizeof(wts));
   for (int c = 2; c < n - 2; c++) {
-    cell_weights(3, y + c, W[c].w5);
-    cell_weights(2, y + c, W[c].w3);
+    W[c].m = smono_indicator(y + c);
+    cell_weights(3, W[c].m, y + c, W[c].w5);
+    cell_weights(2, W[c].m, y + c, W[c].w3);
   }
   for (int c = 4; c < n - 4; c++) {
-    /* compute_weights_ratios: LEFT_WEIGHT = 2, RIGHT_WEIGHT = 0, neighbours at c -/+ 2 */
-    double rl = (W[c].w5[2] + WENO_EPS) / (W[c - 2].w5[0] + WENO_EPS);
-    double rr = (W[c].w5[0] + WENO_EPS) / (W[c + 2].w5[2] + WENO_EPS);
+    /* compute_weights_ratios: LEFT_WEIGHT = 2, RIGHT_WEIGHT = 0, neighbours at c -/+ 2; the
+       ratio is formed in long double, as WENO_EPSILON is a long double constant there */
+    const long double eps = (500.0L * DBL_EPSILON) * (500.0L * DBL_EPSILON);
+    double rl = (double)((W[c].w5[2] + eps) / (W[c - 2].w5[0] + eps));
+    double rr = (double)((W[c].w5[0] + eps) / (W[c + 2].w5[2] + eps));
     double ratio = fmin(rl, rr);
     double f = (ratio - 1.3) / (1.6 - 1.3);
     f = fmax(0., fmin(f, 1.0));
     W[c].frac = f;
   }
+  /* apply_additional_reduction_to_weights (reconstructeno.c:795; DO_REDUCE_POST_SHOCK and
+     DO_REDUCE_PRE_SHOCK, REDUCE_DP_FRACTION = 0.5): where the cell's |dP| exceeds 0.25 the
+     reduction of either neighbour, scaled by min((|dP| - 0.25)/0.25, 1), is taken if larger;
+     the neighbours' fractions are the ones before this step */
+  double *lof = (double *)malloc(sizeof(double) * (size_t)n);
+  for (int c = 0; c < n; c++) lof[c] = W[c].frac;
+  if (dP) {
+    for (int c = 5; c < n - 5; c++) {
+      double ss = (fabs(dP[c]) - 0.5 * 0.5) / (0.5 * 0.5);
+      ss = (ss < 1.) ? ss : 1.;
+      double l = W[c].frac, t = ss * W[c + 1].frac;
+      l = (l > t) ? l : t;
+      t = ss * W[c - 1].frac;
+      lof[c] = (l > t) ? l : t;
+    }
+  }
   for (int c = 4; c < n - 4; c++) {
-    double f = W[c].frac;
+    const double m = W[c].m;
+    double y5l = 0.0, y5r = 0.0;
+    if (m != 0) {
+      y5l = edge5(0, y + c);
+      y5r = edge5(1, y + c);
+    }
+    if (m >= 1.0) {  /* the monotone cell's edges are the 5-point values */
+      yl[c] = y5l;
+      yr[c] = y5r;
+      continue;
+    }
+    double f = lof[c];
     double w5[9], w3[6];
     memcpy(w5, W[c].w5, sizeof(w5));
     memcpy(w3, W[c].w3, sizeof(w3));
+    face_weights(3, w5);
+    face_weights(2, w3);
     int two = (0.0 < f);
     if (two) {
       for (int k = 3; k < 9; k++) w5[k] *= (1. - f);
@@ -181,9 +304,10 @@ void o_recon_line_weno5(int n, const double *y, double *yl, double *yr) {
       outl += cvt(2, 0, w3 + 2, y + c);
       outr += cvt(2, 1, w3 + 4, y + c);
     }
-    yl[c] = (1.0 - 0.0) * outl + 0.0 * y[c];
-    yr[c] = (1.0 - 0.0) * outr + 0.0 * y[c];
+    yl[c] = (1.0 - m) * outl + m * y5l;
+    yr[c] = (1.0 - m) * outr + m * y5r;
   }
+  free(lof);
   free(W);
 }
 

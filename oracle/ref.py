@@ -24,7 +24,7 @@ BUILD = os.path.join(HERE, "ref", "build.sh")
 
 # grid -> binary name; MAXBND is 4 for MC/PPM/PARALINE and 6 for WENO5 (the ghost width of
 # the device grid, which also sets the inner radius through setihor, coord.c:2334)
-LIM_NAMES = {0: "mc", 1: "para", 2: "weno5", 3: "paraline"}
+LIM_NAMES = {0: "mc", 1: "para", 2: "weno5bnd", 3: "paraline"}
 FLUX_NAMES = {0: "hll", 1: "laxf"}
 
 # reference pflag positions [k][j][i] -> device order is the same for active cells

@@ -11,14 +11,16 @@
 #      PRODUCTION 1, WENO line memory on (WENOMEMORY 1) with the a2c-only
 #      WENO_REDUCE_A2C_LOOK_OTHER_DIRECTIONS off;
 #   3. renames the problem's init_defcoord/init_grid/init_global to href_fishmon_* so that
-#      oracle/ref/driver.c can wrap them with this build's run configuration;
+#      oracle/ref/driver.c can wrap them with this build's run configuration, and gives
+#      choose_weno_order's weight array static storage (it returns a pointer into it) and
+#      points the WENO pass's primitive line at the line it reads;
 #   4. writes the extern-declaration headers (decs.h and the like) from the definition
 #      headers (prefixing 'extern' to the top-level definitions) and generates
 #      global.defnprs.h with the reference's own generatenprs.c;
 #   5. compiles every source of the reference's GRMHD object lists except main.c, plus
 #      oracle/ref/driver.c, with gcc -O3 -fopenmp -fcommon, and links them with the calls of
-#      advance(), fluxcalc(), post_fixup(), bound_prim_user_dir() and flux_compute_general()
-#      routed through the driver's recording
+#      advance(), fluxcalc(), post_fixup(), bound_prim_user_dir(), flux_compute_general() and
+#      pass_1d_line_multipl_weno() routed through the driver's recording
 #      wrappers (ld --wrap), which call the reference's own functions.
 # gcc on x86-64 without -march emits no fused multiply-add, so the arithmetic is the
 # IEEE operations of the source in its order.
@@ -94,6 +96,23 @@ build_one() {
     edit init.h "s/^#define WENO_REDUCE_A2C_LOOK_OTHER_DIRECTIONS 1/#define WENO_REDUCE_A2C_LOOK_OTHER_DIRECTIONS 0/" \
          "^#define WENO_REDUCE_A2C_LOOK_OTHER_DIRECTIONS 0"
     printf '\n#undef WENOMEMORY\n#define WENOMEMORY 1\n' >> init.h
+    # choose_weno_order (reconstructeno.c:2442) hands back a pointer into its own stack frame
+    # (stencil_weights_array_static_other), so the WENO3 half of a reduced stencil is read
+    # after that frame is gone; built here it reads as zero weights and a fully reduced edge
+    # value comes out 0.  The checker runs on one thread, so the array gets static storage,
+    # which gives the mix of WENO5 and WENO3 the code intends.
+    edit reconstructeno.c "s/^\(\s*\)weno_weights_t stencil_weights_array_static_other\[NUM_POINTS\];/\1static weno_weights_t stencil_weights_array_static_other[NUM_POINTS];/" \
+         "static weno_weights_t stencil_weights_array_static_other\[NUM_POINTS\];"
+    # The line pass with precomputed indicators (slope_lim_linetype_c2e_perijk_precomputeindicators
+    # interpline.c:468) computes the momentum-flux jump indicator dP of the WENO reduction
+    # (compute_df_line_new interpline.c:3557) from its primitive line yprim, which that path
+    # never fills: dP then comes from whatever the stack held (the cell state itself is read
+    # from the stored fluxstatecent, STOREFLUXSTATE).  Its sibling pass
+    # slope_lim_linetype_c2e_perijk (interpline.c:696) points yprim at the line it reads
+    # (yprim=yin); the checker build does the same here, so that dP is the indicator of the
+    # cells' own primitives.
+    edit interpline.c "/^void slope_lim_linetype_c2e_perijk_precomputeindicators(/,/p2interp, yin, &trueijkp);/ s/\(p2interp, yin, &trueijkp);\)\$/\1 yprim=yin;/" \
+         "p2interp, yin, &trueijkp); yprim=yin;"
     for fn in init_defcoord init_grid init_global; do
       edit init.c "s/^int $fn(void)/int href_fishmon_$fn(void)/" "^int href_fishmon_$fn(void)"
     done
@@ -113,7 +132,7 @@ build_one() {
     printf '%s\n' $srcs href_driver.c | xargs -P "$JOBS" -I{} sh -c \
       'gcc '"$CFLAGS"' -c {} -o "$(basename {} .c).o" || { echo "ref_build: compiling {} failed" >&2; exit 255; }'
     objs=$(printf '%s\n' $srcs href_driver.c | sed 's/\.c$/.o/')
-    gcc -fopenmp -mcmodel=medium -no-pie -Wl,--wrap=advance,--wrap=fluxcalc,--wrap=post_fixup,--wrap=bound_prim_user_dir,--wrap=flux_compute_general \
+    gcc -fopenmp -mcmodel=medium -no-pie -Wl,--wrap=advance,--wrap=fluxcalc,--wrap=post_fixup,--wrap=bound_prim_user_dir,--wrap=flux_compute_general,--wrap=pass_1d_line_multipl_weno \
         -o "$bin.tmp" $objs -lm
     mv "$bin.tmp" "$bin"
   )

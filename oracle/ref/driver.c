@@ -473,6 +473,47 @@ int __wrap_flux_compute_general(int i, int j, int k, int dir, struct of_geom *pt
   return r;
 }
 
+/* HREF_WPROBE="dir,j,k[,pl]" (j,k: the transverse indices of the line as the reference's loop
+   passes them): print one primitive's line (default the density) of that WENO reconstruction -- input, SMONO indicator,
+   pressure-jump indicator and the left/right edge values (pass_1d_line_multipl_weno
+   reconstructeno.c:2877, called through a pointer set in interpline.c) */
+void __real_pass_1d_line_multipl_weno(int MULTIPLTYPE, int whichquantity, int dir, int do_weight_or_recon,
+                                      int recontype, int whichreduce, int preforder, int bs, int ps, int pe, int be,
+                                      int *minorder, int *maxorder, int *shift, FTYPE *shockindicator,
+                                      FTYPE *stiffindicator, FTYPE *Vline, FTYPE *Pline,
+                                      FTYPE (*df)[NUMDFS][NBIGM], FTYPE (*dP)[NBIGM], FTYPE (*etai)[NBIGM],
+                                      FTYPE (*monoindicator)[NUMMONOINDICATORS][NBIGM], FTYPE (*yprim)[2][NBIGM],
+                                      FTYPE (*ystencilvar)[2][NBIGM], FTYPE (*yin)[2][NBIGM], FTYPE (*yout)[2][NBIGM],
+                                      FTYPE (*youtpolycoef)[MAXSPACEORDER][NBIGM], struct of_trueijkp *trueijkp);
+
+void __wrap_pass_1d_line_multipl_weno(int MULTIPLTYPE, int whichquantity, int dir, int do_weight_or_recon,
+                                      int recontype, int whichreduce, int preforder, int bs, int ps, int pe, int be,
+                                      int *minorder, int *maxorder, int *shift, FTYPE *shockindicator,
+                                      FTYPE *stiffindicator, FTYPE *Vline, FTYPE *Pline,
+                                      FTYPE (*df)[NUMDFS][NBIGM], FTYPE (*dP)[NBIGM], FTYPE (*etai)[NBIGM],
+                                      FTYPE (*monoindicator)[NUMMONOINDICATORS][NBIGM], FTYPE (*yprim)[2][NBIGM],
+                                      FTYPE (*ystencilvar)[2][NBIGM], FTYPE (*yin)[2][NBIGM], FTYPE (*yout)[2][NBIGM],
+                                      FTYPE (*youtpolycoef)[MAXSPACEORDER][NBIGM], struct of_trueijkp *trueijkp)
+{
+  static int pd = -9999, pj, pk, ppl = RHO;
+  int i;
+  __real_pass_1d_line_multipl_weno(MULTIPLTYPE, whichquantity, dir, do_weight_or_recon, recontype, whichreduce,
+                                   preforder, bs, ps, pe, be, minorder, maxorder, shift, shockindicator,
+                                   stiffindicator, Vline, Pline, df, dP, etai, monoindicator, yprim, ystencilvar, yin,
+                                   yout, youtpolycoef, trueijkp);
+  if (pd == -9999) {
+    const char *s = getenv("HREF_WPROBE");
+    if (!s || sscanf(s, "%d,%d,%d,%d", &pd, &pj, &pk, &ppl) < 3) pd = -9998;
+  }
+  if (dir == pd && trueijkp->j == pj && trueijkp->k == pk && nstep == 0) {
+    fprintf(stderr, "WPROBE dir %d j %d k %d bs %d ps %d pe %d be %d preforder %d\n", dir, pj, pk, bs, ps, pe, be,
+            preforder);
+    for (i = bs; i <= be; i++)
+      fprintf(stderr, "  i %3d y %.17g yprim %.17g mono %.17g dP %.17g shock %.17g l %.17g r %.17g\n", i, yin[ppl][0][i], yprim[ppl][0][i],
+              monoindicator[ppl][MONOINDTYPE][i], dP[0][i], shockindicator[i], yout[ppl][0][i], yout[ppl][1][i]);
+  }
+}
+
 static void do_step(void)
 {
   bnd_calls = 0;

@@ -114,6 +114,7 @@ def test_golden_utoprimgen(kind):
 LIVE = {  # name: (n1, n2, n3, ng, lim, flux, tolerance, measure)
     "2d_mc_64x64": (64, 64, 1, 4, 0, 0, 1e-12, "rel"),
     "2d_paraline_laxf_64x64": (64, 64, 1, 4, 3, 1, 1e-12, "rel"),
+    "2d_weno5_48x48": (48, 48, 1, 6, 2, 0, 1e-12, "rel"),
     # the reference stores its metric per (i,j,k), and its numerically differentiated
     # Jacobian varies with x3 by ~1e-11 of each component; the oracle uses k=0's tables on
     # every plane, so 3-D fluxes agree to ~1e-10 of each field's largest face value
@@ -121,6 +122,8 @@ LIVE = {  # name: (n1, n2, n3, ng, lim, flux, tolerance, measure)
     "3d_para_32x24x8": (32, 24, 8, 4, 1, 0, 2e-10, "norm"),
     "3d_paraline_32x24x8": (32, 24, 8, 4, 3, 0, 2e-10, "norm"),
     "3d_paraline_laxf_32x24x8": (32, 24, 8, 4, 3, 1, 2e-10, "norm"),
+    # WENO5's nonlinear weights carry the same metric difference a little further (2.1e-10)
+    "3d_weno5_32x24x8": (32, 24, 8, 6, 2, 0, 1e-9, "norm"),
 }
 
 # The reference's first flux computation after init in 3-D PARALINE: its shock indicator is
@@ -214,6 +217,14 @@ STEPS = {  # name: (n1, n2, n3, ng, lim, flux, steps, normwise tolerance)
     "c0_2d_mc_128x128_100steps": (128, 128, 1, 4, 0, 0, 100, 1e-12),
     "2d_mc_64x64_10steps": (64, 64, 1, 4, 0, 0, 10, 1e-13),
     "3d_mc_32x24x8_4steps": (32, 24, 8, 4, 0, 0, 4, 1e-9),
+    "2d_weno5_48x48_20steps": (48, 48, 1, 6, 2, 0, 20, 1e-12),
+    "2d_paraline_64x64_20steps": (64, 64, 1, 4, 3, 0, 20, 1e-12),
+    # 3-D WENO5 runs free for two steps only: the SMONO indicator switches between the
+    # 5-point and the WENO edge where the edge derivatives are within ~1e-13 of the stencil's
+    # magnitude, so the ~1e-10 metric difference of the 3-D tables (see LIVE) flips a few
+    # cells near the horizon from the third step on (6e-10 of max |u^3| after two steps, 1e-7
+    # after three).  Substeps 3 and 4 fed the reference's own input agree to 2e-10 like 1 and 2.
+    "3d_weno5_32x24x8_2steps": (32, 24, 8, 6, 2, 0, 2, 1e-8),
 }
 
 
