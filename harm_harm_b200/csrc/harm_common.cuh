@@ -186,7 +186,9 @@ struct ReconGeom<HARM_LIM_PARA> {
 };
 template <>
 struct ReconGeom<HARM_LIM_WENO5> {
-  static constexpr int H = 5, X = 4;
+  // an edge cell c needs the lower-order fractions of c-1 .. c+1, which need the weights of
+  // c-3 .. c+3, which need the cells c-5 .. c+5
+  static constexpr int H = 6, X = 5;
 };
 template <>
 struct ReconGeom<HARM_LIM_PARALINE> {
@@ -200,13 +202,175 @@ struct FluxTile {
   static constexpr int H = ReconGeom<LIM>::H;
   static constexpr int NL = A + H + ReconGeom<LIM>::X;         // staged cells along DIR
   static constexpr int VB = (sizeof(T) == 4) ? 8 : 4;          // primitives per stage
-  static constexpr int NW = (LIM == HARM_LIM_WENO5) ? 3 : 0;   // weights per cell
+  static constexpr int NW = (LIM == HARM_LIM_WENO5) ? 4 : 0;   // WENO5: 3 weights + SMONO per cell
   static constexpr int PLANE = NL * NT;               // staged values of one primitive
   static constexpr int PE = (A + 1) * NT;              // edge values: cells H-1 .. H+A-1
   static constexpr int PW = (NL - 4) * NT;             // WENO5 weights: cells 2 .. NL-3
   static constexpr int NF = (LIM == HARM_LIM_PARALINE) ? 1 : 0;  // PARALINE: V, P, Fi planes
-  static constexpr size_t smem = ((size_t)VB * (PLANE + 2 * PE + NW * PW) + (size_t)NF * (2 * PLANE + PE)) * sizeof(T);
+  static constexpr int ND = (LIM == HARM_LIM_WENO5) ? 1 : 0;     // WENO5: dP of the edge cells
+  static constexpr size_t smem =
+      ((size_t)VB * (PLANE + 2 * PE + NW * PW) + (size_t)NF * (2 * PLANE + PE) + (size_t)ND * PE) * sizeof(T);
+  // WENO5's four per-cell line planes of dP (rho, par, veff, upar) live in the edge planes
+  // until the edges are written
+  static_assert(LIM != HARM_LIM_WENO5 || 2 * VB * PE >= 4 * PLANE, "dP line planes fit the edge planes");
 };
+
+// ------------------------------------------------------------------ WENO5BND tile passes
+// Shared by k_fluxt and k_fluxt_tma.  Layout helpers: sx(c, t) the staged plane, ex(c, t) the
+// edge planes (cells H-1 .. H+A-1), wx(c, t) the weight planes (cells 2 .. NL-3), split(idx,
+// c0, nc, v, c, t) the item order.
+
+// dP line quantities of one staged cell into the four line planes tmp[4][PL]
+template <int DIR, int PL, typename T>
+__device__ __forceinline__ void weno_line_cell(T* tmp, int si, const T* pc, const Geo<T>& g, T gam) {
+  T par, veff, upar;
+  weno_dp_cell<T>(pc, g, gam, DIR, par, veff, upar);
+  tmp[si] = pc[HARM_RHO];
+  tmp[PL + si] = par;
+  tmp[2 * PL + si] = veff;
+  tmp[3 * PL + si] = upar;
+}
+
+// dP of the edge cells from the line planes
+template <int A, int NT, int H, int PL, typename T, typename SX, typename EX, typename SPLIT>
+__device__ __forceinline__ void weno_dp_edges(const T* tmp, T* s_dP, int tid, SX sx, EX ex, SPLIT split) {
+  for (int idx = tid; idx < (A + 1) * NT; idx += 256) {
+    int v, c, t;
+    split(idx, H - 1, A + 1, v, c, t);
+    const int i0 = sx(c, t), im = sx(c - 1, t), ip = sx(c + 1, t);
+    s_dP[ex(c, t)] = weno_dp<T>(tmp[i0], tmp[PL + i0], tmp[3 * PL + i0], tmp[2 * PL + im], tmp[2 * PL + ip],
+                                tmp[3 * PL + im], tmp[3 * PL + ip]);
+  }
+}
+
+// the lower-order fraction of the cell whose weights are at ws[wx(c, t) * 4]
+template <typename T, typename WX>
+__device__ __forceinline__ T weno_frac_at(const T* ws, int c, int t, WX wx) {
+  const T* w0 = ws + wx(c, t) * 4;
+  const T* wm = ws + wx(c - 2, t) * 4;
+  const T* wp = ws + wx(c + 2, t) * 4;
+  T a[3] = {w0[0], w0[1], w0[2]}, b[3] = {wm[0], wm[1], wm[2]}, e[3] = {wp[0], wp[1], wp[2]};
+  return weno_frac<T>(a, b, e);
+}
+
+// WENO5BND edges of NV staged primitives: pass 1 the SMONO indicator and the weights of cells
+// 2 .. NL-3, barrier, pass 2 the lower-order fraction (raised by dP) and the edges of cells
+// H-1 .. H+A-1.  s_dP holds the edge cells' dP and must be ordered before pass 2 by the
+// caller's barriers (pass 1 ends with one).
+template <int NV, int A, int NT, int H, int NL, int PL, int PE, int PW, typename T, typename SX, typename EX,
+          typename WX, typename SPLIT>
+__device__ __forceinline__ void weno_tile_edges(const T* s_y, T* s_w, T* s_el, T* s_er, const T* s_dP, int tid,
+                                                SX sx, EX ex, WX wx, SPLIT split) {
+  if constexpr (sizeof(T) == 4) {
+    // FP32: two cells per thread on the packed FP32 pipe (harm_weno_f32x2.cuh)
+    constexpr int NU = NV * (NL - 4) * NT, NU2 = (NU + 1) / 2;
+    for (int idx = tid; idx < NU2; idx += 256) {
+      const int ib = idx + NU2;
+      const bool hasb = ib < NU;
+      int va, ca, ta, vb, cb, tb;
+      split(idx, 2, NL - 4, va, ca, ta);
+      split(hasb ? ib : idx, 2, NL - 4, vb, cb, tb);
+      const T* ya = s_y + va * PL;
+      const T* yb = s_y + vb * PL;
+      F2 u5[5];
+#pragma unroll
+      for (int q = 0; q < 5; q++) u5[q] = f2((float)ya[sx(ca - 2 + q, ta)], (float)yb[sx(cb - 2 + q, tb)]);
+      F2 w[3];
+      const F2 m = smono_indicator_f2(u5 + 2);
+      weno5_cell_weights_f2(u5 + 2, m, w);
+      T* wsa = s_w + (va * PW + wx(ca, ta)) * 4;
+      T* wsb = s_w + (vb * PW + wx(cb, tb)) * 4;
+      float a, b;
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        f2split(w[k], a, b);
+        wsa[k] = (T)a;
+        if (hasb) wsb[k] = (T)b;
+      }
+      f2split(m, a, b);
+      wsa[3] = (T)a;
+      if (hasb) wsb[3] = (T)b;
+    }
+    __syncthreads();
+    constexpr int NE = NV * (A + 1) * NT, NE2 = (NE + 1) / 2;
+    for (int idx = tid; idx < NE2; idx += 256) {
+      const int ib = idx + NE2;
+      const bool hasb = ib < NE;
+      int va, ca, ta, vb, cb, tb;
+      split(idx, H - 1, A + 1, va, ca, ta);
+      split(hasb ? ib : idx, H - 1, A + 1, vb, cb, tb);
+      const T* ya = s_y + va * PL;
+      const T* yb = s_y + vb * PL;
+      F2 u5[5];
+#pragma unroll
+      for (int q = 0; q < 5; q++) u5[q] = f2((float)ya[sx(ca - 2 + q, ta)], (float)yb[sx(cb - 2 + q, tb)]);
+      const T* wa = s_w + va * PW * 4;
+      const T* wb = s_w + vb * PW * 4;
+      F2 w[3], wm[3], wp[3];
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        w[k] = f2((float)wa[wx(ca, ta) * 4 + k], (float)wb[wx(cb, tb) * 4 + k]);
+        wm[k] = f2((float)wa[wx(ca - 2, ta) * 4 + k], (float)wb[wx(cb - 2, tb) * 4 + k]);
+        wp[k] = f2((float)wa[wx(ca + 2, ta) * 4 + k], (float)wb[wx(cb + 2, tb) * 4 + k]);
+      }
+      const F2 m = f2((float)wa[wx(ca, ta) * 4 + 3], (float)wb[wx(cb, tb) * 4 + 3]);
+      F2 f = weno_frac_f2(w, wm, wp);
+      const float ssa = weno_dp_strength<float>((float)s_dP[ex(ca, ta)]);
+      const float ssb = weno_dp_strength<float>((float)s_dP[ex(cb, tb)]);
+      if (ssa > 0.0f || ssb > 0.0f) {  // rare: a momentum-flux jump above 0.25
+        float fa, fb;
+        f2split(f, fa, fb);
+        if (ssa > 0.0f)
+          fa = weno_lof<float>(fa, (float)weno_frac_at<T>(wa, ca - 1, ta, wx), (float)weno_frac_at<T>(wa, ca + 1, ta, wx), ssa);
+        if (ssb > 0.0f)
+          fb = weno_lof<float>(fb, (float)weno_frac_at<T>(wb, cb - 1, tb, wx), (float)weno_frac_at<T>(wb, cb + 1, tb, wx), ssb);
+        f = f2(fa, fb);
+      }
+      F2 yl, yr;
+      weno5_edges_f2(u5 + 2, w, f, m, yl, yr);
+      float la, lb, ra, rb;
+      f2split(yl, la, lb);
+      f2split(yr, ra, rb);
+      s_el[va * PE + ex(ca, ta)] = (T)la;
+      s_er[va * PE + ex(ca, ta)] = (T)ra;
+      if (hasb) {
+        s_el[vb * PE + ex(cb, tb)] = (T)lb;
+        s_er[vb * PE + ex(cb, tb)] = (T)rb;
+      }
+    }
+  } else {
+    for (int idx = tid; idx < NV * (NL - 4) * NT; idx += 256) {
+      int v, c, t;
+      split(idx, 2, NL - 4, v, c, t);
+      const T* y = s_y + v * PL;
+      T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
+      const T m = smono_indicator<T>(u5 + 2);
+      T w[3];
+      weno5_cell_weights<T>(u5 + 2, m, w);
+      T* ws = s_w + (v * PW + wx(c, t)) * 4;
+      ws[0] = w[0]; ws[1] = w[1]; ws[2] = w[2]; ws[3] = m;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < NV * (A + 1) * NT; idx += 256) {
+      int v, c, t;
+      split(idx, H - 1, A + 1, v, c, t);
+      const T* y = s_y + v * PL;
+      T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
+      const T* ws = s_w + v * PW * 4;
+      const T* w0 = ws + wx(c, t) * 4;
+      T w[3] = {w0[0], w0[1], w0[2]};
+      const T m = w0[3];
+      T f = weno_frac_at<T>(ws, c, t, wx);
+      const T ss = weno_dp_strength<T>(s_dP[ex(c, t)]);
+      if (ss > T(0)) f = weno_lof<T>(f, weno_frac_at<T>(ws, c - 1, t, wx), weno_frac_at<T>(ws, c + 1, t, wx), ss);
+      T yl, yr;
+      weno5_edges<T>(u5 + 2, w, f, m, yl, yr);
+      s_el[v * PE + ex(c, t)] = yl;
+      s_er[v * PE + ex(c, t)] = yr;
+    }
+  }
+}
+
 
 // The face physics of k_fluxt: B^DIR continuity, limit_gamma, states, fluxes, wave speeds and
 // the HLL flux of one face (flux.c:852, vchar.c:34; LAXF where both speeds vanish or where
@@ -269,10 +433,11 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
   T* s_y = reinterpret_cast<T*>(smem_raw);   // [VB][plane]
   T* s_el = s_y + VB * PL;                    // left edge of each cell, [VB][PE]
   T* s_er = s_el + VB * PE;                   // right edge of each cell, [VB][PE]
-  T* s_w = s_er + VB * PE;                    // WENO5 unoptimised weights, [VB][PW][3]
+  T* s_w = s_er + VB * PE;                    // WENO5 weights and SMONO indicator, [VB][PW][4]
   T* s_V = s_w + VB * PW * TL::NW;            // PARALINE: sqrt(-g) rho u^DIR, [plane]
   T* s_P = s_V + PL;                          // PARALINE: p + b^2/2, [plane]
   T* s_F = s_P + PL;                          // PARALINE: flattening coefficient, [PE]
+  T* s_dP = s_w + VB * PW * TL::NW + TL::NF * (2 * PL + PE);  // WENO5: dP of the edge cells, [PE]
   // a plane is [NT][NL] for DIR 1 and [NL][NT] otherwise: the index along i is contiguous
   auto sx = [](int c, int t) -> int { return (DIR == 1) ? t * NL + c : c * NT + t; };
   // edge planes hold cells H-1 .. H+A-1, weight planes cells 2 .. NL-3, in the same layout
@@ -354,6 +519,33 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
       s_F[ex(c, t)] = paraline_fi<T>(vv, pp);
     }
   }
+  // WENO5: the line quantities of dP (compute_df_line_new interpline.c:3557) of every staged
+  // cell from all its primitives and the cell-centre metric, into the edge planes, then dP of
+  // each edge cell.  With all primitives staged at once (FP32) this reads the staged tile
+  // below; otherwise (FP64, two groups) it loads them here.
+  auto weno_line = [&](int cl, int ct, const T* pc) {
+    const int lext = min(max(l0 - H + cl + ngL, 0), nLe - 1);
+    const int text = min(max(t0 + ct + d.ng, 0), nTe - 1);
+    const int ii = (DIR == 1) ? lext : text, jj = (DIR == 1) ? text : (DIR == 2) ? lext : o + d.ng;
+    Geo<T> g;
+    load_geo<T, GT>(geom + (size_t)HARM_LOC_CENT * HARM_NGF * d.plane, d.plane, (size_t)jj * d.n1e + ii, g);
+    weno_line_cell<DIR, PL, T>(s_el, sx(cl, ct), pc, g, (T)ph.gam);
+  };
+  if constexpr (LIM == HARM_LIM_WENO5 && VB < NPR) {
+    for (int idx = tid; idx < PL; idx += 256) {
+      int v, cl, ct;
+      split(idx, 0, NL, v, cl, ct);
+      const int lext = min(max(l0 - H + cl + ngL, 0), nLe - 1);
+      const int text = min(max(t0 + ct + d.ng, 0), nTe - 1);
+      const size_t cid = cell_index(lext, text);
+      T pc[NPR];
+#pragma unroll
+      for (int p = 0; p < NPR; p++) pc[p] = (T)__ldg(P + (size_t)p * d.cells + cid);
+      weno_line(cl, ct, pc);
+    }
+    __syncthreads();
+    weno_dp_edges<A, NT, H, PL, T>(s_el, s_dP, tid, sx, ex, split);
+  }
   T pl[NPR], pr[NPR];
 #pragma unroll
   for (int p0 = 0; p0 < NPR; p0 += VB) {
@@ -370,98 +562,20 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
       s_y[v * PL + sx(cl, ct)] = (T)__ldg(P + (size_t)(p0 + v) * d.cells + cell_index(lext, text));
     }
     __syncthreads();
-    if constexpr (LIM == HARM_LIM_WENO5 && sizeof(T) == 4) {
-      // FP32: two cells per thread on the packed FP32 pipe (harm_weno_f32x2.cuh)
-      constexpr int NU = VB * (NL - 4) * NT, NU2 = (NU + 1) / 2;
-      for (int idx = tid; idx < NU2; idx += 256) {
-        const int ib = idx + NU2;
-        const bool hasb = ib < NU;
-        int va, ca, ta, vb, cb, tb;
-        split(idx, 2, NL - 4, va, ca, ta);
-        split(hasb ? ib : idx, 2, NL - 4, vb, cb, tb);
-        const T* ya = s_y + va * PL;
-        const T* yb = s_y + vb * PL;
-        F2 u5[5];
+    if constexpr (LIM == HARM_LIM_WENO5) {
+      if constexpr (VB == NPR) {
+        for (int idx = tid; idx < PL; idx += 256) {
+          int v, cl, ct;
+          split(idx, 0, NL, v, cl, ct);
+          T pc[NPR];
 #pragma unroll
-        for (int q = 0; q < 5; q++) u5[q] = f2((float)ya[sx(ca - 2 + q, ta)], (float)yb[sx(cb - 2 + q, tb)]);
-        F2 w[3];
-        weno5_unopt_f2(u5 + 2, w);
-        T* wsa = s_w + (va * PW + wx(ca, ta)) * 3;
-        T* wsb = s_w + (vb * PW + wx(cb, tb)) * 3;
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-          float a, b;
-          f2split(w[k], a, b);
-          wsa[k] = (T)a;
-          if (hasb) wsb[k] = (T)b;
+          for (int p = 0; p < NPR; p++) pc[p] = s_y[p * PL + sx(cl, ct)];
+          weno_line(cl, ct, pc);
         }
+        __syncthreads();
+        weno_dp_edges<A, NT, H, PL, T>(s_el, s_dP, tid, sx, ex, split);
       }
-      __syncthreads();
-      constexpr int NE = VB * (A + 1) * NT, NE2 = (NE + 1) / 2;
-      for (int idx = tid; idx < NE2; idx += 256) {
-        const int ib = idx + NE2;
-        const bool hasb = ib < NE;
-        int va, ca, ta, vb, cb, tb;
-        split(idx, H - 1, A + 1, va, ca, ta);
-        split(hasb ? ib : idx, H - 1, A + 1, vb, cb, tb);
-        const T* ya = s_y + va * PL;
-        const T* yb = s_y + vb * PL;
-        F2 u5[5];
-#pragma unroll
-        for (int q = 0; q < 5; q++) u5[q] = f2((float)ya[sx(ca - 2 + q, ta)], (float)yb[sx(cb - 2 + q, tb)]);
-        const T* wa = s_w + va * PW * 3;
-        const T* wb = s_w + vb * PW * 3;
-        F2 w[3], wm[3], wp[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-          w[k] = f2((float)wa[wx(ca, ta) * 3 + k], (float)wb[wx(cb, tb) * 3 + k]);
-          wm[k] = f2((float)wa[wx(ca - 2, ta) * 3 + k], (float)wb[wx(cb - 2, tb) * 3 + k]);
-          wp[k] = f2((float)wa[wx(ca + 2, ta) * 3 + k], (float)wb[wx(cb + 2, tb) * 3 + k]);
-        }
-        F2 yl, yr;
-        weno5_edges_f2(u5 + 2, w, wm, wp, yl, yr);
-        float la, lb, ra, rb;
-        f2split(yl, la, lb);
-        f2split(yr, ra, rb);
-        s_el[va * PE + ex(ca, ta)] = (T)la;
-        s_er[va * PE + ex(ca, ta)] = (T)ra;
-        if (hasb) {
-          s_el[vb * PE + ex(cb, tb)] = (T)lb;
-          s_er[vb * PE + ex(cb, tb)] = (T)rb;
-        }
-      }
-    } else if (LIM == HARM_LIM_WENO5) {
-      // unoptimised weights of cells 2 .. NL-3
-      for (int idx = tid; idx < VB * (NL - 4) * NT; idx += 256) {
-        int v, c, t;
-        split(idx, 2, NL - 4, v, c, t);
-        const T* y = s_y + v * PL;
-        T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
-        T w[3];
-        weno5_unopt<T>(u5 + 2, w);
-        T* ws = s_w + (v * PW + wx(c, t)) * 3;
-        ws[0] = w[0]; ws[1] = w[1]; ws[2] = w[2];
-      }
-      __syncthreads();
-      // edges of cells H-1 .. H+A-1
-      for (int idx = tid; idx < VB * (A + 1) * NT; idx += 256) {
-        int v, c, t;
-        split(idx, H - 1, A + 1, v, c, t);
-        const T* y = s_y + v * PL;
-        T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
-        const T* ws = s_w + v * PW * 3;
-        T w[3], wm[3], wp[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-          w[k] = ws[wx(c, t) * 3 + k];
-          wm[k] = ws[wx(c - 2, t) * 3 + k];
-          wp[k] = ws[wx(c + 2, t) * 3 + k];
-        }
-        T yl, yr;
-        weno5_edges<T>(u5 + 2, w, wm, wp, yl, yr);
-        s_el[v * PE + ex(c, t)] = yl;
-        s_er[v * PE + ex(c, t)] = yr;
-      }
+      weno_tile_edges<VB, A, NT, H, NL, PL, PE, PW, T>(s_y, s_w, s_el, s_er, s_dP, tid, sx, ex, wx, split);
     } else if (LIM == HARM_LIM_PARA) {
       for (int idx = tid; idx < VB * (A + 1) * NT; idx += 256) {
         int v, c, t;

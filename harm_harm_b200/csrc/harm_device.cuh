@@ -335,18 +335,28 @@ __device__ __forceinline__ void paraline_cell(const T* y, T fi, T& lout, T& rout
   rout = r;
 }
 
-// ---------------------------------------------------------------- WENO5 (WENO5BND core)
+// ---------------------------------------------------------------- WENO5 (WENO5BND)
 // eno_line_reconstruct reconstructeno.c:333 for CVT_C2E: smoothness indicators
 // (compute_cf_stencil_weights :1693), desensitising and normalisation (:2001, :2292),
 // 1/(beta+eps)^2 weights (:2211), limit_weight (:3015), optimal face weights (:1905),
-// WENO3 lower-order weights, weight-ratio stencil reduction (compute_weights_ratios :2316,
-// choose_weno_order :2442), edge values (eno_cvt :884).  Sums use the symmetric pairwise
-// order of get_sum_of_elements.  The SMONO indicator is taken as 0 (pure WENO output).
+// WENO3 lower-order weights, weight-ratio stencil reduction (compute_weights_ratios :2311,
+// choose_weno_order :2442) raised by the momentum-flux jump of the cell
+// (apply_additional_reduction_to_weights :795, dP of compute_df_line_new interpline.c:3557),
+// edge values (eno_cvt :884), and the SMONO monotonicity indicator of the 5-point polynomial
+// (compute_mono_indicator_point_eno5 interpline.smono.c:517): a monotone cell (indicator 1)
+// takes the 5-point edge values, a partly monotone one blends its WENO5 weights and its
+// output towards them (mono_adjust_unoptimized_weights reconstructeno.c:852).  Sums use the
+// symmetric pairwise order of get_sum_of_elements.
 // eps: WENO_EPSILON = (500 DBL_EPSILON)^2 (desensitising and weight ratios), the same value
 // in both arithmetic types so that the FP32 reconstruction is the FP64 algorithm up to
 // rounding; weps: the epsilon of 1/(beta+eps)^2, which in FP32 is raised to 1e-18 so that its
 // square stays a normal number (it only acts where a normalised beta is below ~1e-18, far
 // under FP32 resolution); tiny: the smallest normal number (divisions by zero sums).
+// smono: SMONO_EPSILON = 500 DBL_EPSILON in both types: the FP32 indicator then switches
+// where the FP64 one does, up to the FP32 rounding of derivatives that are already within
+// ~1e-7 of the stencil's magnitude (data that flat give the same edges either way); small:
+// the reference's SMALL of the type (global.depnmemonics.h:488-493), the guard of the dP
+// denominator.
 template <typename T>
 struct WenoEps;
 template <>
@@ -354,12 +364,16 @@ struct WenoEps<double> {
   static constexpr double eps = (500.0 * 2.220446049250313e-16) * (500.0 * 2.220446049250313e-16);
   static constexpr double weps = eps;
   static constexpr double tiny = 2.2250738585072014e-308;  // DBL_MIN
+  static constexpr double smono = 500.0 * 2.220446049250313e-16;
+  static constexpr double small = 1.e-300;
 };
 template <>
 struct WenoEps<float> {
   static constexpr float eps = (float)((500.0 * 2.220446049250313e-16) * (500.0 * 2.220446049250313e-16));
   static constexpr float weps = 1e-18f;
   static constexpr float tiny = 1.17549435e-38f;  // FLT_MIN
+  static constexpr float smono = (float)(500.0 * 2.220446049250313e-16);
+  static constexpr float small = 1.e-35f;
 };
 
 template <typename T>
@@ -515,16 +529,130 @@ __device__ __forceinline__ void weno3_unopt(const T* u, T* w) {
   w[1] = n2(w[1]);
 }
 
-// left and right edge values of the cell at u, given its neighbours' unoptimised weights
-// (wm at u-2, wp at u+2) for the stencil-reduction ratio
+// SMONO indicator of the cell at y (y[-2..2]): the left and right edge derivatives of orders
+// 1..3 of the 5-point polynomial (order 1 also min-modded with the outer one-sided difference)
+// must agree in sign; the smallest of them against 500 epsilons of the stencil's magnitude
+// gives 0 .. 1 (SMONO_DO_SMOOTH_TRANSITION)
 template <typename T>
-__device__ __forceinline__ void weno5_edges(const T* u, const T* w, const T* wm, const T* wp, T& yl, T& yr) {
+__device__ __forceinline__ T smono_indicator(const T* y) {
+  const T k12 = T(12), k2 = T(2);
+  T ld1 = wdivk<T>(((T(-3) * y[-2] + y[2]) + (T(-10) * y[-1] - T(6) * y[1])) + T(18) * y[0], k12);
+  T ld2 = wdivk<T>(((T(11) * y[-2] - y[2]) + (T(-20) * y[-1] + T(4) * y[1])) + T(6) * y[0], k12);
+  T ld3 = wdivk<T>(((T(-3) * y[-2] - y[2]) + (T(10) * y[-1] + T(6) * y[1])) - T(12) * y[0], k2);
+  T rd1 = wdivk<T>(((-y[-2] + T(3) * y[2]) + (T(6) * y[-1] + T(10) * y[1])) - T(18) * y[0], k12);
+  T rd2 = wdivk<T>(((-y[-2] + T(11) * y[2]) + (T(4) * y[-1] - T(20) * y[1])) + T(6) * y[0], k12);
+  T rd3 = wdivk<T>(((y[-2] + T(3) * y[2]) - (T(6) * y[-1] + T(10) * y[1])) + T(12) * y[0], k2);
+  auto mm = [](T a, T b) -> T { return (a * b <= T(0)) ? T(0) : ((fabs(a) < fabs(b)) ? a : b); };
+  ld1 = mm(ld1, y[-1] - y[-2]);
+  rd1 = mm(rd1, y[2] - y[1]);
+  T minabs = T(sizeof(T) == 8 ? 1.e+100 : 1.e+30);
+  const T m1 = fabs(mm(ld1, rd1)), m2 = fabs(mm(ld2, rd2)), m3 = fabs(mm(ld3, rd3));
+  minabs = (minabs < m1) ? minabs : m1;
+  minabs = (minabs < m2) ? minabs : m2;
+  minabs = (minabs < m3) ? minabs : m3;
+  const T norm = fabs(y[0]) + ((fabs(y[-1]) + fabs(y[1])) + (fabs(y[-2]) + fabs(y[2])));
+  const T cutoff = norm * WenoEps<T>::smono + WenoEps<T>::tiny;
+  T v = wdiv<T>(minabs - T(0), cutoff - T(0));
+  v = (T(1) < v) ? T(1) : v;
+  return (T(0) > v) ? T(0) : v;
+}
+
+// the cell's WENO5 weights as the ratios and the edges use them: equal weights where the
+// cell is monotone (m = 1), the unoptimised weights blended towards equal ones by m
+template <typename T>
+__device__ __forceinline__ void weno5_cell_weights(const T* u, T m, T* w) {
+  if (m == T(1)) {
+    w[0] = w[1] = w[2] = T(1) / T(3);
+    return;
+  }
+  weno5_unopt<T>(u, w);
+  if (m > T(0) && m < T(1)) {
+#pragma unroll
+    for (int s = 0; s < 3; s++) w[s] = (T(1) - m) * w[s] + m * (T(1) / T(3));
+  }
+}
+
+// lower-order fraction of a cell from the ratios of its outer weights to its neighbours' (at
+// distance 2) inner ones
+template <typename T>
+__device__ __forceinline__ T weno_frac(const T* w, const T* wm, const T* wp) {
   const T E = WenoEps<T>::eps;
   T rl = wdiv<T>(w[2] + E, wm[0] + E);
   T rr = wdiv<T>(w[0] + E, wp[2] + E);
   T ratio = fmin(rl, rr);
   T f = wdivk<T>(ratio - T(1.3), T(1.6) - T(1.3));
-  f = fmax(T(0), fmin(f, T(1)));
+  return fmax(T(0), fmin(f, T(1)));
+}
+
+// the strength of the dP reduction of a cell: min((|dP| - 0.25)/0.25, 1), at most 0 where
+// |dP| <= 0.25 (REDUCE_DP_FRACTION = 0.5); the cell's fraction is then raised to its
+// neighbours' scaled by it
+template <typename T>
+__device__ __forceinline__ T weno_dp_strength(T dP) {
+  T ss = wdivk<T>(fabs(dP) - T(0.5) * T(0.5), T(0.5) * T(0.5));
+  return (ss < T(1)) ? ss : T(1);
+}
+template <typename T>
+__device__ __forceinline__ T weno_lof(T f, T fm, T fp, T ss) {
+  T t = ss * fp;
+  T l = (f > t) ? f : t;
+  t = ss * fm;
+  return (l > t) ? l : t;
+}
+
+// the line quantities of one cell for dP (compute_df_line_new): par = |(1 + u_t) u^dir|,
+// veff = sign(sqrt(-g) rho u^dir) par / (sqrt(par) + SMALL),
+// upar = |(u + p + b^2)(|u^dir| u_t) + p + b^2/2 - b^dir b_t|
+template <typename T>
+__device__ __forceinline__ void weno_dp_cell(const T* pr, const Geo<T>& g, T gam, int dir, T& par, T& veff, T& upar) {
+  State<T> q;
+  get_state<T>(pr, g, gam, q);
+  T bcon[4], bcov0;
+  bcon[0] = pr[HARM_B1] * q.ucov[1] + pr[HARM_B2] * q.ucov[2] + pr[HARM_B3] * q.ucov[3];
+#pragma unroll
+  for (int j = 1; j <= 3; j++) bcon[j] = (pr[HARM_B1 - 1 + j] + bcon[0] * q.ucon[j]) / q.ucon[0];
+  bcov0 = g.gcov[0] * bcon[0] + g.gcov[1] * bcon[1] + g.gcov[2] * bcon[2] + g.gcov[3] * bcon[3];
+  const T ud = q.ucon[dir];
+  const T V = g.gdet * pr[HARM_RHO] * ud;
+  const T btt = -bcon[dir] * bcov0;
+  const T ptot = q.pressure + T(0.5) * q.bsq;
+  par = fabs(q.plus1ud0 * ud);
+  veff = copysign(T(1), V) * par / (sqrt(par) + WenoEps<T>::small);
+  upar = fabs((pr[HARM_UU] + q.pressure + q.bsq) * (fabs(ud) * q.ucov[0]) + ptot + btt);
+}
+// dP of a cell from its rho, par, upar and its neighbours' veff, upar
+template <typename T>
+__device__ __forceinline__ T weno_dp(T rho, T par, T upar, T veffm, T veffp, T uparm, T uparp) {
+  const T dv = veffp - veffm;
+  return (fabs(rho * dv * dv) + fabs(uparp - uparm)) / (fabs(rho * par) + fabs(upar) + WenoEps<T>::small);
+}
+
+// the 5-point edge values (c2e_simple_eno reconstructeno.c:984)
+template <typename T>
+__device__ __forceinline__ T weno_edge5(const T* u, bool right) {
+  const T c0 = right ? T(3. / 128.) : T(-5. / 128.), c1 = right ? T(-5. / 32.) : T(15. / 32.), c2 = T(45. / 64.),
+          c3 = right ? T(15. / 32.) : T(-5. / 32.), c4 = right ? T(-5. / 128.) : T(3. / 128.);
+  T s = T(0);
+  s += c0 * u[-2] + c4 * u[2];
+  s += c1 * u[-1] + c3 * u[1];
+  s += c2 * u[0] * T(1);
+  return s;
+}
+
+// left and right edge values of the cell at u from its (mono-adjusted) WENO5 weights w, its
+// final lower-order fraction f and its SMONO indicator m
+template <typename T>
+__device__ __forceinline__ void weno5_edges(const T* u, const T* w, T f, T m, T& yl, T& yr) {
+  T y5l = T(0), y5r = T(0);
+  if (m != T(0)) {
+    y5l = weno_edge5<T>(u, false);
+    y5r = weno_edge5<T>(u, true);
+  }
+  if (m >= T(1)) {
+    yl = y5l;
+    yr = y5r;
+    return;
+  }
   // optimal face weights (order 3)
   T wl[3] = {w[0] * T(1. / 16.), w[1] * T(5. / 8.), w[2] * T(5. / 16.)};
   T wr[3] = {w[0] * T(5. / 16.), w[1] * T(5. / 8.), w[2] * T(1. / 16.)};
@@ -584,8 +712,8 @@ __device__ __forceinline__ void weno5_edges(const T* u, const T* w, const T* wm,
     outl += symsum2(a0, a1);
     outr += symsum2(b0, b1);
   }
-  yl = (T(1) - T(0)) * outl + T(0) * u[0];
-  yr = (T(1) - T(0)) * outr + T(0) * u[0];
+  yl = (T(1) - m) * outl + m * y5l;
+  yr = (T(1) - m) * outr + m * y5r;
 }
 
 }  // namespace hb

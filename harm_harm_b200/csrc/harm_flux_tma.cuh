@@ -77,7 +77,8 @@ __global__ void __launch_bounds__(256, TmaOcc<LIM>::blocks) k_fluxt_tma(Dims d, 
   T* s_y = reinterpret_cast<T*>(smem_raw + TB::RAW_BYTES);
   T* s_el = s_y + NPR * PL;   // [NPR][PE]
   T* s_er = s_el + NPR * PE;  // [NPR][PE]
-  T* s_w = s_er + NPR * PE;   // [NPR][PW][3]
+  T* s_w = s_er + NPR * PE;   // [NPR][PW][4]
+  T* s_dP = s_w + NPR * PW * TL::NW;  // WENO5: dP of the edge cells, [PE]
   __shared__ uint64_t bar;
   __shared__ int s_ok;
   __shared__ double red[8];
@@ -162,96 +163,28 @@ __global__ void __launch_bounds__(256, TmaOcc<LIM>::blocks) k_fluxt_tma(Dims d, 
     }
     __syncthreads();
     if (tid == 0 && tile + gridDim.x < ntiles) issue(tile + gridDim.x);  // the next tile flies now
-    if constexpr (LIM == HARM_LIM_WENO5 && sizeof(T) == 4) {
-      // FP32: two cells per thread on the packed FP32 pipe (harm_weno_f32x2.cuh)
-      constexpr int NU = NPR * (NL - 4) * NT, NU2 = (NU + 1) / 2;
-      for (int idx = tid; idx < NU2; idx += 256) {
-        const int ib = idx + NU2;
-        const bool hasb = ib < NU;
-        int va, ca, ta, vb, cb, tb;
-        split(idx, 2, NL - 4, va, ca, ta);
-        split(hasb ? ib : idx, 2, NL - 4, vb, cb, tb);
-        const T* ya = s_y + va * PL;
-        const T* yb = s_y + vb * PL;
-        F2 u5[5];
+    if constexpr (LIM == HARM_LIM_WENO5) {
+      // dP line quantities of every staged cell from the staged primitives and the
+      // cell-centre metric (staged cells outside the extended grid arrived as zeros; their
+      // metric is the nearest cell's, and they only feed faces outside the face box)
+      const int nLe = (DIR == 1) ? d.n1e : (DIR == 2) ? d.n2e : d.n3e;
+      const int nTe = (DIR == 1) ? d.n2e : d.n1e;
+      for (int idx = tid; idx < PL; idx += 256) {
+        int v, cl, ct;
+        split(idx, 0, NL, v, cl, ct);
+        T pc[NPR];
 #pragma unroll
-        for (int q = 0; q < 5; q++) u5[q] = f2((float)ya[sx(ca - 2 + q, ta)], (float)yb[sx(cb - 2 + q, tb)]);
-        F2 w[3];
-        weno5_unopt_f2(u5 + 2, w);
-        T* wsa = s_w + (va * PW + wx(ca, ta)) * 3;
-        T* wsb = s_w + (vb * PW + wx(cb, tb)) * 3;
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-          float a, b;
-          f2split(w[k], a, b);
-          wsa[k] = (T)a;
-          if (hasb) wsb[k] = (T)b;
-        }
+        for (int p = 0; p < NPR; p++) pc[p] = s_y[p * PL + sx(cl, ct)];
+        const int lext = min(max(l0 - H + cl + ngL, 0), nLe - 1);
+        const int text = min(max(t0 + ct + d.ng, 0), nTe - 1);
+        const int ii = (DIR == 1) ? lext : text, jj = (DIR == 1) ? text : (DIR == 2) ? lext : o + d.ng;
+        Geo<T> g;
+        load_geo<T, GT>(geom + (size_t)HARM_LOC_CENT * HARM_NGF * d.plane, d.plane, (size_t)jj * d.n1e + ii, g);
+        weno_line_cell<DIR, PL, T>(s_el, sx(cl, ct), pc, g, (T)ph.gam);
       }
       __syncthreads();
-      constexpr int NE = NPR * (A + 1) * NT, NE2 = (NE + 1) / 2;
-      for (int idx = tid; idx < NE2; idx += 256) {
-        const int ib = idx + NE2;
-        const bool hasb = ib < NE;
-        int va, ca, ta, vb, cb, tb;
-        split(idx, H - 1, A + 1, va, ca, ta);
-        split(hasb ? ib : idx, H - 1, A + 1, vb, cb, tb);
-        const T* ya = s_y + va * PL;
-        const T* yb = s_y + vb * PL;
-        F2 u5[5];
-#pragma unroll
-        for (int q = 0; q < 5; q++) u5[q] = f2((float)ya[sx(ca - 2 + q, ta)], (float)yb[sx(cb - 2 + q, tb)]);
-        const T* wa = s_w + va * PW * 3;
-        const T* wb = s_w + vb * PW * 3;
-        F2 w[3], wm[3], wp[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-          w[k] = f2((float)wa[wx(ca, ta) * 3 + k], (float)wb[wx(cb, tb) * 3 + k]);
-          wm[k] = f2((float)wa[wx(ca - 2, ta) * 3 + k], (float)wb[wx(cb - 2, tb) * 3 + k]);
-          wp[k] = f2((float)wa[wx(ca + 2, ta) * 3 + k], (float)wb[wx(cb + 2, tb) * 3 + k]);
-        }
-        F2 yl, yr;
-        weno5_edges_f2(u5 + 2, w, wm, wp, yl, yr);
-        float la, lb, ra, rb;
-        f2split(yl, la, lb);
-        f2split(yr, ra, rb);
-        s_el[va * PE + ex(ca, ta)] = (T)la;
-        s_er[va * PE + ex(ca, ta)] = (T)ra;
-        if (hasb) {
-          s_el[vb * PE + ex(cb, tb)] = (T)lb;
-          s_er[vb * PE + ex(cb, tb)] = (T)rb;
-        }
-      }
-    } else if (LIM == HARM_LIM_WENO5) {
-      for (int idx = tid; idx < NPR * (NL - 4) * NT; idx += 256) {
-        int v, c, t;
-        split(idx, 2, NL - 4, v, c, t);
-        const T* y = s_y + v * PL;
-        T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
-        T w[3];
-        weno5_unopt<T>(u5 + 2, w);
-        T* ws = s_w + (v * PW + wx(c, t)) * 3;
-        ws[0] = w[0]; ws[1] = w[1]; ws[2] = w[2];
-      }
-      __syncthreads();
-      for (int idx = tid; idx < NPR * (A + 1) * NT; idx += 256) {
-        int v, c, t;
-        split(idx, H - 1, A + 1, v, c, t);
-        const T* y = s_y + v * PL;
-        T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
-        const T* ws = s_w + v * PW * 3;
-        T w[3], wm[3], wp[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-          w[k] = ws[wx(c, t) * 3 + k];
-          wm[k] = ws[wx(c - 2, t) * 3 + k];
-          wp[k] = ws[wx(c + 2, t) * 3 + k];
-        }
-        T yl, yr;
-        weno5_edges<T>(u5 + 2, w, wm, wp, yl, yr);
-        s_el[v * PE + ex(c, t)] = yl;
-        s_er[v * PE + ex(c, t)] = yr;
-      }
+      weno_dp_edges<A, NT, H, PL, T>(s_el, s_dP, tid, sx, ex, split);
+      weno_tile_edges<NPR, A, NT, H, NL, PL, PE, PW, T>(s_y, s_w, s_el, s_er, s_dP, tid, sx, ex, wx, split);
     } else if (LIM == HARM_LIM_PARA) {
       for (int idx = tid; idx < NPR * (A + 1) * NT; idx += 256) {
         int v, c, t;

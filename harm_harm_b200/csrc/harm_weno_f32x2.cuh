@@ -1,8 +1,8 @@
 // harm_weno_f32x2.cuh -- the FP32 WENO5 weights and edge values of two cells at once on
 // Blackwell's packed FP32 pipe (add/mul/fma on float2: one instruction, two lanes).
 //
-// The arithmetic is that of weno5_unopt / weno3_unopt / weno5_edges for T = float
-// (harm_device.cuh), lane by lane; operations without a packed form (reciprocals, compares,
+// The arithmetic is that of smono_indicator / weno5_cell_weights / weno3_unopt / weno_frac /
+// weno5_edges for T = float (harm_device.cuh), lane by lane; operations without a packed form (reciprocals, compares,
 // selects, min/max) run on each lane.  Where the scalar code branches on f > 0 (the WENO3
 // blend of the stencil reduction), the packed code evaluates the blend for both lanes when
 // either needs it: with f = 0 it multiplies by 1 and adds zeros, so a lane's value is the
@@ -119,13 +119,70 @@ __device__ __forceinline__ void weno3_unopt_f2(const F2* u, F2* w) {
 // no later sum can tell apart), so the packed path multiplies (and fuses the sums).
 __device__ __forceinline__ F2 nz_mul(F2 wgt, F2 x) { return wgt * x; }
 
-// weno5_edges of two cells
-__device__ __forceinline__ void weno5_edges_f2(const F2* u, const F2* w, const F2* wm, const F2* wp, F2& yl, F2& yr) {
+// smono_indicator<float> of two cells: the derivative combinations on the packed pipe, the
+// min-mods and clamps per lane
+__device__ __forceinline__ F2 smono_indicator_f2(const F2* y) {
+  const F2 r12 = f2(1.0f / 12.0f), h = f2(0.5f);
+  const F2 ld1 = (((f2(-3.f) * y[-2] + y[2]) + (f2(-10.f) * y[-1] - f2(6.f) * y[1])) + f2(18.f) * y[0]) * r12;
+  const F2 ld2 = (((f2(11.f) * y[-2] - y[2]) + (f2(-20.f) * y[-1] + f2(4.f) * y[1])) + f2(6.f) * y[0]) * r12;
+  const F2 ld3 = (((f2(-3.f) * y[-2] - y[2]) + (f2(10.f) * y[-1] + f2(6.f) * y[1])) - f2(12.f) * y[0]) * h;
+  const F2 rd1 = (((y[2] * f2(3.f) - y[-2]) + (f2(6.f) * y[-1] + f2(10.f) * y[1])) - f2(18.f) * y[0]) * r12;
+  const F2 rd2 = (((y[2] * f2(11.f) - y[-2]) + (f2(4.f) * y[-1] - f2(20.f) * y[1])) + f2(6.f) * y[0]) * r12;
+  const F2 rd3 = (((y[-2] + f2(3.f) * y[2]) - (f2(6.f) * y[-1] + f2(10.f) * y[1])) + f2(12.f) * y[0]) * h;
+  const F2 d1l = y[-1] - y[-2], d1r = y[2] - y[1];
+  auto one = [](float y0, float ym1, float yp1, float ym2, float yp2, float l1, float l2, float l3, float r1, float r2,
+                float r3, float dl, float dr) {
+    auto mm = [](float a, float b) { return (a * b <= 0.0f) ? 0.0f : ((fabsf(a) < fabsf(b)) ? a : b); };
+    l1 = mm(l1, dl);
+    r1 = mm(r1, dr);
+    const float minabs = fminf(fminf(fabsf(mm(l1, r1)), fabsf(mm(l2, r2))), fabsf(mm(l3, r3)));
+    const float norm = fabsf(y0) + ((fabsf(ym1) + fabsf(yp1)) + (fabsf(ym2) + fabsf(yp2)));
+    const float v = __fdividef(minabs, norm * WenoEps<float>::smono + WenoEps<float>::tiny);
+    return fmaxf(fminf(v, 1.0f), 0.0f);
+  };
+  return f2(one(y[0].x, y[-1].x, y[1].x, y[-2].x, y[2].x, ld1.x, ld2.x, ld3.x, rd1.x, rd2.x, rd3.x, d1l.x, d1r.x),
+            one(y[0].y, y[-1].y, y[1].y, y[-2].y, y[2].y, ld1.y, ld2.y, ld3.y, rd1.y, rd2.y, rd3.y, d1l.y, d1r.y));
+}
+
+// weno5_cell_weights<float> of two cells: (1 - m) w + m/3 is w itself for m = 0 and exactly
+// 1/3 for m = 1 (finite w), so both lanes take the blend; the unoptimised weights are skipped
+// when both cells are monotone
+__device__ __forceinline__ void weno5_cell_weights_f2(const F2* u, F2 m, F2* w) {
+  if (m.x == 1.0f && m.y == 1.0f) {
+    w[0] = w[1] = w[2] = f2(1.0f / 3.0f);
+    return;
+  }
+  weno5_unopt_f2(u, w);
+  const F2 omm = f2(1.0f) - m, mt = m * f2(1.0f / 3.0f);
+#pragma unroll
+  for (int s = 0; s < 3; s++) w[s] = ffma2(omm, w[s], mt);
+}
+
+// weno_frac<float> of two cells
+__device__ __forceinline__ F2 weno_frac_f2(const F2* w, const F2* wm, const F2* wp) {
   const F2 E = f2(WenoEps<float>::eps);
   const F2 rl = (w[2] + E) * rcp2(wm[0] + E);  // the weight ratios: a fast reciprocal per lane
   const F2 rr = (w[0] + E) * rcp2(wp[2] + E);
   const F2 ratio = lanes(rl, rr, [](float a, float b) { return fminf(a, b); });
-  const F2 f = lanes((ratio - f2(1.3f)) * f2(1.0f / (1.6f - 1.3f)), [](float a) { return fmaxf(0.0f, fminf(a, 1.0f)); });
+  return lanes((ratio - f2(1.3f)) * f2(1.0f / (1.6f - 1.3f)), [](float a) { return fmaxf(0.0f, fminf(a, 1.0f)); });
+}
+
+// weno5_edges<float> of two cells from their weights w, final lower-order fractions f and
+// SMONO indicators m.  (1 - m) out + m y5 is out for m = 0 and y5 for m = 1 (finite out), so
+// the packed code blends both lanes; it skips the WENO sums when both cells are monotone and
+// the 5-point values when neither is partly monotone.
+__device__ __forceinline__ void weno5_edges_f2(const F2* u, const F2* w, F2 f, F2 m, F2& yl, F2& yr) {
+  F2 y5l = f2(0.0f), y5r = f2(0.0f);
+  if (m.x != 0.0f || m.y != 0.0f) {
+    const F2 c0 = f2(-5.f / 128.f), c1 = f2(15.f / 32.f), c2 = f2(45.f / 64.f), c3 = f2(-5.f / 32.f), c4 = f2(3.f / 128.f);
+    y5l = ffma2(c2, u[0], ffma2(c1, u[-1], c3 * u[1]) + ffma2(c0, u[-2], c4 * u[2]));
+    y5r = ffma2(c2, u[0], ffma2(c3, u[-1], c1 * u[1]) + ffma2(c4, u[-2], c0 * u[2]));
+    if (m.x >= 1.0f && m.y >= 1.0f) {
+      yl = y5l;
+      yr = y5r;
+      return;
+    }
+  }
   F2 wl[3] = {w[0] * f2(1.f / 16.f), w[1] * f2(5.f / 8.f), w[2] * f2(5.f / 16.f)};
   F2 wr[3] = {w[0] * f2(5.f / 16.f), w[1] * f2(5.f / 8.f), w[2] * f2(1.f / 16.f)};
   const F2 nl = rcp2(symsum3(wl[0], wl[1], wl[2]) + f2(WenoEps<float>::tiny));
@@ -174,8 +231,9 @@ __device__ __forceinline__ void weno5_edges_f2(const F2* u, const F2* w, const F
     outl = outl + ffma2(l3[0], rl0, nz_mul(l3[1], rl1));
     outr = outr + ffma2(r3[0], rr0, nz_mul(r3[1], rr1));
   }
-  yl = outl;
-  yr = outr;
+  const F2 omm = f2(1.0f) - m;
+  yl = ffma2(omm, outl, m * y5l);
+  yr = ffma2(omm, outr, m * y5r);
 }
 
 }  // namespace hb
