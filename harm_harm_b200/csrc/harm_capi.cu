@@ -358,6 +358,17 @@ extern "C" int harm_b200_utoprimgen_points(harm_ctx* c, size_t n, int guess, con
   return 0;
 }
 
+namespace {
+// CUDA events destroyed on every exit path of the function that holds them
+struct StageEvents {
+  cudaEvent_t ev[6];
+  int made = 0;
+  ~StageEvents() {
+    for (int q = 0; q < made; q++) cudaEventDestroy(ev[q]);
+  }
+};
+}  // namespace
+
 // Stage times of one substep (substep 0 of the RK2 step on d_P; results into scratch).
 extern "C" int harm_b200_time_stages(harm_ctx* c, int precision, int guess, const double* d_P, double dt, int reps,
                                      double* ms) {
@@ -365,8 +376,9 @@ extern "C" int harm_b200_time_stages(harm_ctx* c, int precision, int guess, cons
   static const double Cun[4] = {0.0, 0.0, 0.0, 0.0};
   if (int rc = check_guess(c, guess)) return rc;
   if (reps < 1) reps = 1;
-  cudaEvent_t ev[6];
-  for (int q = 0; q < 6; q++) CK(cudaEventCreate(&ev[q]));
+  StageEvents se;
+  cudaEvent_t* ev = se.ev;
+  for (; se.made < 6; se.made++) CK(cudaEventCreate(&ev[se.made]));
   c->h_scal[0] = dt;
   CK(cudaMemcpyAsync(c->d_dt, c->h_scal, sizeof(double), cudaMemcpyHostToDevice, c->stream));
   for (int q = 0; q < 5; q++) ms[q] = 0.0;
@@ -401,6 +413,5 @@ extern "C" int harm_b200_time_stages(harm_ctx* c, int precision, int guess, cons
   }
   CK(cudaMemsetAsync(c->d_dtslots, 0xFF, 6 * sizeof(unsigned long long), c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  for (int q = 0; q < 6; q++) cudaEventDestroy(ev[q]);
   return check_status(c);
 }

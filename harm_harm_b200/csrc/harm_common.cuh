@@ -9,6 +9,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <atomic>
 #include <stdio.h>
 #include <string.h>
 #include "harm_b200.h"
@@ -26,6 +27,22 @@ int hb_seterr(const char* what, cudaError_t e);
     cudaError_t e_ = (call);                            \
     if (e_ != cudaSuccess) return hb_seterr(#call, e_); \
   } while (0)
+
+// Raise kernel `fn`'s dynamic shared-memory limit to `smem` bytes on the current device, once
+// per device.  `done` is that kernel's own set of devices already raised (one bit per device
+// index, so indices of 64 and above are refused); host threads that drive different devices
+// may call this concurrently (the attribute write itself is idempotent).
+static inline cudaError_t raise_smem_limit_once(std::atomic<unsigned long long>& done, const void* fn, int smem) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  const unsigned long long bit = 1ull << dev;
+  if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_acq_rel);
+  return e;
+}
 
 // ------------------------------------------------------------------ indexing helpers
 
@@ -669,16 +686,9 @@ static inline cudaError_t launch_fluxt(const Dims& d, const Phys& ph, const Face
                                        const GT* geom, T* F, unsigned long long* dtslot, cudaStream_t st) {
   constexpr size_t smem = FluxTile<LIM, T>::smem;
   if (smem > 48 * 1024) {
-    static unsigned long long attr_devices = 0;  // per instantiation: devices already raised
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    static std::atomic<unsigned long long> raised{0};  // per instantiation
+    cudaError_t e = raise_smem_limit_once(raised, (const void*)k_fluxt<DIR, LIM, T, GT>, (int)smem);
     if (e != cudaSuccess) return e;
-    const unsigned long long bit = 1ull << (dev & 63);
-    if (!(attr_devices & bit)) {
-      e = cudaFuncSetAttribute(k_fluxt<DIR, LIM, T, GT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-      attr_devices |= bit;
-    }
   }
   k_fluxt<DIR, LIM, T, GT><<<fluxt_grid<DIR, LIM>(fb), 256, smem, st>>>(d, ph, fb, P, geom, F, dtslot);
   return cudaGetLastError();

@@ -377,12 +377,8 @@ int ensure_train_scratch(harm_ctx* c) {
     c->mlp_work_n = (size_t)TR_GRID * MLP_NPARAMS + 2 * TR_GRID + 4;
     CK(cudaMalloc(&c->d_mlp_work, c->mlp_work_n * sizeof(float)));
   }
-  static unsigned long long attr_devices = 0;  // devices on which the limit is raised
-  const unsigned long long bit = 1ull << (c->device & 63);
-  if (!(attr_devices & bit)) {
-    CK(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TR_SMEM));
-    attr_devices |= bit;
-  }
+  static std::atomic<unsigned long long> raised{0};
+  CK(raise_smem_limit_once(raised, (const void*)k_mlp_grad, (int)TR_SMEM));
   return 0;
 }
 

@@ -18,8 +18,9 @@
 //   - calls that overlap on the GPU (concurrent streams, or several host threads) race on
 //     the shared scratch and must be serialised by the caller;
 //   - the first call on a device looks up the device address of the scratch with
-//     cudaGetSymbolAddress (with that device current) and caches it; make that first call
-//     before any stream capture on that device.
+//     cudaGetSymbolAddress (with that device current) and caches it;
+//   - the call is synchronous: it copies the CFL minima back to the host and waits for its
+//     own stream before returning ndt.
 // The kernels are the FP64 path's, compiled the same way (no FMA contraction), so the
 // results equal harm_b200_fluxcalc's.
 #include <mutex>

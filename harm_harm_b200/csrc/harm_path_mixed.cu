@@ -54,12 +54,8 @@ static int launch_fluxt_tma(harm_ctx* c, const Dims& d, const Phys& ph, const Fa
   using TB = TmaBox<DIR, LIM>;
   CUtensorMap map;
   if (int rc = make_p_map(&map, P, d, TB::BX, TB::BY, TB::BZ)) return rc;
-  static unsigned long long attr_devices = 0;  // per instantiation: devices already raised
-  const unsigned long long bit = 1ull << (c->device & 63);
-  if (!(attr_devices & bit)) {
-    CK(cudaFuncSetAttribute(k_fluxt_tma<DIR, LIM, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TB::smem));
-    attr_devices |= bit;
-  }
+  static std::atomic<unsigned long long> raised{0};  // per instantiation
+  CK(raise_smem_limit_once(raised, (const void*)k_fluxt_tma<DIR, LIM, float>, (int)TB::smem));
   constexpr int A = FluxTile<LIM, float>::A, NT = FluxTile<LIM, float>::NT;
   const long long gx = (DIR == 1) ? (fb.cnt[0] + A - 1) / A : (fb.cnt[0] + NT - 1) / NT;
   const long long gy = (DIR == 1) ? (fb.cnt[1] + NT - 1) / NT : (DIR == 2) ? (fb.cnt[1] + A - 1) / A : (fb.cnt[2] + A - 1) / A;

@@ -353,8 +353,9 @@ int harm_b200_dump(harm_ctx *ctx, const double *d_P, const double *d_U, double t
    `stream` (cudaStream_t, NULL for the default stream).  It allocates nothing: the EMF and
    CFL scratch is a file-scope device array that every GPU loading the library holds until
    exit.  Grids above HARM_NOALLOC_MAX_CELLS are rejected (return 2).  All calls share the
-   scratch, so calls that overlap on the GPU race; the first call on a device looks up the
-   scratch address and should come before any stream capture on that device. */
+   scratch, so calls that overlap on the GPU race.  The call is synchronous: it returns ndt on
+   the host, so it waits for its own work on `stream` before returning.  The first call on a
+   device looks up the scratch address (cudaGetSymbolAddress) with that device current. */
 int harm_b200_fluxcalc_noalloc(const harm_grid *g, const double *d_geom, const double *d_pb,
                                double *d_F1, double *d_F2, double *d_F3, double ndt[3],
                                void *stream);
