@@ -11,8 +11,13 @@ device path and the mixed path with the plain guess are timed on the same grid b
 Multi-GPU: the torus update does not shard in this build (one GPU per grid), so
 `--gpus N` runs N independent replicas, one per rank, and reports their aggregate.
 
-`--impl reference` times the CPU restatement of the reference algorithm (oracle/, OpenMP
-on all host cores) on a bounded sample of the same workload.
+`--impl reference` times the reference HARM code itself (built from its sources into
+oracle/_ref/, OpenMP on all host cores, FP64) on a bounded sample of the same workload: the
+192 x 96 x 64 torus with the same reconstruction, flux formula and flux-CT.  At 384 x 192 x 128
+the reference's static arrays need 117 GB of host memory and its initialisation (metric and
+connection per cell) takes some twenty minutes, so its rate per zone-update is measured on
+the grid an eighth that size.  Where that binary is absent or does not fit the host's
+memory, the CPU restatement of the algorithm (oracle/, OpenMP) is timed on a slab instead.
 """
 from __future__ import annotations
 
@@ -157,14 +162,59 @@ def max_over_ranks(x: float, ws: int) -> float:
     return float(t.item())
 
 
+# the reference binary the CPU legs time: the 192x96x64 torus built with MAXBND 6 (the ghost
+# width WENO5BND needs; MC, PPM and PARALINE run on it unchanged)
+REF_SAMPLE = (192, 96, 64, 6)
+REF_STATIC_BYTES = 17.5e9   # its static arrays (bss), which the host must hold
+
+
+def reference_binary_time(args, lim, nsteps) -> dict | None:
+    """Rate of the reference HARM code itself on the host cores (oracle/_ref/): `nsteps` full
+    RK2 steps of the REF_SAMPLE torus after its initialisation and one untimed step.  None
+    where the binary is absent or the host's memory is too small for it."""
+    from oracle import ref as R
+    n1, n2, n3, ng = REF_SAMPLE
+    if not R.available(n1, n2, n3, ng):
+        return None
+    try:
+        mem = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES")
+    except (ValueError, OSError):
+        mem = 0
+    if mem < 1.25 * REF_STATIC_BYTES:
+        return None
+    cores = os.cpu_count() or 1
+    r = R.time_steps(n1, n2, n3, ng, lim, FLUXES[args.flux], nsteps, cores, timeout=1800)
+    return {"value": r["zone_cycles_per_s"], "unit": "zone-updates/s", "cores": cores, "kind": "reference",
+            "sample": f"the reference HARM code (its own sources, OpenMP, FP64) on the {n1}x{n2}x{n3} torus, "
+                      f"{LIMNAME[lim]} + {args.flux} + flux-CT, {r['steps']} full RK2 steps after its init and "
+                      f"one untimed step ({r['seconds']:.1f} s)"}
+
+
 def run_reference(args, ws, rank):
-    """CPU baseline: the oracle restatement with OpenMP on all host cores (rank 0 only)."""
+    """CPU baseline arm (rank 0 only): the reference HARM code on all host cores (a bounded
+    number of steps of the REF_SAMPLE torus), else the oracle restatement on a slab."""
     if rank != 0:
+        return
+    n1, n2, n3, lim = CONFIGS[args.config]
+    lim = LIMS.get(args.lim, lim)
+    ksteps = max(1, min(args.steps, args.ref_max_steps))
+    ref = reference_binary_time(args, lim, ksteps)
+    if ref is not None:
+        line = {
+            "impl": "reference", "metric": METRIC, "value": ref["value"], "unit": "zone-updates/s", "n_gpus": ws,
+            "steps": ksteps, "warmup": 1, "ms_per_step": 1e3 * REF_SAMPLE[0] * REF_SAMPLE[1] * REF_SAMPLE[2]
+            / ref["value"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (the reference's own seeded Fishbone-Moncrief torus)",
+            "config": {"workload": args.config + f"_{LIMNAME[lim]}_{args.flux}_fluxct",
+                       "sample_grid": list(REF_SAMPLE[:3])},
+            "cpu_baseline": ref,
+            "e2e": {"value": ref["value"], "unit": "zone-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
         return
     from harm_harm_b200 import Grid
     from oracle import oracle as O
-    n1, n2, n3, lim = CONFIGS[args.config]
-    lim = LIMS.get(args.lim, lim)
     sn3 = min(n3, args.cpu_sample_n3)
     g = Grid.torus(n1, n2, sn3, lim=lim, fluxmethod=FLUXES[args.flux])
     geom, conn, aux = g.geometry()
@@ -197,7 +247,12 @@ def run_reference(args, ws, rank):
 
 
 def cpu_baseline_sample(args, lim) -> dict:
-    """Bounded timing of the CPU port on a slab of the workload (for our own line)."""
+    """Bounded timing on the host cores for our own line: the reference HARM code on the
+    REF_SAMPLE torus (a few steps), else the CPU port on a slab of the workload."""
+    if args.cpu_baseline == "reference":
+        ref = reference_binary_time(args, lim, args.cpu_ref_steps)
+        if ref is not None:
+            return ref
     from harm_harm_b200 import Grid
     from oracle import oracle as O
     n1, n2, n3, _ = CONFIGS[args.config]
@@ -288,9 +343,25 @@ def divb_max(g, geom_cent_gdet, P):
     return m, m / max(scale, 1e-300)
 
 
+def vector_errors(gc, a, b):
+    """L1 and Linf of the difference of two spatial vector fields relative to the first, each
+    measured by its metric length sqrt(g_ij x^i x^j); gc: CENT metric records [28][1][n2][n1],
+    a, b: [3][n3][n2][n1]"""
+    g11, g12, g13, g22, g23, g33 = gc[4], gc[5], gc[6], gc[7], gc[8], gc[9]
+
+    def length(x):
+        q = (g11 * x[0] * x[0] + g22 * x[1] * x[1] + g33 * x[2] * x[2]
+             + 2.0 * (g12 * x[0] * x[1] + g13 * x[0] * x[2] + g23 * x[1] * x[2]))
+        return np.sqrt(np.maximum(q, 0.0))
+
+    la, ld = length(a), length(a - b)
+    return float(ld.mean() / max(la.mean(), 1e-300)), float(ld.max() / max(la.max(), 1e-300))
+
+
 def run_ours(args, ws, rank, local):
     import torch
-    from harm_harm_b200 import HARM_GUESS_MLP, HARM_GUESS_PREV, HARM_PREC_FP64, HARM_PREC_MIXED, Grid, Harm
+    from harm_harm_b200 import (HARM_GUESS_MLP, HARM_GUESS_PREV, HARM_PREC_FP64, HARM_PREC_FP64_FMA, HARM_PREC_MIXED,
+                                Grid, Harm)
     torch.cuda.set_device(local)
     n1, n2, n3, lim = CONFIGS[args.config]
     lim = LIMS.get(args.lim, lim)
@@ -327,10 +398,15 @@ def run_ours(args, ws, rank, local):
         ms = e0.elapsed_time(e1)
         return ms, st, dev.launches - l0
 
-    # plain FP64 path on the same grid
+    # plain FP64 path on the same grid: the FP64 build at its best speed (FMA contraction,
+    # shared reciprocals in the inversion) is the denominator of the speed-up; the
+    # IEEE-ordered FP64 build (the one the parity tests pin) is timed beside it
     Pf = Pd.clone()
     k64 = max(1, args.steps // 2)
-    ms64, st64, _ = timed(HARM_PREC_FP64, HARM_GUESS_PREV, Pf, k64, args.warmup)
+    ms64, st64, _ = timed(HARM_PREC_FP64_FMA, HARM_GUESS_PREV, Pf, k64, args.warmup)
+    Pf.copy_(Pd)
+    k64i = max(1, args.steps // 8)
+    ms64i, _, _ = timed(HARM_PREC_FP64, HARM_GUESS_PREV, Pf, k64i, args.warmup)
     del Pf
     # the headline precision with the plain guess
     if guess == HARM_GUESS_MLP:
@@ -347,8 +423,10 @@ def run_ours(args, ws, rank, local):
     th.join(timeout=5)
     ms = max_over_ranks(ms, ws)
     ms64 = max_over_ranks(ms64, ws)
+    ms64i = max_over_ranks(ms64i, ws)
     value = ws * zones * args.steps / (ms * 1e-3)
     value64 = ws * zones * k64 / (ms64 * 1e-3)
+    value64i = ws * zones * k64i / (ms64i * 1e-3)
     if guess == HARM_GUESS_MLP:
         msp = max_over_ranks(msp, ws)
         value_prev = ws * zones * args.steps / (msp * 1e-3)
@@ -363,6 +441,18 @@ def run_ours(args, ws, rank, local):
     fields = (("rho", 0), ("u", 1), ("U1", 2), ("U2", 3), ("U3", 4), ("B1", 5), ("B2", 6), ("B3", 7))
     l1 = {nm: float(np.abs(a[pl] - b[pl]).mean() / max(np.abs(a[pl]).mean(), 1e-300)) for nm, pl in fields}
     linf = {nm: float(np.abs(a[pl] - b[pl]).max() / max(np.abs(a[pl]).max(), 1e-300)) for nm, pl in fields}
+    # the velocity and field vectors measured by their length in the metric (|x|^2 = g_ij x^i x^j
+    # at the cell centre): a component that is small where the vector is not (u~^2, B^3 of a
+    # poloidal loop) is judged against the vector it belongs to
+    gc = geom[0][:, g.active[1], g.active[2]][:, None]
+    for nm, p0 in (("U_vec", 2), ("B_vec", 5)):
+        l1[nm], linf[nm] = vector_errors(gc, a[p0:p0 + 3], b[p0:p0 + 3])
+    # the round-off floor of the same evolution: the FP64 build with FMA contraction against
+    # the IEEE-ordered one
+    Pb.copy_(Pd)
+    dev.step_ch(Pb, dt0, precision=HARM_PREC_FP64_FMA, nsteps=args.err_steps, stats=False)
+    c = Pb.cpu().numpy()[act]
+    l1_fma = {nm: float(np.abs(a[pl] - c[pl]).mean() / max(np.abs(a[pl]).mean(), 1e-300)) for nm, pl in fields[:2]}
     del Pa, Pb
     # stage times and roofline of the dominant kernels
     stages = dev.time_stages(Pm, dt0, precision=prec, guess=guess, reps=3)
@@ -405,8 +495,11 @@ def run_ours(args, ws, rank, local):
                        "l2": "inputs larger than L2 (P is %.0f MB)" % (pbytes / 1e6),
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
             "fp64_value": value64, "speedup_vs_fp64": value / value64,
+            "fp64_of": "FP64 everywhere, FMA contraction and shared reciprocals (HARM_PREC_FP64_FMA)",
+            "fp64_ieee_value": value64i, "speedup_vs_fp64_ieee": value / value64i,
             "plain_guess_value": value_prev if guess == HARM_GUESS_MLP else value,
             "l1_rel_err_vs_fp64": l1, "linf_rel_err_vs_fp64": linf, "err_steps": args.err_steps,
+            "l1_rel_err_fp64_fma_vs_fp64": l1_fma,
             "divb_max": {"abs": divb_abs, "rel": divb_rel,
                          "of": "Toth corner divergence of sqrt(-g) B after the timed steps, rel to max|sqrt(-g) B|/min dx"},
             "newton_iters_per_cell": st["newton_iters"] / ninv,
@@ -414,6 +507,9 @@ def run_ours(args, ws, rank, local):
             / max((stp if guess == HARM_GUESS_MLP else st)["cells_inverted"], 1.0),
             "newton_iters_per_cell_fp64": st64["newton_iters"] / max(st64["cells_inverted"], 1.0),
             "mlp_fallback_rate": st["mlp_fallbacks"] / ninv, "inversion_failures": st["inversion_failures"],
+            "mlp_start_rate": st["mlp_cells"] / ninv,
+            "mlp_engine": os.environ.get("HARM_B200_MLP_ENGINE", "gated"),
+            "mlp_gate": float(os.environ.get("HARM_B200_MLP_GATE", "0.02")),
             "learned_guess": mlp_info,
             "stage_ms": stages,
             "roofline": {"bound": "hbm", "kernel": "k_fluxt (WENO5/PPM/MC reconstruction + HLL, 3 directions)",
@@ -448,7 +544,7 @@ def run_ours(args, ws, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="torus3d_384x192x128", choices=list(CONFIGS))
@@ -461,7 +557,11 @@ def main():
     ap.add_argument("--train-iters", type=int, default=15000, help="Adam steps of the training")
     ap.add_argument("--start-bias", type=float, default=0.0, help="added to the predicted log(W'/D)")
     ap.add_argument("--seed", type=int, default=12345)
-    ap.add_argument("--err-steps", type=int, default=10)
+    ap.add_argument("--err-steps", type=int, default=100, help="steps of the mixed-vs-FP64 error measurement")
+    ap.add_argument("--cpu-baseline", default="reference", choices=["reference", "port"],
+                    help="what our line's cpu_baseline times: the reference binary, or the CPU port")
+    ap.add_argument("--cpu-ref-steps", type=int, default=3, help="reference steps timed for cpu_baseline")
+    ap.add_argument("--ref-max-steps", type=int, default=10, help="at most this many reference steps per run")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--cpu-sample-n3", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")

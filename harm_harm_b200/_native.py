@@ -10,7 +10,7 @@ LIBDIR = os.environ.get("HARM_B200_LIBDIR") or os.path.join(HERE, "lib")
 HARM_NPR = 8
 HARM_LIM_MC, HARM_LIM_PARA, HARM_LIM_WENO5, HARM_LIM_PARALINE = 0, 1, 2, 3
 HARM_FLUX_HLL, HARM_FLUX_LAXF = 0, 1
-HARM_PREC_FP64, HARM_PREC_MIXED = 0, 1
+HARM_PREC_FP64, HARM_PREC_MIXED, HARM_PREC_FP64_FMA = 0, 1, 2
 HARM_GUESS_PREV, HARM_GUESS_MLP = 0, 1
 HARM_LOC_CENT, HARM_LOC_FACE1, HARM_LOC_FACE2, HARM_LOC_CORN3 = 0, 1, 2, 3
 HARM_NLOC = 4
@@ -39,7 +39,7 @@ class harm_grid(C.Structure):
 class harm_stats(C.Structure):
     _fields_ = [("newton_iters", C.c_double), ("cells_inverted", C.c_double),
                 ("mlp_fallbacks", C.c_double), ("inversion_failures", C.c_double),
-                ("floor_hits", C.c_double)]
+                ("floor_hits", C.c_double), ("mlp_cells", C.c_double)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -61,7 +61,12 @@ _DEVICE_SIGS = {
     "harm_b200_fluxcalc": (Ip, [P, Ip, P, P, P, P, C.POINTER(D)]),
     "harm_b200_advance": (Ip, [P, Ip, Ip, Ip, Ip, P, P, P, P, D, C.POINTER(D), C.POINTER(D), C.POINTER(D),
                                C.POINTER(harm_stats)]),
-    "harm_b200_post_fixup": (Ip, [P, P, P]),
+    "harm_b200_post_fixup": (Ip, [P, P, P, Ip]),
+    "harm_b200_from_harm_layout": (Ip, [P, P, P]),
+    "harm_b200_to_harm_layout": (Ip, [P, P, P]),
+    "harm_b200_flags_to_harm": (Ip, [P, P, P, Ip]),
+    "harm_b200_flags_from_harm": (Ip, [P, P, P, Ip]),
+    "harm_b200_step_host_harm": (Ip, [P, Ip, Ip, P, C.POINTER(D), C.POINTER(harm_stats)]),
     "harm_b200_step": (Ip, [P, Ip, Ip, P, C.POINTER(D), C.POINTER(harm_stats)]),
     "harm_b200_step_n": (Ip, [P, Ip, Ip, P, Ip, C.POINTER(D), C.POINTER(harm_stats)]),
     "harm_b200_step_host": (Ip, [P, Ip, Ip, P, C.POINTER(D), C.POINTER(harm_stats)]),

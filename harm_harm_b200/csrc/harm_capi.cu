@@ -39,6 +39,13 @@ static int create_ctx(const harm_grid* g, int device, harm_ctx** out) {
   if (g->lim == HARM_LIM_WENO5 && g->ng < 6) return seterr_msg("WENO5 needs ng >= 6", 2);
   if (g->lim == HARM_LIM_PARALINE && g->ng < 4) return seterr_msg("PARALINE needs ng >= 4", 2);
   if (g->fluxmethod != HARM_FLUX_HLL && g->fluxmethod != HARM_FLUX_LAXF) return seterr_msg("unknown fluxmethod", 2);
+  double mlp_gate = 0.02;  // the gated learned start's threshold (HARM_B200_MLP_GATE)
+  if (const char* e = getenv("HARM_B200_MLP_GATE")) {
+    char* end = nullptr;
+    const double v = strtod(e, &end);
+    if (end == e || !(v >= 0.0)) return seterr_msg("HARM_B200_MLP_GATE is not a non-negative number", 2);
+    mlp_gate = v;
+  }
   harm_ctx* c = new harm_ctx();
   memset((void*)c, 0, sizeof(*c));
   c->g = *g;
@@ -59,6 +66,7 @@ static int create_ctx(const harm_grid* g, int device, harm_ctx** out) {
   }
   CK(cudaMalloc(&c->d_emf, 3 * d.cells * sizeof(double)));
   CK(cudaMalloc(&c->d_emff, 3 * d.cells * sizeof(float)));
+  if (g->lim == HARM_LIM_WENO5) CK(cudaMalloc(&c->d_line, 9 * d.cells * sizeof(double)));
   CK(cudaMalloc(&c->d_pk, NPR * d.cells * sizeof(double)));
   CK(cudaMalloc(&c->d_U, NPR * d.cells * sizeof(double)));
   CK(cudaMalloc(&c->d_rare, (size_t)d.n1 * d.n2 * d.n3 * sizeof(unsigned int)));
@@ -74,6 +82,7 @@ static int create_ctx(const harm_grid* g, int device, harm_ctx** out) {
   c->d_stats = c->d_scal + 16;                          // 5
   c->d_nrec = (unsigned int*)(c->d_scal + 24);
   c->d_nrare = (unsigned int*)(c->d_scal + 25);
+  c->d_nhard = (unsigned int*)(c->d_scal + 26);
   c->d_status = (unsigned int*)(c->d_scal + 28);
   {
     // FP32 flux tiles: plain coalesced loads (default) or TMA ("tma"); both feed the same
@@ -81,13 +90,15 @@ static int create_ctx(const harm_grid* g, int device, harm_ctx** out) {
     // its tile loop, halving the warps that hide the face physics' latency), so it is opt-in.
     const char* e = getenv("HARM_B200_FLUX_STAGING");
     c->flux_tma = (e && strcmp(e, "tma") == 0);
-    // learned start: the mma.sync network as a kernel ahead of the inversion (default) or
-    // inside the inversion kernel ("mma-fused"), the tcgen05 network as a kernel ahead of it
-    // ("tc") or inside the inversion kernel ("tc-fused").  The network's arithmetic is the
-    // same in all four.
+    // learned start: by default ("gated") only for the cells whose previous state is a poor
+    // start, the mma.sync network inside the inversion kernel of those cells; for every
+    // cell: the mma.sync network as a kernel ahead of the inversion ("mma") or inside the
+    // inversion kernel ("mma-fused"), the tcgen05 network as a kernel ahead of it ("tc") or
+    // inside the inversion kernel ("tc-fused").  The network's arithmetic is the same in all.
     const char* m = getenv("HARM_B200_MLP_ENGINE");
     c->mlp_tc = (m && strcmp(m, "tc") == 0) ? 1 : (m && strcmp(m, "tc-fused") == 0) ? 2
-              : (m && strcmp(m, "mma-fused") == 0) ? 3 : 0;
+              : (m && strcmp(m, "mma-fused") == 0) ? 3 : (m && strcmp(m, "mma") == 0) ? 0 : 4;
+    c->mlp_gate = mlp_gate;
     CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
   }
   CK(cudaMemset(c->d_dtslots, 0xFF, 6 * sizeof(unsigned long long)));
@@ -134,7 +145,7 @@ extern "C" int harm_b200_destroy(harm_ctx* c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   void* ptrs[] = {c->d_geom, c->d_geomf, c->d_conn, c->d_aux, c->d_F[0], c->d_F[1], c->d_F[2], c->d_Ff[0], c->d_Ff[1],
-                  c->d_Ff[2], c->d_emf, c->d_emff, c->d_pk, c->d_U, c->d_rare, c->d_pflag, c->d_fixrec, c->d_scal, c->d_Pdev, c->d_mlp, c->d_wpg,
+                  c->d_Ff[2], c->d_emf, c->d_emff, c->d_line, c->d_Paos, c->d_pk, c->d_U, c->d_rare, c->d_pflag, c->d_fixrec, c->d_scal, c->d_Pdev, c->d_mlp, c->d_wpg,
                   c->d_mlp_master, c->d_mlp_adam, c->d_mlp_work};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -158,10 +169,15 @@ extern "C" int harm_b200_bound(harm_ctx* c, double* d_P) { return hp_bound(c, d_
 
 extern "C" int harm_b200_fluxcalc(harm_ctx* c, int precision, const double* d_pb, double* d_F1, double* d_F2,
                                   double* d_F3, double ndt[3]) {
-  if (precision != HARM_PREC_FP64) return seterr_msg("fluxcalc into FP64 arrays needs HARM_PREC_FP64", 2);
+  if (precision != HARM_PREC_FP64 && precision != HARM_PREC_FP64_FMA)
+    return seterr_msg("fluxcalc into FP64 arrays needs HARM_PREC_FP64 or HARM_PREC_FP64_FMA", 2);
   unsigned long long* slots = c->d_dtslots;
   CK(cudaMemsetAsync(slots, 0xFF, 3 * sizeof(unsigned long long), c->stream));
-  if (hp_fluxes_fp64(c, d_pb, d_F1, d_F2, d_F3, c->d_emf, slots)) return 1;
+  if (precision == HARM_PREC_FP64_FMA) {
+    if (hp_fluxes_fp64fma(c, d_pb, d_F1, d_F2, d_F3, c->d_emf, slots)) return 1;
+  } else if (hp_fluxes_fp64(c, d_pb, d_F1, d_F2, d_F3, c->d_emf, slots)) {
+    return 1;
+  }
   if (hp_emf_to_flux_fp64(c, c->d_emf, d_F1, d_F2, d_F3)) return 1;
   unsigned long long hb[3];
   CK(cudaMemcpyAsync(hb, slots, sizeof(hb), cudaMemcpyDeviceToHost, c->stream));
@@ -184,10 +200,17 @@ static int check_guess(harm_ctx* c, int guess) {
 }
 
 // one substep on the device; dt from d_dt, dt minima of this substep into slots
+static int check_precision(int precision) {
+  if (precision != HARM_PREC_FP64 && precision != HARM_PREC_MIXED && precision != HARM_PREC_FP64_FMA)
+    return seterr_msg("unknown precision", 2);
+  return 0;
+}
+
 static int substep(harm_ctx* c, int precision, int guess, int timeorder, int numtimeorders, const double* d_pi,
                    const double* d_pb, double* d_pf, int8_t* d_pflag, const double* CUf, const double* Cunew,
                    unsigned long long* slots, bool with_stats, const SlabWait* sw = nullptr) {
   if (int rc = check_guess(c, guess)) return rc;
+  if (int rc = check_precision(precision)) return rc;
   StepCoef sc;
   sc.CUf0 = CUf[0]; sc.CUf2 = CUf[2];
   sc.Cun0 = Cunew[0]; sc.Cun1 = Cunew[1]; sc.Cun2 = Cunew[2];
@@ -197,6 +220,10 @@ static int substep(harm_ctx* c, int precision, int guess, int timeorder, int num
   if (precision == HARM_PREC_FP64) {
     if (hp_fluxes_fp64(c, d_pb, c->d_F[0], c->d_F[1], c->d_F[2], c->d_emf, slots, sw)) return 1;
     return hp_update_fp64(c, sc, d_pi, d_pb, d_pf, d_pflag, st);
+  }
+  if (precision == HARM_PREC_FP64_FMA) {
+    if (hp_fluxes_fp64fma(c, d_pb, c->d_F[0], c->d_F[1], c->d_F[2], c->d_emf, slots, sw)) return 1;
+    return hp_update_fp64fma(c, sc, d_pi, d_pb, d_pf, d_pflag, st);
   }
   if (hp_fluxes_mixed(c, d_pb, c->d_Ff[0], c->d_Ff[1], c->d_Ff[2], c->d_emff, slots, sw)) return 1;
   return hp_update_mixed(c, sc, d_pi, d_pb, d_pf, d_pflag, st);
@@ -214,10 +241,12 @@ static int check_status(harm_ctx* c) {
   return 0;
 }
 
-static void add_stats(harm_ctx* c, harm_stats* stats, double inverted) {
+static void add_stats(harm_ctx* c, harm_stats* stats, double inverted, int guess) {
   if (!stats) return;
   stats->newton_iters += c->h_scal[8];
   stats->cells_inverted += inverted;
+  // the gated engine counts the cells it gives the learned start; the others give it to all
+  if (guess == HARM_GUESS_MLP) stats->mlp_cells += (c->mlp_tc == 4) ? c->h_scal[9] : inverted;
   stats->mlp_fallbacks += c->h_scal[10];
   stats->inversion_failures += c->h_scal[11];
   stats->floor_hits += c->h_scal[12];
@@ -249,11 +278,13 @@ extern "C" int harm_b200_advance(harm_ctx* c, int precision, int guess, int time
   CK(cudaStreamSynchronize(c->stream));
   if (int rc = check_status(c)) return rc;
   if (ndt) *ndt = c->h_scal[1];
-  add_stats(c, stats, (double)d.n1 * d.n2 * d.n3);
+  add_stats(c, stats, (double)d.n1 * d.n2 * d.n3, guess);
   return 0;
 }
 
-extern "C" int harm_b200_post_fixup(harm_ctx* c, double* d_pf, int8_t* d_pflag) { return hp_fixup(c, d_pf, d_pflag); }
+extern "C" int harm_b200_post_fixup(harm_ctx* c, double* d_pf, int8_t* d_pflag, int finalstep) {
+  return hp_fixup(c, d_pf, d_pflag, finalstep ? 1 : 0);
+}
 
 // enqueue one full RK2 step with dt in d_dt (no host synchronisation)
 // sw: d_P is still arriving in k-slabs (the first substep's flux launches wait for them)
@@ -266,12 +297,12 @@ static int enqueue_step(harm_ctx* c, int precision, int guess, double* d_P, bool
   // bound_prim of p_f and of the flags in one pass (neither depends on the other), post_fixup,
   // bound_prim (post_advance step_ch.c:288-330)
   if (hp_bound(c, c->d_pk, c->d_pflag)) return 1;
-  if (hp_fixup(c, c->d_pk, c->d_pflag, false)) return 1;
+  if (hp_fixup(c, c->d_pk, c->d_pflag, 0, false)) return 1;
   if (hp_bound(c, c->d_pk, nullptr)) return 1;
   if (substep(c, precision, guess, 1, 2, d_P, c->d_pk, d_P, c->d_pflag, CUf[1], Cun[1], c->d_dtslots + 3, with_stats))
     return 1;
   if (hp_bound(c, d_P, c->d_pflag)) return 1;
-  if (hp_fixup(c, d_P, c->d_pflag, false)) return 1;
+  if (hp_fixup(c, d_P, c->d_pflag, 1, false)) return 1;
   if (hp_bound(c, d_P, nullptr)) return 1;
   return hp_finalize_dt(c, c->d_dt, c->d_ndt, 2);
 }
@@ -289,7 +320,7 @@ extern "C" int harm_b200_step_n(harm_ctx* c, int precision, int guess, double* d
   CK(cudaStreamSynchronize(c->stream));
   if (int rc = check_status(c)) return rc;
   *dt = c->h_scal[0];
-  add_stats(c, stats, 2.0 * nsteps * (double)d.n1 * d.n2 * d.n3);
+  add_stats(c, stats, 2.0 * nsteps * (double)d.n1 * d.n2 * d.n3, guess);
   return 0;
 }
 
@@ -300,7 +331,9 @@ extern "C" int harm_b200_step(harm_ctx* c, int precision, int guess, double* d_P
 // H2D of the state in at most HARM_H2D_SLABS slabs of k-planes (one cudaMemcpyAsync per
 // primitive and slab, each slab followed by an event) on the copy stream, after the context
 // stream's earlier work
-static int h2d_slabs(harm_ctx* c, const double* h_P, SlabWait* sw) {
+// harm_layout: h_P is in HARM's [k][j][i][pl] layout (one copy per slab into d_Paos, converted
+// into d_Pdev on the context stream after the slab's event)
+static int h2d_slabs(harm_ctx* c, const double* h_P, SlabWait* sw, bool harm_layout = false) {
   if (!c->copy_stream) {
     CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&c->entry_ev, cudaEventDisableTiming));
@@ -314,39 +347,66 @@ static int h2d_slabs(harm_ctx* c, const double* h_P, SlabWait* sw) {
   for (int s = 0; s < nslab; s++) {
     const int z0 = s * planes, z1 = (z0 + planes < n3e) ? z0 + planes : n3e;
     const size_t off = (size_t)z0 * c->plane, bytes = (size_t)(z1 - z0) * c->plane * sizeof(double);
-    for (int p = 0; p < NPR; p++)
-      CK(cudaMemcpyAsync(c->d_Pdev + (size_t)p * c->cells + off, h_P + (size_t)p * c->cells + off, bytes,
-                         cudaMemcpyHostToDevice, c->copy_stream));
+    if (harm_layout) {
+      CK(cudaMemcpyAsync(c->d_Paos + NPR * off, h_P + NPR * off, NPR * bytes, cudaMemcpyHostToDevice, c->copy_stream));
+    } else {
+      for (int p = 0; p < NPR; p++)
+        CK(cudaMemcpyAsync(c->d_Pdev + (size_t)p * c->cells + off, h_P + (size_t)p * c->cells + off, bytes,
+                           cudaMemcpyHostToDevice, c->copy_stream));
+    }
     CK(cudaEventRecord(c->slab_ev[s], c->copy_stream));
   }
   sw->ev = c->slab_ev;
   sw->nslab = nslab;
   sw->planes = planes;
+  sw->ctx = c;
+  sw->aos = harm_layout ? c->d_Paos : nullptr;
+  sw->soa = c->d_Pdev;
   return 0;
 }
 
 // One full step over a host array: the state goes to the device in k-slabs while the first
 // substep's flux tiles of the slabs already resident run, then the rest of the step, then the
-// state comes back.  Results are those of harm_b200_step on the same state.
-extern "C" int harm_b200_step_host(harm_ctx* c, int precision, int guess, double* h_P, double* dt, harm_stats* stats) {
+// state comes back.  Results are those of harm_b200_step on the same state.  harm_layout: the
+// host array is in HARM's [k][j][i][pl] layout (converted on the device as each slab arrives,
+// and back before the copy out).
+static int step_host(harm_ctx* c, int precision, int guess, double* h_P, double* dt, harm_stats* stats,
+                     bool harm_layout) {
   if (int rc = check_guess(c, guess)) return rc;
+  if (int rc = check_precision(precision)) return rc;
   Dims d = dims_of(c->g);
   const size_t bytes = NPR * c->cells * sizeof(double);
   if (!c->d_Pdev) CK(cudaMalloc(&c->d_Pdev, bytes));
+  if (harm_layout && !c->d_Paos) CK(cudaMalloc(&c->d_Paos, bytes));
   c->h_scal[0] = *dt;
   CK(cudaMemcpyAsync(c->d_dt, c->h_scal, sizeof(double), cudaMemcpyHostToDevice, c->stream));
   if (stats) CK(cudaMemsetAsync(c->d_stats, 0, 5 * sizeof(double), c->stream));
   SlabWait sw;
-  if (int rc = h2d_slabs(c, h_P, &sw)) return rc;
+  if (int rc = h2d_slabs(c, h_P, &sw, harm_layout)) return rc;
   if (enqueue_step(c, precision, guess, c->d_Pdev, stats != nullptr, &sw)) return 1;
-  CK(cudaMemcpyAsync(h_P, c->d_Pdev, bytes, cudaMemcpyDeviceToHost, c->stream));
+  if (harm_layout) {
+    if (hp_soa_to_harm(c, c->d_Pdev, c->d_Paos)) return 1;
+    CK(cudaMemcpyAsync(h_P, c->d_Paos, bytes, cudaMemcpyDeviceToHost, c->stream));
+  } else {
+    CK(cudaMemcpyAsync(h_P, c->d_Pdev, bytes, cudaMemcpyDeviceToHost, c->stream));
+  }
   CK(cudaMemcpyAsync(c->h_scal, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   if (stats) CK(cudaMemcpyAsync(c->h_scal + 8, c->d_stats, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   if (int rc = check_status(c)) return rc;
   *dt = c->h_scal[0];
-  add_stats(c, stats, 2.0 * (double)d.n1 * d.n2 * d.n3);
+  add_stats(c, stats, 2.0 * (double)d.n1 * d.n2 * d.n3, guess);
   return 0;
+}
+
+extern "C" int harm_b200_step_host(harm_ctx* c, int precision, int guess, double* h_P, double* dt, harm_stats* stats) {
+  return step_host(c, precision, guess, h_P, dt, stats, false);
+}
+
+extern "C" int harm_b200_step_host_harm(harm_ctx* c, int precision, int guess, double* h_P, double* dt,
+                                        harm_stats* stats) {
+  if (((uintptr_t)h_P % 16) != 0) return seterr_msg("the HARM-layout array must be 16-byte aligned", 2);
+  return step_host(c, precision, guess, h_P, dt, stats, true);
 }
 
 extern "C" int harm_b200_utoprimgen_points(harm_ctx* c, size_t n, int guess, const double* d_U, const double* d_geom,
@@ -375,6 +435,7 @@ extern "C" int harm_b200_time_stages(harm_ctx* c, int precision, int guess, cons
   static const double CUf[4] = {1.0, 0.0, 0.5, 0.0};
   static const double Cun[4] = {0.0, 0.0, 0.0, 0.0};
   if (int rc = check_guess(c, guess)) return rc;
+  if (int rc = check_precision(precision)) return rc;
   if (reps < 1) reps = 1;
   StageEvents se;
   cudaEvent_t* ev = se.ev;
@@ -389,6 +450,8 @@ extern "C" int harm_b200_time_stages(harm_ctx* c, int precision, int guess, cons
     CK(cudaEventRecord(ev[0], c->stream));
     if (precision == HARM_PREC_FP64) {
       if (hp_fluxes_fp64(c, d_P, c->d_F[0], c->d_F[1], c->d_F[2], c->d_emf, c->d_dtslots)) return 1;
+    } else if (precision == HARM_PREC_FP64_FMA) {
+      if (hp_fluxes_fp64fma(c, d_P, c->d_F[0], c->d_F[1], c->d_F[2], c->d_emf, c->d_dtslots)) return 1;
     } else {
       if (hp_fluxes_mixed(c, d_P, c->d_Ff[0], c->d_Ff[1], c->d_Ff[2], c->d_emff, c->d_dtslots)) return 1;
     }
@@ -396,13 +459,15 @@ extern "C" int harm_b200_time_stages(harm_ctx* c, int precision, int guess, cons
     CK(cudaEventRecord(ev[2], c->stream));
     if (precision == HARM_PREC_FP64) {
       if (hp_update_fp64(c, sc, d_P, d_P, c->d_pk, c->d_pflag, nullptr)) return 1;
+    } else if (precision == HARM_PREC_FP64_FMA) {
+      if (hp_update_fp64fma(c, sc, d_P, d_P, c->d_pk, c->d_pflag, nullptr)) return 1;
     } else {
       if (hp_update_mixed(c, sc, d_P, d_P, c->d_pk, c->d_pflag, nullptr)) return 1;
     }
     CK(cudaEventRecord(ev[3], c->stream));
     if (hp_bound(c, c->d_pk, nullptr)) return 1;
     CK(cudaEventRecord(ev[4], c->stream));
-    if (hp_fixup(c, c->d_pk, c->d_pflag)) return 1;
+    if (hp_fixup(c, c->d_pk, c->d_pflag, 0)) return 1;
     CK(cudaEventRecord(ev[5], c->stream));
     CK(cudaEventSynchronize(ev[5]));
     float t;

@@ -21,7 +21,16 @@
 
 using namespace hb;
 
+// HARM_TU: a tag that keeps the kernel template instantiations of translation units compiled
+// with different arithmetic flags apart (the FP64 path is built twice: without and with FMA
+// contraction); every kernel template takes it as its last, defaulted, parameter.
+#ifndef HARM_TU
+#define HARM_TU 0
+#endif
+
 int hb_seterr(const char* what, cudaError_t e);
+// HARM's [k][j][i][pl] layout -> [pl][k][j][i], planes [k0, k1) (harm_layout.cu)
+int hp_harm_to_soa(harm_ctx* c, const double* aos, double* soa, int k0, int k1);
 #define CK(call)                                        \
   do {                                                  \
     cudaError_t e_ = (call);                            \
@@ -109,6 +118,7 @@ __device__ __forceinline__ void warp_add_atomic(double v, double* slot) {
 struct FixRec {
   long long id;
   double v[5];
+  int flag;  // the cell's flag after the fix
 };
 
 // Cell tiles of the per-cell kernels: a block of 256 threads covers TI consecutive i times TK
@@ -440,10 +450,13 @@ __device__ __forceinline__ double face_hll(const Dims& d, const Phys& ph, const 
 #else
 #define HARM_FLUXT_LB __launch_bounds__(256)
 #endif
-template <int DIR, int LIM, typename T, typename GT>
+// L (WENO5, optional): the dP line quantities of every extended cell from k_cellprep,
+// [3 (DIR-1) + q][cells] for q = par, veff, upar; where null, the kernel computes them.
+template <int DIR, int LIM, typename T, typename GT, int TU = HARM_TU>
 __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double* __restrict__ P,
                                                const GT* __restrict__ geom, T* __restrict__ F,
-                                               unsigned long long* __restrict__ dtslot) {
+                                               unsigned long long* __restrict__ dtslot,
+                                               const T* __restrict__ L = nullptr) {
   using TL = FluxTile<LIM, T>;
   constexpr int A = TL::A, NT = TL::NT, H = TL::H, NL = TL::NL, VB = TL::VB, PL = TL::PLANE, PE = TL::PE, PW = TL::PW;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -536,10 +549,12 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
       s_F[ex(c, t)] = paraline_fi<T>(vv, pp);
     }
   }
-  // WENO5: the line quantities of dP (compute_df_line_new interpline.c:3557) of every staged
-  // cell from all its primitives and the cell-centre metric, into the edge planes, then dP of
-  // each edge cell.  With all primitives staged at once (FP32) this reads the staged tile
-  // below; otherwise (FP64, two groups) it loads them here.
+  // WENO5: the line quantities of dP (compute_df_line_new interpline.c:3557) of the staged
+  // cells H-2 .. H+A (the edge cells and their neighbours along DIR), from all the cell's
+  // primitives and the cell-centre metric, into the edge planes, then dP of each edge cell.
+  // From L where the cell pass computed them; otherwise here: with all primitives staged at
+  // once (FP32) from the staged tile below, else (FP64, two groups) loaded here.
+  constexpr int DPC = A + 3;  // cells with line quantities per line
   auto weno_line = [&](int cl, int ct, const T* pc) {
     const int lext = min(max(l0 - H + cl + ngL, 0), nLe - 1);
     const int text = min(max(t0 + ct + d.ng, 0), nTe - 1);
@@ -548,20 +563,39 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
     load_geo<T, GT>(geom + (size_t)HARM_LOC_CENT * HARM_NGF * d.plane, d.plane, (size_t)jj * d.n1e + ii, g);
     weno_line_cell<DIR, PL, T>(s_el, sx(cl, ct), pc, g, (T)ph.gam);
   };
-  if constexpr (LIM == HARM_LIM_WENO5 && VB < NPR) {
-    for (int idx = tid; idx < PL; idx += 256) {
-      int v, cl, ct;
-      split(idx, 0, NL, v, cl, ct);
-      const int lext = min(max(l0 - H + cl + ngL, 0), nLe - 1);
-      const int text = min(max(t0 + ct + d.ng, 0), nTe - 1);
-      const size_t cid = cell_index(lext, text);
-      T pc[NPR];
+  const bool dp_from_L = (LIM == HARM_LIM_WENO5) && (L != nullptr);
+  if constexpr (LIM == HARM_LIM_WENO5) {
+    if (dp_from_L) {
+      const T* Lq = L + (size_t)3 * (DIR - 1) * d.cells;
+      for (int idx = tid; idx < DPC * NT; idx += 256) {
+        int v, cl, ct;
+        split(idx, H - 2, DPC, v, cl, ct);
+        const int lext = min(max(l0 - H + cl + ngL, 0), nLe - 1);
+        const int text = min(max(t0 + ct + d.ng, 0), nTe - 1);
+        const size_t cid = cell_index(lext, text);
+        const int si = sx(cl, ct);
+        s_el[si] = (T)__ldg(P + (size_t)HARM_RHO * d.cells + cid);
+        s_el[PL + si] = __ldg(Lq + cid);
+        s_el[2 * PL + si] = __ldg(Lq + d.cells + cid);
+        s_el[3 * PL + si] = __ldg(Lq + 2 * d.cells + cid);
+      }
+      __syncthreads();
+      weno_dp_edges<A, NT, H, PL, T>(s_el, s_dP, tid, sx, ex, split);
+    } else if constexpr (VB < NPR) {
+      for (int idx = tid; idx < DPC * NT; idx += 256) {
+        int v, cl, ct;
+        split(idx, H - 2, DPC, v, cl, ct);
+        const int lext = min(max(l0 - H + cl + ngL, 0), nLe - 1);
+        const int text = min(max(t0 + ct + d.ng, 0), nTe - 1);
+        const size_t cid = cell_index(lext, text);
+        T pc[NPR];
 #pragma unroll
-      for (int p = 0; p < NPR; p++) pc[p] = (T)__ldg(P + (size_t)p * d.cells + cid);
-      weno_line(cl, ct, pc);
+        for (int p = 0; p < NPR; p++) pc[p] = (T)__ldg(P + (size_t)p * d.cells + cid);
+        weno_line(cl, ct, pc);
+      }
+      __syncthreads();
+      weno_dp_edges<A, NT, H, PL, T>(s_el, s_dP, tid, sx, ex, split);
     }
-    __syncthreads();
-    weno_dp_edges<A, NT, H, PL, T>(s_el, s_dP, tid, sx, ex, split);
   }
   T pl[NPR], pr[NPR];
 #pragma unroll
@@ -581,16 +615,18 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
     __syncthreads();
     if constexpr (LIM == HARM_LIM_WENO5) {
       if constexpr (VB == NPR) {
-        for (int idx = tid; idx < PL; idx += 256) {
-          int v, cl, ct;
-          split(idx, 0, NL, v, cl, ct);
-          T pc[NPR];
+        if (!dp_from_L) {
+          for (int idx = tid; idx < DPC * NT; idx += 256) {
+            int v, cl, ct;
+            split(idx, H - 2, DPC, v, cl, ct);
+            T pc[NPR];
 #pragma unroll
-          for (int p = 0; p < NPR; p++) pc[p] = s_y[p * PL + sx(cl, ct)];
-          weno_line(cl, ct, pc);
+            for (int p = 0; p < NPR; p++) pc[p] = s_y[p * PL + sx(cl, ct)];
+            weno_line(cl, ct, pc);
+          }
+          __syncthreads();
+          weno_dp_edges<A, NT, H, PL, T>(s_el, s_dP, tid, sx, ex, split);
         }
-        __syncthreads();
-        weno_dp_edges<A, NT, H, PL, T>(s_el, s_dP, tid, sx, ex, split);
       }
       weno_tile_edges<VB, A, NT, H, NL, PL, PE, PW, T>(s_y, s_w, s_el, s_er, s_dP, tid, sx, ex, wx, split);
     } else if (LIM == HARM_LIM_PARA) {
@@ -679,18 +715,58 @@ static inline bool face_box_k(FaceBox b, int klo, int khi, FaceBox* out) {
   return true;
 }
 
+// The cell pass of a WENO5 flux stage: the dP line quantities (par, veff, upar of
+// compute_df_line_new interpline.c:3557) of every extended cell of planes [k0, k1), for the
+// three directions, from one evaluation of the cell's state (get_state) in the arithmetic
+// type T of the flux tiles; L[3 (dir-1) + q][cells].  The tiles of the three directions
+// read them instead of evaluating the state of each staged cell once per direction.
+template <typename T, typename GT, int TU = HARM_TU>
+__global__ void __launch_bounds__(256) k_cellprep(Dims d, Phys ph, const double* __restrict__ P,
+                                                  const GT* __restrict__ geom, T* __restrict__ L, int k0, int k1) {
+  const long long n = (long long)(k1 - k0) * d.plane;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const size_t id = (size_t)k0 * d.plane + (size_t)t;
+  const size_t c2 = (size_t)t % d.plane;
+  T pc[NPR];
+#pragma unroll
+  for (int p = 0; p < NPR; p++) pc[p] = (T)__ldg(P + (size_t)p * d.cells + id);
+  Geo<T> g;
+  load_geo<T, GT>(geom + (size_t)HARM_LOC_CENT * HARM_NGF * d.plane, d.plane, c2, g);
+  State<T> q;
+  get_state<T>(pc, g, (T)ph.gam, q);
+#pragma unroll
+  for (int dir = 1; dir <= 3; dir++) {
+    T par, veff, upar;
+    weno_dp_of_state<T>(pc, g, q, dir, par, veff, upar);
+    L[(size_t)(3 * (dir - 1) + 0) * d.cells + id] = par;
+    L[(size_t)(3 * (dir - 1) + 1) * d.cells + id] = veff;
+    L[(size_t)(3 * (dir - 1) + 2) * d.cells + id] = upar;
+  }
+}
+
+template <typename T, typename GT>
+static inline cudaError_t launch_cellprep(const Dims& d, const Phys& ph, const double* P, const GT* geom, T* L, int k0,
+                                          int k1, cudaStream_t st) {
+  const long long n = (long long)(k1 - k0) * d.plane;
+  if (n <= 0) return cudaSuccess;
+  k_cellprep<T, GT><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d, ph, P, geom, L, k0, k1);
+  return cudaGetLastError();
+}
+
 // launch k_fluxt<DIR, LIM, T, GT>; the first launch of an instantiation on a device raises
 // its dynamic shared-memory limit where the tile needs more than 48 KB (FP32 WENO5: 63 KB)
 template <int DIR, int LIM, typename T, typename GT>
 static inline cudaError_t launch_fluxt(const Dims& d, const Phys& ph, const FaceBox& fb, const double* P,
-                                       const GT* geom, T* F, unsigned long long* dtslot, cudaStream_t st) {
+                                       const GT* geom, T* F, unsigned long long* dtslot, cudaStream_t st,
+                                       const T* L = nullptr) {
   constexpr size_t smem = FluxTile<LIM, T>::smem;
   if (smem > 48 * 1024) {
     static std::atomic<unsigned long long> raised{0};  // per instantiation
     cudaError_t e = raise_smem_limit_once(raised, (const void*)k_fluxt<DIR, LIM, T, GT>, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  k_fluxt<DIR, LIM, T, GT><<<fluxt_grid<DIR, LIM>(fb), 256, smem, st>>>(d, ph, fb, P, geom, F, dtslot);
+  k_fluxt<DIR, LIM, T, GT><<<fluxt_grid<DIR, LIM>(fb), 256, smem, st>>>(d, ph, fb, P, geom, F, dtslot, L);
   return cudaGetLastError();
 }
 
@@ -698,10 +774,12 @@ static inline cudaError_t launch_fluxt(const Dims& d, const Phys& ph, const Face
 // (SlabWait): after each slab's copy, the x1 and x2 faces of its planes (their stencils stay in
 // the plane) and every row of x3 tiles (A faces along k) whose staged planes have all arrived.
 // Same kernels and results as the whole-grid launches.
+// L (WENO5, optional): the cell pass's output buffer; each slab's cell pass runs once the
+// slab has arrived, before the tiles that stage its planes.
 template <int LIM, typename T, typename GT>
 static inline cudaError_t launch_flux_slabs(const Dims& d, const Phys& ph, const double* pb, const GT* geom, T* F1,
                                             T* F2, T* F3, unsigned long long* slots, cudaStream_t st,
-                                            const SlabWait& sw, unsigned long long& launches) {
+                                            const SlabWait& sw, unsigned long long& launches, T* L = nullptr) {
   constexpr int A = FluxTile<LIM, T>::A, X = ReconGeom<LIM>::X;
   const FaceBox b1 = face_box(d, 1), b2 = face_box(d, 2), b3 = face_box(d, 3);
   int f3 = b3.lo[2];  // first x3 face not launched yet
@@ -710,13 +788,20 @@ static inline cudaError_t launch_flux_slabs(const Dims& d, const Phys& ph, const
     if ((e = cudaStreamWaitEvent(st, sw.ev[s], 0)) != cudaSuccess) return e;
     const int resident = (s + 1) * sw.planes;  // planes [0, resident) are on the device
     const int klo = s * sw.planes - d.ng3, khi = resident - 1 - d.ng3;
+    if (sw.aos && hp_harm_to_soa(sw.ctx, sw.aos, sw.soa, s * sw.planes, resident < d.n3e ? resident : d.n3e))
+      return cudaErrorLaunchFailure;
+    if (L) {
+      const int k1 = resident < d.n3e ? resident : d.n3e;
+      if ((e = launch_cellprep<T, GT>(d, ph, pb, geom, L, s * sw.planes, k1, st)) != cudaSuccess) return e;
+      launches++;
+    }
     FaceBox sb;
     if (face_box_k(b1, klo, khi, &sb)) {
-      if ((e = launch_fluxt<1, LIM, T, GT>(d, ph, sb, pb, geom, F1, slots + 0, st)) != cudaSuccess) return e;
+      if ((e = launch_fluxt<1, LIM, T, GT>(d, ph, sb, pb, geom, F1, slots + 0, st, L)) != cudaSuccess) return e;
       launches++;
     }
     if (face_box_k(b2, klo, khi, &sb)) {
-      if ((e = launch_fluxt<2, LIM, T, GT>(d, ph, sb, pb, geom, F2, slots + 1, st)) != cudaSuccess) return e;
+      if ((e = launch_fluxt<2, LIM, T, GT>(d, ph, sb, pb, geom, F2, slots + 1, st, L)) != cudaSuccess) return e;
       launches++;
     }
     // x3 tile rows: a row from face f0 stages planes up to f0 + ng3 + A + X - 1 (clamped)
@@ -725,7 +810,7 @@ static inline cudaError_t launch_flux_slabs(const Dims& d, const Phys& ph, const
       if (top > d.n3e - 1) top = d.n3e - 1;
       if (top >= resident && s + 1 < sw.nslab) break;
       if (face_box_k(b3, f3, f3 + A - 1, &sb)) {
-        if ((e = launch_fluxt<3, LIM, T, GT>(d, ph, sb, pb, geom, F3, slots + 2, st)) != cudaSuccess) return e;
+        if ((e = launch_fluxt<3, LIM, T, GT>(d, ph, sb, pb, geom, F3, slots + 2, st, L)) != cudaSuccess) return e;
         launches++;
       }
       f3 += A;
@@ -736,7 +821,7 @@ static inline cudaError_t launch_flux_slabs(const Dims& d, const Phys& ph, const
 
 // ------------------------------------------------------------------ EMF kernel
 
-template <typename T, typename GT>
+template <typename T, typename GT, int TU = HARM_TU>
 __global__ void __launch_bounds__(256) k_emf(Dims d, const T* __restrict__ F1, const T* __restrict__ F2,
                                              const T* __restrict__ F3, const GT* __restrict__ geom, T* __restrict__ emf) {
   const int has3 = d.n3 > 1;
@@ -945,7 +1030,7 @@ __device__ __forceinline__ void stage_conn_geom(const Dims& d, const double* __r
   }
 }
 
-template <typename T, bool STAGE = false>
+template <typename T, bool STAGE = false, int TU = HARM_TU>
 __global__ void __launch_bounds__(256, HARM_CONSERVED_BLOCKS) k_conserved(Dims d, Phys ph, StepCoef sc, const double* __restrict__ dtp,
                                                       const double* __restrict__ pi, const double* __restrict__ pb,
                                                       const T* __restrict__ F1, const T* __restrict__ F2,
@@ -1001,7 +1086,7 @@ __device__ __forceinline__ void conserved_ab(const StepCoef& sc, double& a, doub
   b = sc.finalstep ? sc.Cun1 + sc.Cun2 * sc.CUf2 : sc.CUf2;
 }
 
-template <typename T, bool STAGE>
+template <typename T, bool STAGE, int TU = HARM_TU>
 __global__ void __launch_bounds__(256, HARM_CONSERVED_SRC_BLOCKS) k_conserved_src(Dims d, Phys ph, StepCoef sc, const double* __restrict__ dtp,
                                                       const double* __restrict__ pi, const double* __restrict__ pb,
                                                       const double* __restrict__ geom, const double* __restrict__ conn,
@@ -1037,7 +1122,7 @@ __global__ void __launch_bounds__(256, HARM_CONSERVED_SRC_BLOCKS) k_conserved_sr
   for (int p = 0; p < NPR; p++) Uout[(size_t)p * d.cells + id] = a * Ui[p] + bdt * dUg[p];
 }
 
-template <typename T>
+template <typename T, int TU = HARM_TU>
 __global__ void __launch_bounds__(256) k_conserved_div(Dims d, Phys ph, StepCoef sc, const double* __restrict__ dtp,
                                                       const T* __restrict__ F1, const T* __restrict__ F2,
                                                       const T* __restrict__ F3, const T* __restrict__ emf,
@@ -1132,6 +1217,57 @@ __global__ void __launch_bounds__(256, HARM_INVERT_BLOCKS) k_invert(Dims d, Phys
     warp_add_atomic(iters_d, stats + 0);
     if (GUESS) warp_add_atomic(fb_d, stats + 2);
   }
+}
+
+// The gated learned start, first kernel: the plain inversion of k_invert (the same operations
+// from the previous-state W'), except that a cell whose first Newton step exceeds `gate` of
+// the convergence scale (its previous state is a poor start: a floored cell, a shock, a cold
+// start) stops after that step and is appended to the list `hard`; k_invert_hard then solves
+// it from the learned start.  Every other cell's result is the plain path's, bit for bit.
+template <int PATH>
+__global__ void __launch_bounds__(256, HARM_INVERT_BLOCKS) k_invert_gated(Dims d, Phys ph, const double* __restrict__ U,
+                                                   const double* __restrict__ pb, double* __restrict__ pf,
+                                                   int8_t* __restrict__ pflag, const double* __restrict__ geom,
+                                                   const double* __restrict__ aux, unsigned int* __restrict__ rare,
+                                                   unsigned int* __restrict__ nrare, double* __restrict__ stats,
+                                                   CellTile ct, double gate, unsigned int* __restrict__ hard,
+                                                   unsigned int* __restrict__ nhard) {
+  double iters_d = 0.0;
+  int i, j, k;
+  if (tile_cell(d.n1, d.n2, d.n3, ct, blockIdx.x, blockIdx.y, blockIdx.z, i, j, k)) {
+    const long long t = i + (long long)d.n1 * (j + (long long)d.n2 * k);
+    const int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
+    const size_t id = cidx(d, ii, jj, kk), c2 = (size_t)jj * d.n1e + ii;
+    Geo<double> g;
+    load_geo<double, double>(geom, d.plane, c2, g);
+    double Ugf[NPR], pr[NPR];
+#pragma unroll
+    for (int p = 0; p < NPR; p++) { Ugf[p] = U[(size_t)p * d.cells + id] * g.igdet; pr[p] = pb[(size_t)p * d.cells + id]; }
+    int8_t flag = 0;
+    int it = 0;
+    JonSetup s;
+    jon_prepare(false, Ugf, g, pr, ph.gam, ph.gammafail, s);
+    const bool poor = jon_solve<true>(s, s.Wp_prev, pr, flag, it, nullptr, gate);
+    iters_d = (double)it;
+    if (poor) {
+      hard[atomicAdd(nhard, 1u)] = (unsigned int)t;
+    } else {
+      bool defer = (flag != 0);
+      if (!defer) {
+        double rhofl = __ldg(aux + (size_t)HARM_AUX_RHOFLOOR * d.plane + c2);
+        double ufl = __ldg(aux + (size_t)HARM_AUX_UFLOOR * d.plane + c2);
+        rhofl = (rhofl < kSMALL) ? kSMALL : rhofl;
+        ufl = (ufl < kSMALL) ? kSMALL : ufl;
+        defer = (rhofl > pr[HARM_RHO]) || (ufl > pr[HARM_UU]);
+        if (!defer) limit_gamma<double>(ph.gammamax, pr, g);
+      }
+      if (defer) rare[atomicAdd(nrare, 1u)] = (unsigned int)t;
+      pflag[id] = flag;
+#pragma unroll
+      for (int p = 0; p < NPR; p++) pf[(size_t)p * d.cells + id] = pr[p];
+    }
+  }
+  if (stats) warp_add_atomic(iters_d, stats + 0);
 }
 
 // The learned start of the inversion, one kernel before k_invert: per cell the
@@ -1240,7 +1376,7 @@ __global__ void __launch_bounds__(128) k_invert_rare(Dims d, Phys ph, const doub
 }
 
 // field fluxes of the faces of active cells from the EMFs (for the standalone fluxcalc)
-template <typename T>
+template <typename T, int TU = HARM_TU>
 __global__ void k_emf_to_flux(Dims d, const T* __restrict__ emf, T* F1, T* F2, T* F3) {
   const int has3 = d.n3 > 1;
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;

@@ -8,11 +8,17 @@
 // an event the first substep's flux launches of that slab wait for
 #define HARM_H2D_SLABS 8
 
+struct harm_ctx;
+
 // which copy event each k-plane's flux launches wait for (planes [s*planes, (s+1)*planes) of
-// the extended grid arrive with ev[s])
+// the extended grid arrive with ev[s]); with aos set, the slabs arrive in HARM's
+// [k][j][i][pl] layout there and are converted into soa after their event
 struct SlabWait {
   const cudaEvent_t* ev;
   int nslab, planes;
+  harm_ctx* ctx;
+  const double* aos;
+  double* soa;
 };
 
 struct harm_ctx {
@@ -33,6 +39,8 @@ struct harm_ctx {
   float* d_Ff[3];
   double* d_emf;
   float* d_emff;
+  void* d_line;     // WENO5: dP line quantities of the flux stage's cell pass, [9][cells] (FP64
+                    // path: double, mixed path: float)
   double* d_pk;     // midpoint primitives of the RK2 step
   double* d_U;      // conserved variables to invert (UEVOLVE)
   unsigned int* d_rare;   // cells finished by the rare inversion path
@@ -49,6 +57,7 @@ struct harm_ctx {
   unsigned int* d_nrec;
   double* h_scal;   // pinned host mirror
   double* d_Pdev;   // device state used by the host-buffer entry point
+  double* d_Paos;   // the same in HARM's [k][j][i][pl] layout (harm_b200_step_host_harm)
   // learned guess
   float* d_mlp;        // inference records (MlpPacked for mma.sync, then MlpTc for tcgen05)
   double* d_wpg;       // learned starting W' of each active cell (k_mlp_guess)
@@ -60,11 +69,16 @@ struct harm_ctx {
   unsigned int* d_status; // device error word (bit 0: a TMA tile wait timed out, bit 1: a
                           // tensor-core MMA wait of the learned start timed out)
   int flux_tma;            // stage the FP32 flux tiles with TMA (HARM_B200_FLUX_STAGING=tma)
-  int mlp_tc;              // learned start: 0 mma.sync network kernel ahead of the inversion
-                           // (default), 1 tcgen05 network kernel ahead of it
-                           // (HARM_B200_MLP_ENGINE=tc), 2 tcgen05 inside the inversion
-                           // kernel (=tc-fused), 3 mma.sync inside the inversion kernel
-                           // (=mma-fused)
+  int mlp_tc;              // learned start: 4 gated (default: the network, fused with the
+                           // inversion, only for cells whose previous state is a poor start),
+                           // or for every cell: 0 mma.sync network kernel ahead of the
+                           // inversion (HARM_B200_MLP_ENGINE=mma), 1 tcgen05 network kernel
+                           // ahead of it (=tc), 2 tcgen05 inside the inversion kernel
+                           // (=tc-fused), 3 mma.sync inside the inversion kernel (=mma-fused)
+  double mlp_gate;         // gated engine: a first Newton step above this fraction of the
+                           // convergence scale marks a poor previous-state start
+                           // (HARM_B200_MLP_GATE, default 0.02)
+  unsigned int* d_nhard;   // gated engine: length of its list of poorly started cells
   int num_sms;
   unsigned long long launches;  // kernels launched by this context
 };

@@ -604,9 +604,8 @@ __device__ __forceinline__ T weno_lof(T f, T fm, T fp, T ss) {
 // veff = sign(sqrt(-g) rho u^dir) par / (sqrt(par) + SMALL),
 // upar = |(u + p + b^2)(|u^dir| u_t) + p + b^2/2 - b^dir b_t|
 template <typename T>
-__device__ __forceinline__ void weno_dp_cell(const T* pr, const Geo<T>& g, T gam, int dir, T& par, T& veff, T& upar) {
-  State<T> q;
-  get_state<T>(pr, g, gam, q);
+__device__ __forceinline__ void weno_dp_of_state(const T* pr, const Geo<T>& g, const State<T>& q, int dir, T& par,
+                                                 T& veff, T& upar) {
   T bcon[4], bcov0;
   bcon[0] = pr[HARM_B1] * q.ucov[1] + pr[HARM_B2] * q.ucov[2] + pr[HARM_B3] * q.ucov[3];
 #pragma unroll
@@ -619,6 +618,12 @@ __device__ __forceinline__ void weno_dp_cell(const T* pr, const Geo<T>& g, T gam
   par = fabs(q.plus1ud0 * ud);
   veff = copysign(T(1), V) * par / (sqrt(par) + WenoEps<T>::small);
   upar = fabs((pr[HARM_UU] + q.pressure + q.bsq) * (fabs(ud) * q.ucov[0]) + ptot + btt);
+}
+template <typename T>
+__device__ __forceinline__ void weno_dp_cell(const T* pr, const Geo<T>& g, T gam, int dir, T& par, T& veff, T& upar) {
+  State<T> q;
+  get_state<T>(pr, g, gam, q);
+  weno_dp_of_state<T>(pr, g, q, dir, par, veff, upar);
 }
 // dP of a cell from its rho, par, upar and its neighbours' veff, upar
 template <typename T>

@@ -148,7 +148,11 @@ __device__ __forceinline__ bool errcheck(double errx, double x0, const InvC& c) 
 __device__ __forceinline__ int extracheck(double x0, const InvC& c) { return ultrarel(x0, c) ? 4 : 2; }
 
 // general_newton_raphson, n=1, no line search.  Returns 0/1 (retval), updates flag.
-static __device__ int newton(int8_t& flag, double& xio, const InvC& c, int& lntries, int& nstroke) {
+// GATED: when the first Newton step from the start is larger than `gate` relative to
+// max(|w0|, |x|) (the scale of the convergence test), the start is judged poor and the
+// iteration stops there, returning 2 with xio unchanged (one iteration counted).
+template <bool GATED = false>
+static __device__ int newton(int8_t& flag, double& xio, const InvC& c, int& lntries, int& nstroke, double gate = 0.0) {
   double x = xio, x_old = x, x_older = x;
   double dx, dx_old = kVERYBIG, resid, jac, f = 1.0, errx = 1.0, damp = 1.0;
   int n_iter = 0, diddamp = 0, i_extra = 0, doing_extra = 0;
@@ -158,6 +162,10 @@ static __device__ int newton(int8_t& flag, double& xio, const InvC& c, int& lntr
     lntries++;
     if (lntries > kITERDAMPSTART && diddamp == 0) damp = 0.5;
     inv_func(x, c, resid, jac, dx, f);
+    if (GATED && n_iter == 0) {
+      const double first = (c.w0 == 0.) ? fabs(dx) : fabs(dx) / fmax(fabs(c.w0), fabs(x));
+      if (!(first <= gate)) return 2;
+    }
     x_older = x_old;
     x_old = x;
     diddamp = 0;
@@ -351,12 +359,25 @@ static __device__ __forceinline__ void jon_prepare(bool cold, const double* Ugf,
 
 // The rest of the inversion from the starting W' `Wp`: prim[RHO..U3] receive the
 // primitives on success; flag the outcome; wp_out (optional) the final W'.
-static __device__ __forceinline__ void jon_solve(const JonSetup& s, double Wp, double* prim, int8_t& flag, int& nstroke,
-                                                 double* wp_out = nullptr) {
+// GATED: returns true, with prim and flag untouched, where the first Newton step from Wp
+// exceeds `gate` (newton<true>); otherwise the same operations as without GATED.
+template <bool GATED = false>
+static __device__ __forceinline__ bool jon_solve(const JonSetup& s, double Wp, double* prim, int8_t& flag, int& nstroke,
+                                                 double* wp_out = nullptr, double gate = 0.0) {
   int lntries = 0;
+  int8_t flag_in = flag;
   flag = s.flag0;
   int retval = inv_verify_guess(Wp, s.c, flag);
-  retval += newton(flag, Wp, s.c, lntries, nstroke);
+  if (GATED && retval == 0) {
+    const int r = newton<true>(flag, Wp, s.c, lntries, nstroke, gate);
+    if (r == 2) {
+      flag = flag_in;
+      return true;
+    }
+    retval += r;
+  } else {
+    retval += newton(flag, Wp, s.c, lntries, nstroke);
+  }
   if (wp_out) *wp_out = Wp;
   double pt[5];
   if (retval == 0) retval = inv_finish(Wp, s.c, s.Qtcon, s.Bcon, pt, flag);
@@ -366,6 +387,7 @@ static __device__ __forceinline__ void jon_solve(const JonSetup& s, double Wp, d
   } else {
     if (flag <= 0) flag = (int8_t)(retval + HARM_UTOPRIMFAILCONVRET + 1);
   }
+  return false;
 }
 
 // Hot or cold Jon inversion on geometry-free U (Utoprim_jon_nonrelcompat_inputnorestmass).

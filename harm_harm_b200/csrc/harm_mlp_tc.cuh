@@ -447,6 +447,79 @@ static int launch_invert_mma(harm_ctx* c, const Dims& d, const Phys& ph, const C
   return 0;
 }
 
+// The gated learned start, second kernel: the cells k_invert_gated listed in `hard` (those
+// whose previous state is a poor start), with the network inside the inversion kernel as in
+// k_invert_mma: per round each warp evaluates the network for 32 listed cells (mma.sync BF16,
+// FP32 accumulation), then each thread runs the Newton inversion of its cell from that start;
+// a start that does not converge is replaced by the previous-state W' (invert_cell<true>), so
+// the result is the plain path's within the Newton tolerance.  The list's length is read on
+// the device, so the launch needs no host synchronisation; an empty list returns at once.
+// stats[1] receives the number of listed cells.
+template <int PATH>
+__global__ void __launch_bounds__(256) k_invert_hard(Dims d, Phys ph, const double* __restrict__ U,
+                                                     const double* __restrict__ pb, double* __restrict__ pf,
+                                                     int8_t* __restrict__ pflag, const double* __restrict__ geom,
+                                                     const double* __restrict__ aux, unsigned int* __restrict__ rare,
+                                                     unsigned int* __restrict__ nrare, double* __restrict__ stats,
+                                                     const unsigned int* __restrict__ hard,
+                                                     const unsigned int* __restrict__ nhard,
+                                                     const MlpPacked* __restrict__ mlp) {
+  __shared__ MlpPacked sm;
+  __shared__ MlpWarpScratch wsc[8];
+  const unsigned int n = *nhard;
+  if (blockIdx.x * 256u >= n) return;  // the same for every thread of the block
+  mlp_load_packed(sm, mlp);
+  __syncthreads();
+  double iters_d = 0.0, fb_d = 0.0, listed = 0.0;
+  for (unsigned int base = blockIdx.x * 256u; base < n; base += gridDim.x * 256u) {
+    const unsigned int slot = base + threadIdx.x;
+    const bool valid = slot < n;
+    int i = 0, j = 0, k = 0;
+    float f[MLP_IN];
+    double D = 0.0;
+    if (valid) {
+      const long long t = hard[slot];
+      i = (int)(t % d.n1);
+      const long long r = t / d.n1;
+      j = (int)(r % d.n2);
+      k = (int)(r / d.n2);
+      mlp_cell_features(d, U, geom, i, j, k, f, D);
+    }
+    float y[MLP_OUT];
+    mlp_warp_eval(sm, wsc[threadIdx.x >> 5], f, valid, y);
+    if (valid) {
+      double w = D * exp((double)y[0] + (double)sm.start_bias);
+      w = (w > 0.0 && isfinite(w)) ? w : -1.0;
+      invert_cell<true>(d, ph, U, pb, pf, pflag, geom, aux, rare, nrare, i, j, k, w, iters_d, fb_d);
+      listed += 1.0;
+    }
+  }
+  if (stats) {
+    warp_add_atomic(iters_d, stats + 0);
+    warp_add_atomic(listed, stats + 1);
+    warp_add_atomic(fb_d, stats + 2);
+  }
+}
+
+// The gated learned start: k_invert_gated over every active cell, then k_invert_hard over
+// the cells it listed (at most one block per 256 cells of the grid, at most two per SM).
+template <int PATH>
+static int launch_invert_gated(harm_ctx* c, const Dims& d, const Phys& ph, const CellTile& ct, const double* pb,
+                               double* pf, int8_t* pflag, double* stats) {
+  unsigned int* hard = reinterpret_cast<unsigned int*>(c->d_wpg);  // n1*n2*n3 doubles: room for the list
+  CK(cudaMemsetAsync(c->d_nhard, 0, sizeof(unsigned int), c->stream));
+  k_invert_gated<PATH><<<cell_grid(d.n1, d.n2, d.n3, ct), 256, 0, c->stream>>>(
+      d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare, c->d_nrare, stats, ct, c->mlp_gate, hard, c->d_nhard);
+  const long long ncell = (long long)d.n1 * d.n2 * d.n3;
+  const long long cap = 2LL * c->num_sms, need = (ncell + 255) / 256;
+  k_invert_hard<PATH><<<(unsigned)(need < cap ? need : cap), 256, 0, c->stream>>>(
+      d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare, c->d_nrare, stats, hard, c->d_nhard,
+      reinterpret_cast<const MlpPacked*>(c->d_mlp));
+  c->launches += 2;
+  CK(cudaGetLastError());
+  return 0;
+}
+
 // The tensor-core record follows the mma.sync record in the context's network buffer.
 static inline const MlpTc* mlp_tc_of(const harm_ctx* c) {
   return reinterpret_cast<const MlpTc*>(reinterpret_cast<const char*>(c->d_mlp) + sizeof(MlpPacked));
@@ -459,8 +532,9 @@ static inline MlpTc* mlp_tc_of(harm_ctx* c) {
 // memory (at most 4 by its shared memory, so its TMEM columns always fit: 4 x 128 = 512),
 // after raising its dynamic shared-memory limit, once per device and kernel.
 template <typename K>
-static int tc_blocks_per_sm(harm_ctx* c, K kernel, unsigned& configured, int& per_sm) {
-  if (!(configured & (1u << c->device))) {
+static int tc_blocks_per_sm(harm_ctx* c, K kernel, std::atomic<unsigned long long>& configured, std::atomic<int>& per_sm) {
+  if (c->device < 0 || c->device >= 64) return hb_seterr("tensor-core kernel set-up", cudaErrorInvalidDevice);
+  if (!(configured.load(std::memory_order_acquire) & (1ull << c->device))) {
     CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpTcBlock)));
     CK(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
     cudaFuncAttributes fa;
@@ -475,8 +549,8 @@ static int tc_blocks_per_sm(harm_ctx* c, K kernel, unsigned& configured, int& pe
     int n = by_regs < by_smem ? by_regs : by_smem;
     n = n < thr_sm / 256 ? n : thr_sm / 256;
     n = n < 4 ? n : 4;
-    per_sm = n < 1 ? 1 : n;
-    configured |= 1u << c->device;
+    per_sm.store(n < 1 ? 1 : n, std::memory_order_relaxed);
+    configured.fetch_or(1ull << c->device, std::memory_order_acq_rel);
   }
   return 0;
 }
@@ -485,12 +559,12 @@ static int tc_blocks_per_sm(harm_ctx* c, K kernel, unsigned& configured, int& pe
 template <int PATH>
 static int launch_invert_tc(harm_ctx* c, const Dims& d, const Phys& ph, const double* pb, double* pf, int8_t* pflag,
                             double* stats) {
-  static unsigned configured = 0;
-  static int per_sm = 1;
+  static std::atomic<unsigned long long> configured{0};
+  static std::atomic<int> per_sm{1};
   if (int rc = tc_blocks_per_sm(c, k_invert_tc<PATH>, configured, per_sm)) return rc;
   const Tile128 tt = tile128_of(d);
   const long long pairs = ((long long)tt.gx * tt.gy * tt.gz + 1) / 2;
-  const long long cap = (long long)per_sm * c->num_sms;
+  const long long cap = (long long)per_sm.load(std::memory_order_relaxed) * c->num_sms;
   const unsigned grid = (unsigned)(pairs < cap ? pairs : cap);
   k_invert_tc<PATH><<<grid, 256, sizeof(MlpTcBlock), c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux,
                                                                    c->d_rare, c->d_nrare, stats, tt, mlp_tc_of(c),
@@ -503,12 +577,12 @@ static int launch_invert_tc(harm_ctx* c, const Dims& d, const Phys& ph, const do
 // the learned start of every active cell into wpg with k_mlp_guess_tc
 template <int PATH>
 static int launch_mlp_guess_tc(harm_ctx* c, const Dims& d) {
-  static unsigned configured = 0;
-  static int per_sm = 1;
+  static std::atomic<unsigned long long> configured{0};
+  static std::atomic<int> per_sm{1};
   if (int rc = tc_blocks_per_sm(c, k_mlp_guess_tc<PATH>, configured, per_sm)) return rc;
   const Tile128 tt = tile128_of(d);
   const long long pairs = ((long long)tt.gx * tt.gy * tt.gz + 1) / 2;
-  const long long cap = (long long)per_sm * c->num_sms;
+  const long long cap = (long long)per_sm.load(std::memory_order_relaxed) * c->num_sms;
   const unsigned grid = (unsigned)(pairs < cap ? pairs : cap);
   k_mlp_guess_tc<PATH><<<grid, 256, sizeof(MlpTcBlock), c->stream>>>(d, c->d_U, c->d_geom, c->d_wpg, tt, mlp_tc_of(c),
                                                                       c->d_status);

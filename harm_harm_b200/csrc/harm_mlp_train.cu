@@ -527,15 +527,15 @@ extern "C" int harm_b200_mlp_predict(harm_ctx* c, size_t n, const float* d_feat,
   if (!c || !d_feat || !d_out) return hb_setmsg("null argument", 1);
   if (!c->d_mlp || !c->mlp_step) return hb_setmsg("no network set (harm_b200_mlp_set)", 3);
   if (n == 0) return 0;
-  if (c->mlp_tc) {
-    static unsigned configured = 0;
-    static int per_sm = 1;
+  if (c->mlp_tc == 1 || c->mlp_tc == 2) {  // the tcgen05 engines: their network kernel
+    static std::atomic<unsigned long long> configured{0};
+    static std::atomic<int> per_sm{1};
     if (int rc = tc_blocks_per_sm(c, k_mlp_predict_tc, configured, per_sm)) return rc;
     const size_t pairs = (n + 255) / 256;
-    const unsigned int nb = (unsigned int)std::min<size_t>(pairs, (size_t)per_sm * c->num_sms);
+    const unsigned int nb = (unsigned int)std::min<size_t>(pairs, (size_t)per_sm.load() * c->num_sms);
     k_mlp_predict_tc<<<nb, 256, sizeof(MlpTcBlock), c->stream>>>(n, d_feat, mlp_tc_of(c), d_out, c->d_status);
   } else {
-    const unsigned int nb = (unsigned int)std::min<size_t>((n + 255) / 256, (size_t)4 * 148);
+    const unsigned int nb = (unsigned int)std::min<size_t>((n + 255) / 256, (size_t)4 * c->num_sms);
     k_mlp_predict<<<nb, 256, 0, c->stream>>>(n, d_feat, reinterpret_cast<const MlpPacked*>(c->d_mlp), d_out);
   }
   c->launches++;

@@ -1,10 +1,25 @@
 // harm_path_fp64.cu -- FP64 path of the step (compiled with -fmad=false) and the FP64
 // kernels shared by both paths: boundary conditions, fixups, dt finalisation, point
 // inversions.
+//
+// harm_path_fp64fma.cu compiles this file's flux and update launchers a second time, with
+// FMA contraction and the inversion's shared reciprocals (HARM_FP64_FMA_TU): the FP64 path as
+// fast as the compiler makes it, for comparisons of speed (HARM_PREC_FP64_FMA); this build
+// (HARM_PREC_FP64) performs the CPU restatement's IEEE operations in its order.
 #include <algorithm>
 #include "harm_common.cuh"
 #include "harm_mlp_tc.cuh"
 #include "harm_paths.h"
+
+#ifdef HARM_FP64_FMA_TU
+#define FP64_PATH 2
+#define FP64_FN(name) name##fma
+#else
+#define FP64_PATH 0
+#define FP64_FN(name) name
+#endif
+
+#ifndef HARM_FP64_FMA_TU
 
 // copy p_b into the ghost zones of p_f (advance.c:654 copies the full grid)
 __global__ void k_copy_ghosts(Dims d, const double* __restrict__ pb, double* __restrict__ pf) {
@@ -246,43 +261,55 @@ __global__ void k_bound_x3(Dims d, double* P, int8_t* flag) {
     for (int p = 0; p < NPR; p++) P[(size_t)p * d.cells + dst] = P[(size_t)p * d.cells + src];
 }
 
-// ghost-zone flags for post_fixup's neighbour test (bound_pflag step_ch.c:1637): x1 copies
-// of the nearest active cell, x2 reflection across the pole (with n3 > 1 from the column
-// across the pole), then x3 periodic (k_bound_x3)
+// Ghost flags for post_fixup's neighbour test, as bound_pflag_user (boundsint.c:18) sets
+// them for the torus, in its order: x3 periodic first over the full i, j extent (k_bound_x3;
+// ghost cells in x1 or x2 of the x3 ghost planes so take the values their periodic partners
+// hold from the previous call), then the x1 outer OUTFLOW copy of the last active cell over
+// the active j, k (k_bound_flags_x1; the inner x1 boundary is FREEOUTFLOW, which leaves its
+// ghost flags alone), then the x2 POLARAXIS mirror within the same k plane over the full i
+// extent and the active k (k_bound_flags_x2).
 __global__ void k_bound_flags_x1(Dims d, int8_t* flag) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long n = (long long)2 * d.ng * d.n2e * d.n3e;
+  long long n = (long long)d.ng * d.n2 * d.n3;
   if (t >= n) return;
-  int gq = (int)(t % (2 * d.ng));
-  long long r = t / (2 * d.ng);
-  int jj = (int)(r % d.n2e), kk = (int)(r / d.n2e);
-  int ii = (gq < d.ng) ? gq : d.ng + d.n1 + (gq - d.ng);
-  int is = (gq < d.ng) ? d.ng : d.ng + d.n1 - 1;
-  flag[cidx(d, ii, jj, kk)] = flag[cidx(d, is, jj, kk)];
+  int gq = (int)(t % d.ng);
+  long long r = t / d.ng;
+  int jj = (int)(r % d.n2) + d.ng, kk = (int)(r / d.n2) + d.ng3;
+  int ii = d.ng + d.n1 + gq;
+  flag[cidx(d, ii, jj, kk)] = flag[cidx(d, d.ng + d.n1 - 1, jj, kk)];
 }
 
 __global__ void k_bound_flags_x2(Dims d, int8_t* flag) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long n = (long long)2 * d.ng * d.n1e * d.n3e;
+  long long n = (long long)2 * d.ng * d.n1e * d.n3;
   if (t >= n) return;
   int ii = (int)(t % d.n1e);
   long long r = t / d.n1e;
-  int gq = (int)(r % (2 * d.ng)), kk = (int)(r / (2 * d.ng));
-  int k = kk - d.ng3;
-  int ks = (d.n3 > 1) ? ((k + d.n3 / 2) % d.n3 + d.n3) % d.n3 + d.ng3 : kk;
+  int gq = (int)(r % (2 * d.ng)), kk = (int)(r / (2 * d.ng)) + d.ng3;
   int jj, js;
   if (gq < d.ng) { jj = gq; js = 2 * d.ng - 1 - jj; }
   else { jj = d.ng + d.n2 + (gq - d.ng); js = 2 * (d.ng + d.n2) - 1 - jj; }
-  flag[cidx(d, ii, jj, kk)] = flag[cidx(d, ii, js, ks)];
+  flag[cidx(d, ii, jj, kk)] = flag[cidx(d, ii, js, kk)];
 }
 
 // ------------------------------------------------------------------ post_fixup
 
 
+// fixup_utoprim (fixup.c:1061) of post_fixup (fixup.c:53), the torus configuration: per failed
+// active cell, from the values before any fix, the primitives to fix (u alone for
+// U2AVG1/U2AVG2/UPERC, else rho .. u^3), general_average (fixup.c:1830: the mean of the unfailed
+// neighbours of the 3x3(x3) box summed in pairs, or for U2AVG the smallest u of the pairs
+// whose both members are at least the cell's), where no neighbour is usable fixup_nogood
+// (fixup.c:2291: the mean of the 8 in-plane neighbours, failed or not; in the reset region of
+// USERRESETREGION, the first 10 radial cells and two cells at either pole, rho and u so and
+// a zero velocity), the Lorentz-factor limit of a fixed velocity to the cell's own (at most
+// GAMMAMAX), and the flag of fixuputoprim_accounting (fixup.c:1592): -1, for the negative
+// density/energy and U2AVG codes only on the final substep.  Each fixed cell is recorded and
+// written by k_fixup_apply, so that every cell's fix reads the unfixed neighbours.
 __global__ void __launch_bounds__(256) k_fixup_compute(Dims d, Phys ph, const double* __restrict__ P,
                                                        const int8_t* __restrict__ flag, const double* __restrict__ geom,
                                                        FixRec* __restrict__ recs, unsigned int* __restrict__ nrec,
-                                                       unsigned int cap) {
+                                                       unsigned int cap, int finalstep) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)d.n1 * d.n2 * d.n3) return;
   int i = (int)(t % d.n1);
@@ -321,12 +348,30 @@ __global__ void __launch_bounds__(256) k_fixup_compute(Dims d, Phys ph, const do
   }
   double out[5];
   for (int p = 0; p < 5; p++) out[p] = P[(size_t)p * d.cells + id];
+  int numavg;
   if (!u2) {
     if (numavg0 != 0)
       for (int p = startpl; p <= endpl; p++) out[p] = (sum0[p] + sum1[p]) / (double)numavg0;
+    numavg = numavg0;
   } else {
     if (numavg1 != 0)
       for (int p = startpl; p <= endpl; p++) out[p] = lastmin[p];
+    numavg = numavg1;
+  }
+  if (f == HARM_UTOPRIMFAILU2AVG2) numavg++;
+  if (numavg == 0) {  // fixup_nogood: 0.5 (AVG4_1 + AVG4_2) in the cell's k plane
+    const bool reset = (j <= 1 || j >= d.n2 - 2) || (i < 10);
+    const int lo = reset ? HARM_RHO : startpl, hi = reset ? HARM_UU : endpl;
+    for (int p = lo; p <= hi; p++) {
+      const double* q = P + (size_t)p * d.cells;
+      const double a4 = 0.25 * ((q[cidx(d, ii, jj + 1, kk)] + q[cidx(d, ii, jj - 1, kk)]) +
+                                (q[cidx(d, ii - 1, jj, kk)] + q[cidx(d, ii + 1, jj, kk)]));
+      const double b4 = 0.25 * ((q[cidx(d, ii + 1, jj + 1, kk)] + q[cidx(d, ii + 1, jj - 1, kk)]) +
+                                (q[cidx(d, ii - 1, jj + 1, kk)] + q[cidx(d, ii - 1, jj - 1, kk)]));
+      out[p] = 0.5 * (a4 + b4);
+    }
+    if (reset)
+      for (int p = HARM_U1; p <= HARM_U3; p++) out[p] = 0.0;
   }
   if (startpl <= HARM_U1 && endpl >= HARM_U3) {
     Geo<double> g;
@@ -340,20 +385,23 @@ __global__ void __launch_bounds__(256) k_fixup_compute(Dims d, Phys ph, const do
     limit_gamma<double>(gamma, pv, g);
     for (int p = 0; p < 5; p++) out[p] = pv[p];
   }
+  const bool soft = (f == HARM_UTOPRIMFAILRHONEG || f == HARM_UTOPRIMFAILUNEG || f == HARM_UTOPRIMFAILRHOUNEG || u2);
   unsigned int slot = atomicAdd(nrec, 1u);
   if (slot < cap) {
     recs[slot].id = (long long)id;
     for (int p = 0; p < 5; p++) recs[slot].v[p] = out[p];
+    recs[slot].flag = (!soft || finalstep) ? HARM_UTOPRIMFAILFIXEDUTOPRIM : f;
   }
 }
 
-__global__ void k_fixup_apply(Dims d, double* __restrict__ P, const FixRec* __restrict__ recs,
-                              const unsigned int* __restrict__ nrec, unsigned int cap) {
+__global__ void k_fixup_apply(Dims d, double* __restrict__ P, int8_t* __restrict__ flag,
+                              const FixRec* __restrict__ recs, const unsigned int* __restrict__ nrec, unsigned int cap) {
   unsigned int n = *nrec;
   if (n > cap) n = cap;
   for (unsigned int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
     size_t id = (size_t)recs[s].id;
     for (int p = 0; p < 5; p++) P[(size_t)p * d.cells + id] = recs[s].v[p];
+    flag[id] = (int8_t)recs[s].flag;
   }
 }
 
@@ -445,28 +493,36 @@ __global__ void __launch_bounds__(256, 2) k_utoprim_points_mlp(size_t n, Phys ph
   if (stats) warp_add_atomic(fb_d, stats + 2);
 }
 
+#endif  // HARM_FP64_FMA_TU
+
 // ------------------------------------------------------------------ launchers
 
 template <int LIM>
 static int flux_dirs_double(harm_ctx* c, const Dims& d, const Phys& ph, const double* pb, double* F1, double* F2, double* F3,
                          unsigned long long* slots, const SlabWait* sw) {
+  // WENO5: the cell pass computes the dP line quantities once per cell for the three directions
+  double* L = (LIM == HARM_LIM_WENO5) ? reinterpret_cast<double*>(c->d_line) : nullptr;
   if (sw) {
-    CK((launch_flux_slabs<LIM, double, double>(d, ph, pb, c->d_geom, F1, F2, F3, slots, c->stream, *sw, c->launches)));
+    CK((launch_flux_slabs<LIM, double, double>(d, ph, pb, c->d_geom, F1, F2, F3, slots, c->stream, *sw, c->launches, L)));
     return 0;
   }
+  if (L) {
+    CK((launch_cellprep<double, double>(d, ph, pb, c->d_geom, L, 0, d.n3e, c->stream)));
+    c->launches++;
+  }
   FaceBox b1 = face_box(d, 1), b2 = face_box(d, 2), b3 = face_box(d, 3);
-  CK((launch_fluxt<1, LIM, double, double>(d, ph, b1, pb, c->d_geom, F1, slots + 0, c->stream)));
-  CK((launch_fluxt<2, LIM, double, double>(d, ph, b2, pb, c->d_geom, F2, slots + 1, c->stream)));
+  CK((launch_fluxt<1, LIM, double, double>(d, ph, b1, pb, c->d_geom, F1, slots + 0, c->stream, L)));
+  CK((launch_fluxt<2, LIM, double, double>(d, ph, b2, pb, c->d_geom, F2, slots + 1, c->stream, L)));
   c->launches += 2;
   if (d.n3 > 1) {
-    CK((launch_fluxt<3, LIM, double, double>(d, ph, b3, pb, c->d_geom, F3, slots + 2, c->stream)));
+    CK((launch_fluxt<3, LIM, double, double>(d, ph, b3, pb, c->d_geom, F3, slots + 2, c->stream, L)));
     c->launches++;
   }
   return 0;
 }
 
-int hp_fluxes_fp64(harm_ctx* c, const double* pb, double* F1, double* F2, double* F3, double* emf,
-                   unsigned long long* slots, const SlabWait* sw) {
+int FP64_FN(hp_fluxes_fp64)(harm_ctx* c, const double* pb, double* F1, double* F2, double* F3, double* emf,
+                            unsigned long long* slots, const SlabWait* sw) {
   Dims d = dims_of(c->g);
   Phys ph = phys_of(c->g);
   if (c->g.lim == HARM_LIM_WENO5) { int rc = flux_dirs_double<HARM_LIM_WENO5>(c, d, ph, pb, F1, F2, F3, slots, sw); if (rc) return rc; }
@@ -480,8 +536,8 @@ int hp_fluxes_fp64(harm_ctx* c, const double* pb, double* F1, double* F2, double
   return 0;
 }
 
-int hp_update_fp64(harm_ctx* c, const StepCoef& sc, const double* pi, const double* pb, double* pf, int8_t* pflag,
-                   double* stats) {
+int FP64_FN(hp_update_fp64)(harm_ctx* c, const StepCoef& sc, const double* pi, const double* pb, double* pf,
+                            int8_t* pflag, double* stats) {
   Dims d = dims_of(c->g);
   Phys ph = phys_of(c->g);
   const CellTile ct = cell_tile(d.n3, HARM_INVERT_LTK);
@@ -494,33 +550,36 @@ int hp_update_fp64(harm_ctx* c, const StepCoef& sc, const double* pi, const doub
                                                             c->d_F[2], c->d_emf, c->d_geom, c->d_conn, c->d_U, cct);
   }
   CK(cudaMemsetAsync(c->d_nrare, 0, sizeof(unsigned int), c->stream));
-  if (sc.guess == HARM_GUESS_MLP && c->mlp_tc == 2) {
-    if (int rc = launch_invert_tc<0>(c, d, ph, pb, pf, pflag, stats)) return rc;
+  if (sc.guess == HARM_GUESS_MLP && c->mlp_tc == 4) {
+    if (int rc = launch_invert_gated<FP64_PATH>(c, d, ph, ct, pb, pf, pflag, stats)) return rc;
+  } else if (sc.guess == HARM_GUESS_MLP && c->mlp_tc == 2) {
+    if (int rc = launch_invert_tc<FP64_PATH>(c, d, ph, pb, pf, pflag, stats)) return rc;
   } else if (sc.guess == HARM_GUESS_MLP && c->mlp_tc == 3) {
-    if (int rc = launch_invert_mma<0>(c, d, ph, ct, pb, pf, pflag, stats)) return rc;
+    if (int rc = launch_invert_mma<FP64_PATH>(c, d, ph, ct, pb, pf, pflag, stats)) return rc;
   } else if (sc.guess == HARM_GUESS_MLP) {
     if (c->mlp_tc == 1) {
-      if (int rc = launch_mlp_guess_tc<0>(c, d)) return rc;
+      if (int rc = launch_mlp_guess_tc<FP64_PATH>(c, d)) return rc;
     } else {
-      k_mlp_guess<0><<<HARM_MLP_GUESS_BLOCKS * c->num_sms, 256, 0, c->stream>>>(d, c->d_U, c->d_geom, c->d_wpg,
+      k_mlp_guess<FP64_PATH><<<HARM_MLP_GUESS_BLOCKS * c->num_sms, 256, 0, c->stream>>>(d, c->d_U, c->d_geom, c->d_wpg,
                                                       reinterpret_cast<const MlpPacked*>(c->d_mlp), ct);
       c->launches++;
     }
-    k_invert<0, true><<<cell_grid(d.n1, d.n2, d.n3, ct), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag,
+    k_invert<FP64_PATH, true><<<cell_grid(d.n1, d.n2, d.n3, ct), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag,
                                                           c->d_geom, c->d_aux, c->d_rare, c->d_nrare, stats, ct, c->d_wpg);
     c->launches++;
   } else {
-    k_invert<0><<<cell_grid(d.n1, d.n2, d.n3, ct), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom,
+    k_invert<FP64_PATH><<<cell_grid(d.n1, d.n2, d.n3, ct), 256, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom,
                                                     c->d_aux, c->d_rare, c->d_nrare, stats, ct);
     c->launches++;
   }
-  k_invert_rare<0><<<2 * 148, 128, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
+  k_invert_rare<FP64_PATH><<<2 * c->num_sms, 128, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
                                                      c->d_nrare, stats);
   c->launches += 2;
   CK(cudaGetLastError());
   return 0;
 }
 
+#ifndef HARM_FP64_FMA_TU
 int hp_emf_to_flux_fp64(harm_ctx* c, const double* emf, double* F1, double* F2, double* F3) {
   Dims d = dims_of(c->g);
   long long nc = (long long)(d.n1 + 1) * (d.n2 + 1) * (d.n3 > 1 ? d.n3 + 1 : 1);
@@ -544,13 +603,13 @@ int hp_bound(harm_ctx* c, double* P, int8_t* flag) {
     }
   }
   if (flag) {
-    k_bound_flags_x1<<<nblk(2LL * d.ng * d.n2e * d.n3e), 256, 0, c->stream>>>(d, flag);
-    k_bound_flags_x2<<<nblk(2LL * d.ng * d.n1e * d.n3e), 256, 0, c->stream>>>(d, flag);
-    c->launches += 2;
     if (d.n3 > 1) {
       k_bound_x3<<<nblk(2LL * d.ng3 * (long long)d.plane), 256, 0, c->stream>>>(d, nullptr, flag);
       c->launches++;
     }
+    k_bound_flags_x1<<<nblk((long long)d.ng * d.n2 * d.n3), 256, 0, c->stream>>>(d, flag);
+    k_bound_flags_x2<<<nblk(2LL * d.ng * d.n1e * d.n3), 256, 0, c->stream>>>(d, flag);
+    c->launches += 2;
   }
   CK(cudaGetLastError());
   return 0;
@@ -564,15 +623,15 @@ int hp_copy_ghosts(harm_ctx* c, const double* pb, double* pf) {
   return 0;
 }
 
-int hp_fixup(harm_ctx* c, double* pf, int8_t* pflag, bool bound_flags) {
+int hp_fixup(harm_ctx* c, double* pf, int8_t* pflag, int finalstep, bool bound_flags) {
   Dims d = dims_of(c->g);
   Phys ph = phys_of(c->g);
   if (bound_flags && hp_bound(c, nullptr, pflag)) return 1;
   CK(cudaMemsetAsync(c->d_nrec, 0, sizeof(unsigned int), c->stream));
   long long ncell = (long long)d.n1 * d.n2 * d.n3;
   k_fixup_compute<<<nblk(ncell), 256, 0, c->stream>>>(d, ph, pf, pflag, c->d_geom, (FixRec*)c->d_fixrec, c->d_nrec,
-                                                       c->fix_cap);
-  k_fixup_apply<<<4 * 148, 256, 0, c->stream>>>(d, pf, (const FixRec*)c->d_fixrec, c->d_nrec, c->fix_cap);
+                                                       c->fix_cap, finalstep);
+  k_fixup_apply<<<4 * c->num_sms, 256, 0, c->stream>>>(d, pf, pflag, (const FixRec*)c->d_fixrec, c->d_nrec, c->fix_cap);
   c->launches += 2;
   CK(cudaGetLastError());
   return 0;
@@ -590,7 +649,7 @@ int hp_points(harm_ctx* c, size_t n, int guess, const double* U, const double* g
               int32_t* iters) {
   Phys ph = phys_of(c->g);
   if (guess == HARM_GUESS_MLP) {
-    const unsigned int nb = (unsigned int)std::min<size_t>((n + 255) / 256, (size_t)2 * 148);
+    const unsigned int nb = (unsigned int)std::min<size_t>((n + 255) / 256, (size_t)2 * c->num_sms);
     k_utoprim_points_mlp<<<nb, 256, 0, c->stream>>>(n, ph, U, geom, P, pflag, iters,
                                                    reinterpret_cast<const MlpPacked*>(c->d_mlp), c->d_stats);
   } else {
@@ -600,3 +659,4 @@ int hp_points(harm_ctx* c, size_t n, int guess, const double* U, const double* g
   CK(cudaGetLastError());
   return 0;
 }
+#endif  // HARM_FP64_FMA_TU

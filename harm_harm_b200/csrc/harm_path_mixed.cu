@@ -69,8 +69,11 @@ static int launch_fluxt_tma(harm_ctx* c, const Dims& d, const Phys& ph, const Fa
 template <int LIM>
 static int flux_dirs_float(harm_ctx* c, const Dims& d, const Phys& ph, const double* pb, float* F1, float* F2, float* F3,
                          unsigned long long* slots, const SlabWait* sw) {
+  // WENO5: the cell pass computes the dP line quantities once per cell for the three
+  // directions (the plain-load tiles read them; the TMA-staged tiles compute their own)
+  float* L = (LIM == HARM_LIM_WENO5) ? reinterpret_cast<float*>(c->d_line) : nullptr;
   if (sw) {  // state arriving in slabs: plain-load tiles, launched slab by slab
-    CK((launch_flux_slabs<LIM, float, float>(d, ph, pb, c->d_geomf, F1, F2, F3, slots, c->stream, *sw, c->launches)));
+    CK((launch_flux_slabs<LIM, float, float>(d, ph, pb, c->d_geomf, F1, F2, F3, slots, c->stream, *sw, c->launches, L)));
     return 0;
   }
   FaceBox b1 = face_box(d, 1), b2 = face_box(d, 2), b3 = face_box(d, 3);
@@ -87,11 +90,15 @@ static int flux_dirs_float(harm_ctx* c, const Dims& d, const Phys& ph, const dou
       return 0;
     }
   }
-  CK((launch_fluxt<1, LIM, float, float>(d, ph, b1, pb, c->d_geomf, F1, slots + 0, c->stream)));
-  CK((launch_fluxt<2, LIM, float, float>(d, ph, b2, pb, c->d_geomf, F2, slots + 1, c->stream)));
+  if (L) {
+    CK((launch_cellprep<float, float>(d, ph, pb, c->d_geomf, L, 0, d.n3e, c->stream)));
+    c->launches++;
+  }
+  CK((launch_fluxt<1, LIM, float, float>(d, ph, b1, pb, c->d_geomf, F1, slots + 0, c->stream, L)));
+  CK((launch_fluxt<2, LIM, float, float>(d, ph, b2, pb, c->d_geomf, F2, slots + 1, c->stream, L)));
   c->launches += 2;
   if (d.n3 > 1) {
-    CK((launch_fluxt<3, LIM, float, float>(d, ph, b3, pb, c->d_geomf, F3, slots + 2, c->stream)));
+    CK((launch_fluxt<3, LIM, float, float>(d, ph, b3, pb, c->d_geomf, F3, slots + 2, c->stream, L)));
     c->launches++;
   }
   return 0;
@@ -129,7 +136,9 @@ int hp_update_mixed(harm_ctx* c, const StepCoef& sc, const double* pi, const dou
                                                                                  c->d_Ff[2], c->d_emff, c->d_U, cct);
   c->launches++;
   CK(cudaMemsetAsync(c->d_nrare, 0, sizeof(unsigned int), c->stream));
-  if (sc.guess == HARM_GUESS_MLP && c->mlp_tc == 2) {
+  if (sc.guess == HARM_GUESS_MLP && c->mlp_tc == 4) {
+    if (int rc = launch_invert_gated<1>(c, d, ph, ct, pb, pf, pflag, stats)) return rc;
+  } else if (sc.guess == HARM_GUESS_MLP && c->mlp_tc == 2) {
     if (int rc = launch_invert_tc<1>(c, d, ph, pb, pf, pflag, stats)) return rc;
   } else if (sc.guess == HARM_GUESS_MLP && c->mlp_tc == 3) {
     if (int rc = launch_invert_mma<1>(c, d, ph, ct, pb, pf, pflag, stats)) return rc;
@@ -149,7 +158,7 @@ int hp_update_mixed(harm_ctx* c, const StepCoef& sc, const double* pi, const dou
                                                     c->d_aux, c->d_rare, c->d_nrare, stats, ct);
     c->launches++;
   }
-  k_invert_rare<1><<<2 * 148, 128, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
+  k_invert_rare<1><<<2 * c->num_sms, 128, 0, c->stream>>>(d, ph, c->d_U, pb, pf, pflag, c->d_geom, c->d_aux, c->d_rare,
                                                      c->d_nrare, stats);
   c->launches += 2;
   CK(cudaGetLastError());

@@ -171,15 +171,24 @@ __device__ __forceinline__ F2 weno_frac_f2(const F2* w, const F2* wm, const F2* 
 // SMONO indicators m.  (1 - m) out + m y5 is out for m = 0 and y5 for m = 1 (finite out), so
 // the packed code blends both lanes; it skips the WENO sums when both cells are monotone and
 // the 5-point values when neither is partly monotone.
+// Offset form: every candidate edge value is the cell's value plus a combination of the
+// differences d_k = u_k - u_0 (each stencil's coefficients sum to one), and the weighted
+// combination is u_0 + sum_k w_k (rec_k - u_0).  In exact arithmetic this is the scalar
+// code's sum_k w_k rec_k (the normalised weights sum to one); in FP32 the rounding of the
+// weights' normalisation then scales only the offsets, not the cell value, so a constant
+// line reconstructs to its value exactly and the reconstruction carries no bias of the
+// order of that rounding times the value, which a near-steady flow would accumulate step
+// after step.
 __device__ __forceinline__ void weno5_edges_f2(const F2* u, const F2* w, F2 f, F2 m, F2& yl, F2& yr) {
-  F2 y5l = f2(0.0f), y5r = f2(0.0f);
+  const F2 dm2 = u[-2] - u[0], dm1 = u[-1] - u[0], dp1 = u[1] - u[0], dp2 = u[2] - u[0];
+  F2 o5l = f2(0.0f), o5r = f2(0.0f);
   if (m.x != 0.0f || m.y != 0.0f) {
-    const F2 c0 = f2(-5.f / 128.f), c1 = f2(15.f / 32.f), c2 = f2(45.f / 64.f), c3 = f2(-5.f / 32.f), c4 = f2(3.f / 128.f);
-    y5l = ffma2(c2, u[0], ffma2(c1, u[-1], c3 * u[1]) + ffma2(c0, u[-2], c4 * u[2]));
-    y5r = ffma2(c2, u[0], ffma2(c3, u[-1], c1 * u[1]) + ffma2(c4, u[-2], c0 * u[2]));
+    const F2 c0 = f2(-5.f / 128.f), c1 = f2(15.f / 32.f), c3 = f2(-5.f / 32.f), c4 = f2(3.f / 128.f);
+    o5l = ffma2(c1, dm1, c3 * dp1) + ffma2(c0, dm2, c4 * dp2);
+    o5r = ffma2(c3, dm1, c1 * dp1) + ffma2(c4, dm2, c0 * dp2);
     if (m.x >= 1.0f && m.y >= 1.0f) {
-      yl = y5l;
-      yr = y5r;
+      yl = u[0] + o5l;
+      yr = u[0] + o5r;
       return;
     }
   }
@@ -200,15 +209,15 @@ __device__ __forceinline__ void weno5_edges_f2(const F2* u, const F2* w, F2 f, F
       wr[s] = wr[s] * omf;
     }
   }
-  const F2 k158 = f2(15.f / 8.f), k54 = f2(-5.f / 4.f), k38 = f2(3.f / 8.f), k34 = f2(3.f / 4.f), k18 = f2(-1.f / 8.f);
-  // the symmetric sums (a0 + a2) + a1 of the scalar code, contracted into packed FMAs
+  const F2 k54 = f2(-5.f / 4.f), k38 = f2(3.f / 8.f), k34 = f2(3.f / 4.f), k18 = f2(-1.f / 8.f);
+  // the stencils' edge values less u_0: (15/8, -5/4, 3/8) -> -5/4 d1 + 3/8 d2, and so on
+  const F2 recl0 = ffma2(k54, dp1, k38 * dp2);
+  const F2 recl1 = ffma2(k38, dm1, k18 * dp1);
+  const F2 recl2 = ffma2(k18, dm2, k34 * dm1);
+  const F2 recr0 = ffma2(k34, dp1, k18 * dp2);
+  const F2 recr1 = ffma2(k18, dm1, k38 * dp1);
+  const F2 recr2 = ffma2(k38, dm2, k54 * dm1);
   auto poly3 = [](F2 k0, F2 x0, F2 k1, F2 x1, F2 k2, F2 x2) { return ffma2(k1, x1, ffma2(k0, x0, k2 * x2)); };
-  const F2 recl0 = poly3(k158, u[0], k54, u[1], k38, u[2]);
-  const F2 recl1 = poly3(k38, u[-1], k34, u[0], k18, u[1]);
-  const F2 recl2 = poly3(k18, u[-2], k34, u[-1], k38, u[0]);
-  const F2 recr0 = poly3(k38, u[0], k34, u[1], k18, u[2]);
-  const F2 recr1 = poly3(k18, u[-1], k34, u[0], k38, u[1]);
-  const F2 recr2 = poly3(k38, u[-2], k54, u[-1], k158, u[0]);
   F2 outl = poly3(wl[0], recl0, wl[1], recl1, wl[2], recl2);
   F2 outr = poly3(wr[0], recr0, wr[1], recr1, wr[2], recr2);
   if (two) {
@@ -223,17 +232,14 @@ __device__ __forceinline__ void weno5_edges_f2(const F2* u, const F2* w, F2 f, F
       l3[s] = (l3[s] * nl3) * f;
       r3[s] = (r3[s] * nr3) * f;
     }
-    const F2 h = f2(0.5f), k32 = f2(1.5f), km12 = f2(-0.5f);
-    const F2 rl0 = ffma2(k32, u[0], km12 * u[1]);
-    const F2 rl1 = ffma2(h, u[-1], h * u[0]);
-    const F2 rr0 = ffma2(h, u[0], h * u[1]);
-    const F2 rr1 = ffma2(km12, u[-1], k32 * u[0]);
-    outl = outl + ffma2(l3[0], rl0, nz_mul(l3[1], rl1));
-    outr = outr + ffma2(r3[0], rr0, nz_mul(r3[1], rr1));
+    const F2 h = f2(0.5f), km12 = f2(-0.5f);
+    // (3/2, -1/2) -> -1/2 d1; (1/2, 1/2) -> 1/2 d-1; (1/2, 1/2) -> 1/2 d1; (-1/2, 3/2) -> -1/2 d-1
+    outl = outl + ffma2(l3[0], km12 * dp1, nz_mul(l3[1], h * dm1));
+    outr = outr + ffma2(r3[0], h * dp1, nz_mul(r3[1], km12 * dm1));
   }
   const F2 omm = f2(1.0f) - m;
-  yl = ffma2(omm, outl, m * y5l);
-  yr = ffma2(omm, outr, m * y5r);
+  yl = u[0] + ffma2(omm, outl, m * o5l);
+  yr = u[0] + ffma2(omm, outr, m * o5r);
 }
 
 }  // namespace hb

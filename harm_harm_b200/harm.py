@@ -201,8 +201,9 @@ class Harm:
                     "advance")
         return ndt.value, st.as_dict()
 
-    def post_fixup(self, pf, pflag) -> None:
-        self._check(self._ordered(self.lib.harm_b200_post_fixup, self._ctx, _ptr(pf), _ptr(pflag)), "post_fixup")
+    def post_fixup(self, pf, pflag, finalstep: int = 1) -> None:
+        self._check(self._ordered(self.lib.harm_b200_post_fixup, self._ctx, _ptr(pf), _ptr(pflag), int(finalstep)),
+                    "post_fixup")
 
     def step_ch(self, P, dt: float, precision: int = N.HARM_PREC_FP64, guess: int = N.HARM_GUESS_PREV,
                 nsteps: int = 1, stats: bool = True):
@@ -219,6 +220,30 @@ class Harm:
         self._check(self._ordered(self.lib.harm_b200_step_host, self._ctx, precision, guess, _ptr(P_host), C.byref(d), C.byref(st)),
                     "step_ch_host")
         return d.value, st.as_dict()
+
+    def step_ch_host_harm(self, P_harm: np.ndarray, dt: float, precision: int = N.HARM_PREC_FP64,
+                          guess: int = N.HARM_GUESS_PREV):
+        """one step over a host array in HARM's [k][j][i][pl] layout"""
+        d = C.c_double(dt)
+        st = N.harm_stats()
+        self._check(self._ordered(self.lib.harm_b200_step_host_harm, self._ctx, precision, guess, _ptr(P_harm), C.byref(d),
+                                  C.byref(st)), "step_ch_host_harm")
+        return d.value, st.as_dict()
+
+    def from_harm_layout(self, P_harm, P) -> None:
+        """[k][j][i][pl] (HARM's ORDERSTORAGE 5) -> [pl][k][j][i], device arrays"""
+        self._check(self._ordered(self.lib.harm_b200_from_harm_layout, self._ctx, _ptr(P_harm), _ptr(P)), "from_harm_layout")
+
+    def to_harm_layout(self, P, P_harm) -> None:
+        self._check(self._ordered(self.lib.harm_b200_to_harm_layout, self._ctx, _ptr(P), _ptr(P_harm)), "to_harm_layout")
+
+    def flags_to_harm(self, pflag, harm_pflag, numpflags: int) -> None:
+        self._check(self._ordered(self.lib.harm_b200_flags_to_harm, self._ctx, _ptr(pflag), _ptr(harm_pflag), numpflags),
+                    "flags_to_harm")
+
+    def flags_from_harm(self, harm_pflag, pflag, numpflags: int) -> None:
+        self._check(self._ordered(self.lib.harm_b200_flags_from_harm, self._ctx, _ptr(harm_pflag), _ptr(pflag), numpflags),
+                    "flags_from_harm")
 
     def Utoprimgen(self, U, geomrec, P, pflag, iters=None, guess: int = N.HARM_GUESS_PREV) -> None:
         n = U.shape[-1]

@@ -62,9 +62,12 @@ enum { HARM_LIM_MC = 0, HARM_LIM_PARA = 1, HARM_LIM_WENO5 = 2, HARM_LIM_PARALINE
    where both wave speeds vanish, or LAXF (Rusanov) everywhere */
 enum { HARM_FLUX_HLL = 0, HARM_FLUX_LAXF = 1 };
 
-/* arithmetic of the flux path: FP64 everywhere, or FP32 reconstruction/HLL/CT with the
-   conserved update, inversion and metric kept in FP64 */
-enum { HARM_PREC_FP64 = 0, HARM_PREC_MIXED = 1 };
+/* arithmetic of the flux path: FP64 everywhere in the IEEE operations of the reference's C
+   in its order (HARM_PREC_FP64, no FMA contraction), FP32 reconstruction/HLL/CT with the
+   conserved update, inversion and metric kept in FP64 (HARM_PREC_MIXED), or FP64 everywhere
+   compiled with FMA contraction and the inversion's shared reciprocals (HARM_PREC_FP64_FMA:
+   round-off-level differences from HARM_PREC_FP64; the FP64 path at its best speed) */
+enum { HARM_PREC_FP64 = 0, HARM_PREC_MIXED = 1, HARM_PREC_FP64_FMA = 2 };
 
 /* initial guess of the Newton inversion: the previous primitive (set_guess_Wp,
    utoprim_jon.c:890) or the learned network with fallback to the previous primitive */
@@ -132,6 +135,8 @@ typedef struct harm_stats {
   double mlp_fallbacks;    /* cells whose learned guess failed and were re-solved */
   double inversion_failures; /* cells whose final pflag was a failure before fixup */
   double floor_hits;       /* cells where fixup1zone raised rho or u */
+  double mlp_cells;        /* cells given the learned start (every cell inverted, except with
+                              the gated engine: the cells whose previous state is a poor start) */
 } harm_stats;
 
 /* ------------------------------------------------------------------------------------
@@ -166,13 +171,17 @@ typedef struct harm_ctx harm_ctx;
    The caller owns the primitive arrays.  Read at creation, from the environment:
      HARM_B200_FLUX_STAGING=tma   stage the FP32 flux tiles with TMA tensor loads
                                   (default: coalesced loads; same arithmetic)
-     HARM_B200_MLP_ENGINE=tc      learned start on tcgen05 tensor cores, in a kernel ahead
-                                  of the inversion
-     HARM_B200_MLP_ENGINE=tc-fused  the same inside the inversion kernel
-     HARM_B200_MLP_ENGINE=mma-fused the mma.sync network inside the inversion kernel
-                                  (default: mma.sync tensor cores, in a kernel ahead of the
-                                  inversion; same network, same results to the BF16
-                                  rounding of its activations) */
+     HARM_B200_MLP_ENGINE          the learned start (HARM_GUESS_MLP): "gated" (default)
+                                  gives it only to the cells whose first Newton step from
+                                  the previous state exceeds HARM_B200_MLP_GATE (default
+                                  0.02) of the convergence scale, with the mma.sync network
+                                  inside the inversion kernel of those cells; every other
+                                  cell is the plain inversion.  For every cell: "mma" (the
+                                  mma.sync network in a kernel ahead of the inversion),
+                                  "mma-fused" (inside the inversion kernel), "tc" (tcgen05
+                                  tensor cores, a kernel ahead of it), "tc-fused" (inside
+                                  it); the same network, the same results to the BF16
+                                  rounding of its activations */
 int harm_b200_create(const harm_grid *g, const double *geom_h, const double *conn_h,
                      const double *aux_h, int device, harm_ctx **out);
 /* Create a context whose metric (CENT/FACE1/FACE2/CORN3), connection and floor tables are
@@ -216,9 +225,15 @@ int harm_b200_advance(harm_ctx *ctx, int precision, int guess, int timeorder,
                       double *d_pf, int8_t *d_pflag, double dt, const double CUf[4],
                       const double Cunew[4], double *ndt, harm_stats *stats);
 
-/* post_fixup() (fixup.c:53 -> fixup_utoprim fixup.c:1061): replace failed-inversion
-   cells by the average of their successful neighbours, then limit_gamma. */
-int harm_b200_post_fixup(harm_ctx *ctx, double *d_pf, int8_t *d_pflag);
+/* post_fixup() (fixup.c:53 -> bound_pflag, fixup_utoprim fixup.c:1061) of the final substep
+   (finalstep 1) or an earlier one (0): every failed active cell (flag > 0) takes the average
+   of its unfailed neighbours (for the U2AVG codes the smallest u of neighbour pairs not below
+   its own), or where none is usable the average of its 8 in-plane neighbours (zero velocity
+   in the reset region of the first 10 radial cells and two cells at either pole), then its
+   Lorentz factor is limited to its own before the fix; its flag becomes -1 (the soft
+   negative-density/energy and U2AVG codes only when finalstep is set).  d_pf's ghost zones
+   must be bounded; the flags' ghost zones are filled here. */
+int harm_b200_post_fixup(harm_ctx *ctx, double *d_pf, int8_t *d_pflag, int finalstep);
 
 /* One full RK2 step (step_ch_full step_ch.c:35 with TIMEORDER=2, setup_rktimestep
    step_ch.c:1244-1266): two advance() substeps, each followed by bound, post_fixup,
@@ -237,6 +252,27 @@ int harm_b200_step_n(harm_ctx *ctx, int precision, int guess, double *d_P, int n
    back.  Results are those of harm_b200_step. */
 int harm_b200_step_host(harm_ctx *ctx, int precision, int guess, double *h_P, double *dt,
                         harm_stats *stats);
+
+/* ------------------------------------------------------------------------------------
+ * HARM's own array layout.  HARM stores primitives, conserved variables and fluxes as
+ * FTYPE [N3M][N2M][N1M][NPR] (ORDERSTORAGE 5, global.storage.h:320-340) and its flags as
+ * PFTYPE [N3M][N2M][N1M][NUMPFLAGS]; this library's device arrays are [pl][k][j][i] (HARM_NPR
+ * planes of one primitive each, i fastest).  Both cover the extended grid with the same ghost
+ * width (HARM's MAXBND must equal harm_grid.ng).  The conversions run on the context's stream
+ * and return without waiting; HARM-layout arrays must be 16-byte aligned.
+ * ------------------------------------------------------------------------------------ */
+int harm_b200_from_harm_layout(harm_ctx *ctx, const double *d_harm, double *d_P);
+int harm_b200_to_harm_layout(harm_ctx *ctx, const double *d_P, double *d_harm);
+/* slot 0 (FLAGUTOPRIMFAIL) of each cell's numpflags ints <-> the int8 flag per cell */
+int harm_b200_flags_to_harm(harm_ctx *ctx, const int8_t *d_pflag, int32_t *d_harm_pflag, int numpflags);
+int harm_b200_flags_from_harm(harm_ctx *ctx, const int32_t *d_harm_pflag, int8_t *d_pflag, int numpflags);
+
+/* harm_b200_step_host over a host array in HARM's layout (step_ch_full step_ch.c:35 with
+   HARM's own p array): one copy per k-slab, each slab converted on the device as it arrives
+   (ahead of the first substep's flux tiles that stage it), the state converted back and
+   copied out after the step.  Results equal harm_b200_step's on the converted state. */
+int harm_b200_step_host_harm(harm_ctx *ctx, int precision, int guess, double *h_P_harm, double *dt,
+                             harm_stats *stats);
 
 /* Utoprimgen() (utoprimgen.c:32) over n independent points: d_U[8][n] in UEVOLVE form,
    d_geom[HARM_NGF][n] CENT metric of each point, d_P[8][n] guess in / primitives out,

@@ -58,7 +58,7 @@ def lib() -> C.CDLL:
             "orc_bound_dir": (I, [C.POINTER(orc), P, I, I]),
             "orc_fluxcalc": (I, [C.POINTER(orc), P, P, P, P, P]),
             "orc_advance": (I, [C.POINTER(orc), I, I, P, P, P, P, D, P, P, C.POINTER(D), C.POINTER(N.harm_stats)]),
-            "orc_post_fixup": (I, [C.POINTER(orc), P, P]),
+            "orc_post_fixup": (I, [C.POINTER(orc), P, P, I]),
             "orc_step": (I, [C.POINTER(orc), P, C.POINTER(D), C.POINTER(N.harm_stats)]),
             "orc_reconstruct_line": (None, [I, I, P, P, P]),
             "orc_paraline_flattener": (None, [I, P, P, P]),
@@ -114,8 +114,8 @@ class Oracle:
                           _p(Cun), C.byref(ndt), C.byref(st))
         return ndt.value, st.as_dict()
 
-    def post_fixup(self, pf, pflag):
-        lib().orc_post_fixup(C.byref(self.o), _p(pf), _p(pflag))
+    def post_fixup(self, pf, pflag, finalstep: int = 1):
+        lib().orc_post_fixup(C.byref(self.o), _p(pf), _p(pflag), int(finalstep))
 
     def dump_rows(self, P, cells, U=None):
         """the main dump's 52 columns (dump_content, dump.c:449) of the active cells (i, j, k)"""

@@ -22,32 +22,29 @@ void orc_init(orc *o, const harm_grid *g, const double *geom, const double *conn
   o->nthreads = nthreads > 0 ? nthreads : 1;
 }
 
-/* Ghost-zone flags for post_fixup's neighbour test (bound_pflag step_ch.c:1637): x1 copies of
-   the nearest active cell, x2 reflection across the pole (with n3>1 from the column across the
-   pole, phi+pi), x3 periodic; applied in the order x1, x2, x3 over the full transverse extent. */
+/* Ghost-zone flags for post_fixup's neighbour test: bound_pflag_user (boundsint.c:18) with the
+   torus boundaries, in its order: x3 periodic over the full i, j extent first (so ghost cells
+   in x1 or x2 of the x3 ghost planes take the values their periodic partners hold from the
+   previous call), then the x1 outer OUTFLOW copy of the last active cell over the active j, k
+   (the x1 inner boundary is FREEOUTFLOW, which bound_pflag_user leaves alone), then the x2
+   POLARAXIS mirror within the same k plane over the full i extent and the active k. */
 static void bound_flags(orc *o, int8_t *flag) {
   const harm_grid *g = &o->g;
-  const int n1e = g->n1e, n2e = g->n2e, n3e = g->n3e, ng = g->ng, ng3 = g->ng3;
-  for (int kk = 0; kk < n3e; kk++)
-    for (int jj = 0; jj < n2e; jj++) {
-      for (int ii = 0; ii < ng; ii++) flag[oidx(o, ii, jj, kk)] = flag[oidx(o, ng, jj, kk)];
-      for (int ii = ng + g->n1; ii < n1e; ii++) flag[oidx(o, ii, jj, kk)] = flag[oidx(o, ng + g->n1 - 1, jj, kk)];
-    }
-  const int n3 = g->n3;
-  for (int kk = 0; kk < n3e; kk++)
-    for (int ii = 0; ii < n1e; ii++) {
-      int k = kk - ng3;
-      int ks = (n3 > 1) ? ((k + n3 / 2) % n3 + n3) % n3 + ng3 : kk;
-      for (int jj = 0; jj < ng; jj++) flag[oidx(o, ii, jj, kk)] = flag[oidx(o, ii, 2 * ng - 1 - jj, ks)];
-      for (int jj = ng + g->n2; jj < n2e; jj++)
-        flag[oidx(o, ii, jj, kk)] = flag[oidx(o, ii, 2 * (ng + g->n2) - 1 - jj, ks)];
-    }
+  const int n1e = g->n1e, n2e = g->n2e, ng = g->ng, ng3 = g->ng3, n3 = g->n3;
   if (n3 > 1)
     for (int jj = 0; jj < n2e; jj++)
       for (int ii = 0; ii < n1e; ii++) {
         for (int kk = 0; kk < ng3; kk++) flag[oidx(o, ii, jj, kk)] = flag[oidx(o, ii, jj, kk + n3)];
-        for (int kk = ng3 + n3; kk < n3e; kk++) flag[oidx(o, ii, jj, kk)] = flag[oidx(o, ii, jj, kk - n3)];
+        for (int kk = ng3 + n3; kk < g->n3e; kk++) flag[oidx(o, ii, jj, kk)] = flag[oidx(o, ii, jj, kk - n3)];
       }
+  for (int kk = ng3; kk < ng3 + n3; kk++)
+    for (int jj = ng; jj < ng + g->n2; jj++)
+      for (int ii = ng + g->n1; ii < n1e; ii++) flag[oidx(o, ii, jj, kk)] = flag[oidx(o, ng + g->n1 - 1, jj, kk)];
+  for (int kk = ng3; kk < ng3 + n3; kk++)
+    for (int ii = 0; ii < n1e; ii++) {
+      for (int jj = 0; jj < ng; jj++) flag[oidx(o, ii, jj, kk)] = flag[oidx(o, ii, 2 * ng - 1 - jj, kk)];
+      for (int jj = ng + g->n2; jj < n2e; jj++) flag[oidx(o, ii, jj, kk)] = flag[oidx(o, ii, 2 * (ng + g->n2) - 1 - jj, kk)];
+    }
 }
 
 
@@ -137,9 +134,24 @@ int orc_advance(orc *o, int timeorder, int numtimeorders, const double *pi, cons
   return 0;
 }
 
-/* fixup_utoprim (fixup.c:1061) with general_average (fixup.c:1830), CAUSALAVG=0,
-   HOWTOAVG_WHEN_U2AVG=MAXUPOSAVG; cells with no usable neighbour keep their value. */
-int orc_post_fixup(orc *o, double *pf, int8_t *pflag) {
+/* fixup_utoprim (fixup.c:1061) of post_fixup (fixup.c:53) with the torus configuration:
+   UTOPRIMADJUST=UTOPRIMAVG, GENERALAVERAGE, CAUSALAVG=0, HOWTOAVG_WHEN_U2AVG=MAXUPOSAVG,
+   HANDLE*NEG=0, DO_CONSERVE_D_INFAILFIXUPS=0, TODONOGOOD=NOGOODAVERAGE, USERRESETREGION=1
+   (initboundcode/init.fishmon.h), WHICHPTOUSEWHENNOGOOD=0, STEPOVERNEG*=NEVERFIXUP.
+   Per failed active cell (flag > 0), from the values before any fix (ptoavg):
+   - which primitives: u alone for U2AVG1/U2AVG2/UPERC, else rho .. u^3 (fixup.c:1196-1218);
+   - general_average (fixup.c:1830): the mean of the unfailed neighbours of the 3x3(x3) box
+     summed in pairs, or for U2AVG the smallest u of the pairs whose both members are at
+     least the cell's u;
+   - no usable neighbour (fixup_nogood fixup.c:2291; never for U2AVG2): the mean of the 8
+     in-plane neighbours (AVG4_1, AVG4_2 fixup.c:1812), failed or not, of those primitives;
+     in the reset region (first 10 radial cells, two cells at either pole) rho and u are
+     averaged so and the velocity set to the normal observer (zero ũ);
+   - a fixed velocity has its Lorentz factor limited to the cell's own before the fix
+     (at most GAMMAMAX);
+   - fixuputoprim_accounting (fixup.c:1592): the flag becomes UTOPRIMFAILFIXEDUTOPRIM (-1),
+     for the negative-density/energy and U2AVG codes only on the final substep. */
+int orc_post_fixup(orc *o, double *pf, int8_t *pflag, int finalstep) {
   const harm_grid *g = &o->g;
   const size_t cells = o->cells;
   bound_flags(o, pflag);
@@ -158,14 +170,15 @@ int orc_post_fixup(orc *o, double *pf, int8_t *pflag) {
         size_t id = oidx(o, ii, jj, kk);
         int8_t f = forig[id];
         if (f <= 0) continue;
-        int startpl, endpl, looptype;
-        if (f == HARM_UTOPRIMFAILU2AVG1 || f == HARM_UTOPRIMFAILU2AVG2 || f == 13) {
+        const int u2 = (f == HARM_UTOPRIMFAILU2AVG1 || f == HARM_UTOPRIMFAILU2AVG2);
+        int startpl, endpl;
+        if (u2 || f == 13) {
           startpl = endpl = HARM_UU;
         } else {
           startpl = HARM_RHO;
           endpl = HARM_U3;
         }
-        looptype = (f == HARM_UTOPRIMFAILU2AVG1 || f == HARM_UTOPRIMFAILU2AVG2) ? 1 : 0;
+        const int looptype = u2 ? 1 : 0;
         double mysum[2][HARM_NPR] = {{0}}, lastmin[HARM_NPR];
         for (int p = 0; p < HARM_NPR; p++) lastmin[p] = 1E50;
         int numavg0 = 0, numavg1 = 0;
@@ -187,12 +200,33 @@ int orc_post_fixup(orc *o, double *pf, int8_t *pflag) {
             }
           }
         }
+        int numavg;
         if (looptype == 0) {
           if (numavg0 != 0)
             for (int p = startpl; p <= endpl; p++) pf[p * cells + id] = (mysum[0][p] + mysum[1][p]) / (double)numavg0;
+          numavg = numavg0;
         } else {
           if (numavg1 != 0)
             for (int p = startpl; p <= endpl; p++) pf[p * cells + id] = lastmin[p];
+          numavg = numavg1;
+        }
+        if (f == HARM_UTOPRIMFAILU2AVG2) numavg++;
+        if (numavg == 0) {
+          /* fixup_nogood: 0.5 (AVG4_1 + AVG4_2) of ptoavg in the cell's k plane */
+          const size_t ijp = oidx(o, ii, jj + 1, kk), ijm = oidx(o, ii, jj - 1, kk);
+          const size_t imj = oidx(o, ii - 1, jj, kk), ipj = oidx(o, ii + 1, jj, kk);
+          const size_t pp = oidx(o, ii + 1, jj + 1, kk), pm = oidx(o, ii + 1, jj - 1, kk);
+          const size_t mp = oidx(o, ii - 1, jj + 1, kk), mm = oidx(o, ii - 1, jj - 1, kk);
+          const int reset = (j <= 1 || j >= g->n2 - 2) || (i < 10);
+          const int lo = reset ? HARM_RHO : startpl, hi = reset ? HARM_UU : endpl;
+          for (int p = lo; p <= hi; p++) {
+            const double *q = ptoavg + p * cells;
+            double a4 = 0.25 * ((q[ijp] + q[ijm]) + (q[imj] + q[ipj]));
+            double b4 = 0.25 * ((q[pp] + q[pm]) + (q[mp] + q[mm]));
+            pf[p * cells + id] = 0.5 * (a4 + b4);
+          }
+          if (reset)
+            for (int p = HARM_U1; p <= HARM_U3; p++) pf[p * cells + id] = 0.0;
         }
         if (startpl <= HARM_U1 && endpl >= HARM_U3) {
           ogeom gc;
@@ -204,6 +238,9 @@ int orc_post_fixup(orc *o, double *pf, int8_t *pflag) {
           o_limit_gamma(gamma, pv, &gc);
           for (int p = 0; p < HARM_NPR; p++) pf[p * cells + id] = pv[p];
         }
+        const int soft = (f == HARM_UTOPRIMFAILRHONEG || f == HARM_UTOPRIMFAILUNEG || f == HARM_UTOPRIMFAILRHOUNEG ||
+                          u2);
+        if (!soft || finalstep) pflag[id] = HARM_UTOPRIMFAILFIXEDUTOPRIM;
       }
   free(ptoavg);
   free(forig);
@@ -222,13 +259,13 @@ int orc_step(orc *o, double *P, double *dt, harm_stats *st) {
   orc_advance(o, 0, 2, P, P, pk, pflag, *dt, CUf[0], Cun[0], &ndt, st);
   if (ndt < lastndt) lastndt = ndt;
   orc_bound(o, pk);
-  orc_post_fixup(o, pk, pflag);
+  orc_post_fixup(o, pk, pflag, 0);
   orc_bound(o, pk);
   /* substep 1: pi=P, pb=pk, pf=P */
   orc_advance(o, 1, 2, P, pk, P, pflag, *dt, CUf[1], Cun[1], &ndt, st);
   if (ndt < lastndt) lastndt = ndt;
   orc_bound(o, P);
-  orc_post_fixup(o, P, pflag);
+  orc_post_fixup(o, P, pflag, 1);
   orc_bound(o, P);
   /* post_stepch (step_ch.c:213) */
   if (lastndt > o->g.safe * (*dt)) lastndt = o->g.safe * (*dt);

@@ -114,6 +114,30 @@ def points(n1: int, n2: int, n3: int, ng: int, ij: np.ndarray, U: np.ndarray, gu
     return out
 
 
+def fixup(n1: int, n2: int, n3: int, ng: int, P_ext: np.ndarray, flags: np.ndarray,
+          finalstep: int = 1) -> tuple[np.ndarray, np.ndarray]:
+    """post_fixup (fixup.c:53) of the reference on a given state: P_ext the extended state in
+    the device layout [8][n3e][n2e][n1e] (ghost zones filled), flags the failure flag of each
+    active cell [n3][n2][n1] (every ghost flag starts at 0), on the final substep or an
+    earlier one.  Returns the extended state afterwards [8][n3e][n2e][n1e] and the extended
+    flags afterwards [n3e][n2e][n1e]."""
+    exe = binary(n1, n2, n3, ng)
+    work = tempfile.mkdtemp(prefix="harm_ref_fix_")
+    inp = os.path.join(work, "in.bin")
+    aos = np.ascontiguousarray(np.moveaxis(np.asarray(P_ext, np.float64), 0, 3))
+    with open(inp, "wb") as f:
+        aos.tofile(f)
+        np.ascontiguousarray(np.asarray(flags, np.float64)).tofile(f)
+    r = subprocess.run([exe, "fixup", work, "1", inp, str(int(finalstep))], cwd=work, env=_env(0, 0, 2, 0.8, 12345),
+                       capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference fixup failed ({r.returncode}):\n{r.stderr[-3000:]}")
+    out = np.ascontiguousarray(np.moveaxis(np.load(os.path.join(work, "post_fixout.npy")), 3, 0))
+    fl = np.load(os.path.join(work, "post_fixflag.npy")).astype(np.int8)
+    subprocess.run(["rm", "-rf", work])
+    return out, fl
+
+
 def time_steps(n1: int, n2: int, n3: int, ng: int, lim: int, flux: int, nsteps: int, nthreads: int,
                timeout: float | None = None) -> dict:
     """Wall time of `nsteps` full reference steps on `nthreads` OpenMP threads (after one

@@ -34,6 +34,13 @@
  *       Utoprimgen (utoprimgen.c:32) of every record of <infile> (raw doubles: i, j, U[8],
  *       guess P[8]; U in UEVOLVE form at CENT of cell (i,j,0)); writes points.npy with
  *       P[8], pflag and the Newton iteration count of each record
+ *   harm_ref_<cfg> fixup  <outdir> <nthreads> <infile> [finalstep]
+ *       post_fixup (fixup.c:53, with its bound_pflag and fixup_utoprim) of a given state on
+ *       the final substep (finalstep 1, the default) or an earlier one (0):
+ *       <infile> holds the extended primitive state [k][j][i][pl] (raw doubles, ghost zones
+ *       filled by the caller) followed by the failure flag of every active cell [k][j][i]
+ *       (raw doubles); writes fixout.npy (the extended state afterwards) and fixflag.npy
+ *       (the extended flags afterwards)
  *   harm_ref_<cfg> time   <outdir> <nthreads> <nsteps>
  *       times <nsteps> full steps on <nthreads> OpenMP threads; writes time.npy
  *       (zone-cycles/s, seconds, steps, cells)
@@ -628,6 +635,38 @@ int main(int argc, char *argv[])
     write_npy(outdir, "points.npy", "<f8", out, sizeof(double), 2, shape);
     free(in);
     free(out);
+    return 0;
+  }
+  if (!strcmp(mode, "fixup")) {
+    const int n1e = N1 + 2 * N1BND, n2e = N2 + 2 * N2BND, n3e = N3 + 2 * N3BND;
+    const size_t next = (size_t)n1e * n2e * n3e, nact = (size_t)N1 * N2 * N3;
+    FILE *f;
+    double *in;
+    size_t o = 0;
+    int i, j, k, pl;
+    if (argc < 5) return 2;
+    f = fopen(argv[4], "rb");
+    if (!f) return 3;
+    in = (double *)malloc(sizeof(double) * (next * NPR + nact));
+    if (fread(in, sizeof(double), next * NPR + nact, f) != next * NPR + nact) return 3;
+    fclose(f);
+    for (k = -N3BND; k < N3 + N3BND; k++)
+      for (j = -N2BND; j < N2 + N2BND; j++)
+        for (i = -N1BND; i < N1 + N1BND; i++)
+          for (pl = 0; pl < NPR; pl++) GLOBALMACP0A1(pglobal, i, j, k, pl) = in[o++];
+    for (k = -N3BND; k < N3 + N3BND; k++)
+      for (j = -N2BND; j < N2 + N2BND; j++)
+        for (i = -N1BND; i < N1 + N1BND; i++) GLOBALMACP0A1(pflag, i, j, k, FLAGUTOPRIMFAIL) = UTOPRIMNOFAIL;
+    for (k = 0; k < N3; k++)
+      for (j = 0; j < N2; j++)
+        for (i = 0; i < N1; i++) GLOBALMACP0A1(pflag, i, j, k, FLAGUTOPRIMFAIL) = (PFTYPE)in[o++];
+    sub_dir = outdir;
+    snprintf(sub_prefix, sizeof sub_prefix, "post");
+    __real_post_fixup(STAGEM1, t, GLOBALPOINT(pglobal), GLOBALPOINT(pglobal), GLOBALPOINT(unewglobal),
+                      (argc > 5) ? atoi(argv[5]) : 1);
+    dump_ext("fixout", GLOBALPOINT(pglobal));
+    dump_flags("fixflag");
+    free(in);
     return 0;
   }
   if (!strcmp(mode, "time")) {

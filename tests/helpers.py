@@ -109,3 +109,21 @@ def read_dump(path, fmt="text"):
         rest = data[nl + 1:]
         body = np.frombuffer(rest, dtype=np.float64) if fmt == "mixed" else np.array(rest.split(), dtype=np.float64)
     return head, body.reshape(-1, head["ncol"])
+
+
+def harm_with_env(g, geom, conn, aux, **env):
+    """a device context created with the given environment settings (HARM_B200_MLP_ENGINE,
+    HARM_B200_MLP_GATE, ...), which a context reads once at creation"""
+    import os
+
+    from harm_harm_b200 import Harm
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update({k: str(v) for k, v in env.items()})
+    try:
+        return Harm(g, geom, conn, aux)
+    finally:
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v

@@ -15,7 +15,7 @@
 import numpy as np
 import pytest
 
-from helpers import make_torus, rel_err
+from helpers import harm_with_env, make_torus, rel_err
 from harm_harm_b200 import HARM_GUESS_MLP, HARM_GUESS_PREV, HARM_PREC_FP64, HARM_PREC_MIXED, Harm
 from oracle import oracle as O
 
@@ -168,6 +168,48 @@ def test_learned_guess_steps_match_plain_steps(torus2d, precision):
     print("iters/cell plain %.3f learned %.3f fallback rate %.5f" % (
         sta["newton_iters"] / sta["cells_inverted"], stb["newton_iters"] / stb["cells_inverted"],
         stb["mlp_fallbacks"] / stb["cells_inverted"]))
+
+
+@pytest.mark.parametrize("precision", [HARM_PREC_FP64, HARM_PREC_MIXED])
+def test_gated_learned_start(torus2d, precision):
+    """The default engine gives the learned start only to cells whose first Newton step from
+    the previous state exceeds HARM_B200_MLP_GATE of the convergence scale.  With no cell
+    above the gate the step is the plain step bit for bit; with a zero gate every cell takes
+    the learned start (listed, then inverted by the fused network + Newton kernel) and the
+    step matches the plain step within the Newton tolerance; the default gate lies between."""
+    torch, g, geom, conn, aux, P0, dev = torus2d
+    _, f, t, _ = _torus_pairs(torch, dev, P0)
+    norm, params, _ = _train(torch, dev, f, t, steps=3000)
+    Pa = torch.from_numpy(P0).cuda()
+    dev.bound_prim(Pa)
+    P1 = Pa.clone()
+    _, sta = dev.step_ch(Pa, 1e-3, precision=precision, guess=HARM_GUESS_PREV, nsteps=3)
+    a = Pa.cpu().numpy()
+    for gate in ("1e300", "0", None):
+        env = {"HARM_B200_MLP_ENGINE": "gated"}
+        if gate is not None:
+            env["HARM_B200_MLP_GATE"] = gate
+        dg = harm_with_env(g, geom, conn, aux, **env)
+        try:
+            dg.mlp_set(params, norm)
+            Pb = P1.clone()
+            _, stb = dg.step_ch(Pb, 1e-3, precision=precision, guess=HARM_GUESS_MLP, nsteps=3)
+        finally:
+            dg.close()
+        b = Pb.cpu().numpy()
+        assert stb["cells_inverted"] == sta["cells_inverted"]
+        print("gate %s: listed %.0f of %.0f, iters/cell %.3f (plain %.3f), fallbacks %.0f" % (
+            gate, stb["mlp_cells"], stb["cells_inverted"], stb["newton_iters"] / stb["cells_inverted"],
+            sta["newton_iters"] / sta["cells_inverted"], stb["mlp_fallbacks"]))
+        if gate == "1e300":
+            assert np.array_equal(a, b)
+            assert stb["mlp_cells"] == 0 and stb["newton_iters"] == sta["newton_iters"]
+            continue
+        for pl in range(8):
+            assert rel_err(a[pl], b[pl], 1e-8) < 1e-9, (gate, pl, rel_err(a[pl], b[pl], 1e-8))
+        assert stb["mlp_fallbacks"] <= 0.01 * max(stb["mlp_cells"], 1.0)
+        if gate == "0":
+            assert stb["mlp_cells"] >= 0.99 * stb["cells_inverted"]
 
 
 def test_learned_guess_gains_over_a_cold_start(torus2d):

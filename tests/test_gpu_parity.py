@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from helpers import divb_corner, make_torus, plant_compression, rel_err
-from harm_harm_b200 import HARM_PREC_FP64, HARM_PREC_MIXED, Harm
+from harm_harm_b200 import HARM_PREC_FP64, HARM_PREC_FP64_FMA, HARM_PREC_MIXED, Harm
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -168,6 +168,41 @@ def test_mixed_precision_close_to_fp64(setup, cuda):
     # flux-CT keeps the corner divergence at round-off in the mixed path too (the field
     # fluxes average their FP32 edge EMFs exactly, in FP64)
     assert divb_corner(g, geom, Pb.cpu().numpy()).max() / scale < 1e-10
+
+
+def test_fp64_fma_close_to_fp64(setup, cuda):
+    """The FP64 path compiled with FMA contraction and shared reciprocals (the FP64 path at
+    its best speed) against the IEEE-ordered FP64 path: the fluxes of one state to 1e-12 of
+    each field's largest face value, five steps to 1e-10 of each field's maximum (WENO5:
+    1e-6, since its SMONO indicator switches a cell between the 5-point and the WENO edge
+    where the edge derivatives are within ~1e-13 of the stencil's magnitude, so round-off
+    differences flip a few cells)."""
+    g, geom, conn, aux, P, orc, dev = setup
+    Pd = dev_array(cuda, P)
+    Fa = [cuda.zeros_like(Pd) for _ in range(3)]
+    Fb = [cuda.zeros_like(Pd) for _ in range(3)]
+    ndt_a = dev.fluxcalc(Pd, *Fa, precision=HARM_PREC_FP64)
+    ndt_b = dev.fluxcalc(Pd, *Fb, precision=HARM_PREC_FP64_FMA)
+    nd = 3 if g.g.n3 > 1 else 2
+    for d in range(nd):
+        a = Fa[d].cpu().numpy()[faces_of_active(g, d + 1)]
+        b = Fb[d].cpu().numpy()[faces_of_active(g, d + 1)]
+        for pl in range(8):
+            e = np.abs(a[pl] - b[pl]).max() / max(np.abs(a[pl]).max(), 1e-300)
+            assert e < 1e-12, (d + 1, pl, e)
+        assert abs(ndt_a[d] - ndt_b[d]) <= 1e-12 * ndt_a[d]
+    dt0 = 1.0 / sum(1.0 / x for x in ndt_a[:nd])
+    Pa, Pb = Pd.clone(), Pd.clone()
+    dta, sta = dev.step_ch(Pa, dt0, precision=HARM_PREC_FP64, nsteps=5)
+    dtb, stb = dev.step_ch(Pb, dt0, precision=HARM_PREC_FP64_FMA, nsteps=5)
+    a = Pa.cpu().numpy()[(slice(None),) + g.active]
+    b = Pb.cpu().numpy()[(slice(None),) + g.active]
+    tol = 1e-6 if g.g.lim == 2 else 1e-10
+    for pl in range(8):
+        e = np.abs(a[pl] - b[pl]).max() / max(np.abs(a[pl]).max(), 1e-300)
+        assert e < tol, (pl, e)
+    assert abs(dta - dtb) <= tol * dta
+    assert abs(stb["newton_iters"] - sta["newton_iters"]) <= 0.01 * sta["newton_iters"]
 
 
 @pytest.mark.parametrize("lim", [0, 1, 2])

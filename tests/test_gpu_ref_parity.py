@@ -172,3 +172,37 @@ def test_live_full_steps_device(cuda, name):
                     assert normwise(a[pl], b[pl]) < tol, (s, pl, normwise(a[pl], b[pl]))
     finally:
         h.close()
+
+
+@pytest.mark.parametrize("finalstep", [1, 0])
+@pytest.mark.parametrize("name", ["2d_32x32", "3d_32x24x8"])
+def test_live_post_fixup_planted_failures_device(cuda, name, finalstep):
+    """the device's post_fixup (harm_b200_post_fixup) on the reference's bounded substep state
+    with planted failure flags of every code (random cells, cells at every boundary, a block
+    whose centre has no usable neighbour, the reset region): values and flags equal the
+    reference's post_fixup"""
+    from test_ref_pins import FIXUP, normwise, planted_failures
+    from oracle import ref as R
+    n1, n2, n3, ng, tol, how = FIXUP[name]
+    if not R.available(n1, n2, n3, ng):
+        pytest.skip("reference binary not built")
+    g = Grid.torus(n1, n2, n3, lim=0)
+    rr = R.RefRun(R.run(n1, n2, n3, ng, lim=0, nsteps=1, every=1, substeps=(1,)), g)
+    P = rr.sub(1, 0, "fixin")
+    fl = planted_failures(n1, n2, n3)
+    out, flr = R.fixup(n1, n2, n3, ng, P, fl, finalstep=finalstep)
+    h = Harm(g, rr.geom, rr.conn, rr.aux)
+    try:
+        Pd = dev(cuda, P)
+        flh = np.zeros(P.shape[1:], np.int8)
+        flh[g.active] = fl.astype(np.int8)
+        fd = dev(cuda, flh)
+        h.post_fixup(Pd, fd, finalstep)
+        a = Pd.cpu().numpy()[(slice(None),) + g.active]
+        b = out[(slice(None),) + g.active]
+        err = rel if how == "rel" else normwise
+        for pl in range(8):
+            assert err(a[pl], b[pl]) < tol, (pl, err(a[pl], b[pl]))
+        assert (fd.cpu().numpy()[g.active] == flr[g.active]).all()
+    finally:
+        h.close()

@@ -258,3 +258,63 @@ def test_live_full_steps(name):
             b = rr.state(s)[act]
             for pl in range(8):
                 assert normwise(P[act][pl], b[pl]) < tol, (s, pl)
+
+
+# ------------------------------------------------------------------ post_fixup with failures
+
+FIX_CODES = (1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 50, 51, -1)
+
+
+def planted_failures(n1, n2, n3, seed=3):
+    """failure flags [n3][n2][n1] of every code the inversion reports, at random cells, at cells
+    next to each grid boundary, in a 3x3 block (whose centre has no usable neighbour) inside and
+    at the inner radial edge (the reset region of fixup_nogood) -- the cases post_fixup treats
+    differently"""
+    rng = np.random.default_rng(seed)
+    fl = np.zeros((n3, n2, n1))
+    for c in FIX_CODES:
+        for _ in range(3):
+            fl[rng.integers(0, n3), rng.integers(0, n2), rng.integers(0, n1)] = c
+    k0 = n3 // 2
+    for c, (j, i) in zip((1, 14, 1, 9, 15, 10, 1, 14),
+                         ((0, 12), (n2 - 1, 14), (10, 0), (11, n1 - 1), (1, 20), (n2 - 2, 3), (5, n1 - 2), (n2 // 2, 1))):
+        fl[k0, j, i] = c
+    fl[k0, n2 // 2 - 1:n2 // 2 + 2, n1 // 2 - 1:n1 // 2 + 2] = 1
+    fl[k0, 3:6, 0:3] = 14
+    if n3 > 1:
+        fl[0, 7, 17] = 1
+        fl[n3 - 1, 8, 19] = 14
+        fl[0, 0, n1 - 1] = 1
+    return fl
+
+
+# 3-D: the reference's metric varies with x3 by ~1e-11 (see LIVE), which the Lorentz-factor
+# limit of a fixed velocity sees
+FIXUP = {"2d_32x32": (32, 32, 1, 4, 1e-12, "rel"), "3d_32x24x8": (32, 24, 8, 4, 1e-10, "norm")}
+
+
+@pytest.mark.parametrize("finalstep", [1, 0])
+@pytest.mark.parametrize("name", list(FIXUP))
+def test_live_post_fixup_planted_failures(name, finalstep):
+    """post_fixup of the reference on its own bounded substep state with planted failure flags
+    of every code: the oracle's values (to 1e-12) and flags equal the reference's"""
+    n1, n2, n3, ng, tol, how = FIXUP[name]
+    if not R.available(n1, n2, n3, ng):
+        pytest.skip("reference binary not built (oracle/ref/build.sh needs the reference sources)")
+    g = Grid.torus(n1, n2, n3, lim=0)
+    rr = R.RefRun(R.run(n1, n2, n3, ng, lim=0, nsteps=1, every=1, substeps=(1,)), g)
+    P = rr.sub(1, 0, "fixin")
+    fl = planted_failures(n1, n2, n3)
+    out, flr = R.fixup(n1, n2, n3, ng, P, fl, finalstep=finalstep)
+    orc = O.Oracle(g, rr.geom, rr.conn, rr.aux)
+    Po = P.copy()
+    flo = np.zeros(P.shape[1:], np.int8)
+    flo[g.active] = fl.astype(np.int8)
+    orc.post_fixup(Po, flo, finalstep)
+    act = (slice(None),) + g.active
+    err = rel if how == "rel" else normwise
+    for pl in range(8):
+        assert err(Po[act][pl], out[act][pl]) < tol, pl
+    assert (flo[g.active] == flr[g.active]).all()
+    # the planted cells were changed where the reference changed them
+    assert (np.abs(out[act] - P[act]).max(axis=0) > 0).sum() > 30
