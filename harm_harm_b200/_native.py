@@ -62,6 +62,8 @@ _DEVICE_SIGS = {
     "harm_b200_advance": (Ip, [P, Ip, Ip, Ip, Ip, P, P, P, P, D, C.POINTER(D), C.POINTER(D), C.POINTER(D),
                                C.POINTER(harm_stats)]),
     "harm_b200_post_fixup": (Ip, [P, P, P, Ip]),
+    "harm_b200_advance_u": (Ip, [P, Ip, Ip, Ip, Ip, P, P, P, P, P, P, P, D, C.POINTER(D), C.POINTER(D), C.POINTER(D),
+                                 C.POINTER(harm_stats)]),
     "harm_b200_from_harm_layout": (Ip, [P, P, P]),
     "harm_b200_to_harm_layout": (Ip, [P, P, P]),
     "harm_b200_flags_to_harm": (Ip, [P, P, P, Ip]),

@@ -206,16 +206,20 @@ static int check_precision(int precision) {
   return 0;
 }
 
+// u: the caller's conserved arrays of the RK step (ui, uf, ucum) or NULL
 static int substep(harm_ctx* c, int precision, int guess, int timeorder, int numtimeorders, const double* d_pi,
                    const double* d_pb, double* d_pf, int8_t* d_pflag, const double* CUf, const double* Cunew,
-                   unsigned long long* slots, bool with_stats, const SlabWait* sw = nullptr) {
+                   unsigned long long* slots, bool with_stats, const SlabWait* sw = nullptr,
+                   double* const* u = nullptr) {
   if (int rc = check_guess(c, guess)) return rc;
   if (int rc = check_precision(precision)) return rc;
-  StepCoef sc;
-  sc.CUf0 = CUf[0]; sc.CUf2 = CUf[2];
+  StepCoef sc{};
+  sc.CUf0 = CUf[0]; sc.CUf1 = CUf[1]; sc.CUf2 = CUf[2];
   sc.Cun0 = Cunew[0]; sc.Cun1 = Cunew[1]; sc.Cun2 = Cunew[2];
   sc.finalstep = (timeorder == numtimeorders - 1);
   sc.guess = guess;
+  sc.first = (timeorder == 0);
+  if (u) { sc.ui = u[0]; sc.uf = u[1]; sc.ucum = u[2]; }
   double* st = with_stats ? c->d_stats : nullptr;
   if (precision == HARM_PREC_FP64) {
     if (hp_fluxes_fp64(c, d_pb, c->d_F[0], c->d_F[1], c->d_F[2], c->d_emf, slots, sw)) return 1;
@@ -259,7 +263,8 @@ extern "C" int harm_b200_advance(harm_ctx* c, int precision, int guess, int time
   // CUf2 dt dU (UFSET global.stepch.h:1 without the CUf1 U_f term) and, on the final
   // substep, ucum = Cunew0 U_i + Cunew1 dt dU + Cunew2 U_f (UCUMUPDATE :10 into an empty
   // ucum).  That is exact for setup_rktimestep's TIMEORDER 1 and its RK2 midpoint; sets that
-  // carry U_f or ucum across substeps (TVD RK2, RK3, RK4) are refused.
+  // carry U_f or ucum across substeps (TVD RK2, RK3, RK4) are refused here and run through
+  // harm_b200_advance_u, which takes the conserved arrays.
   if (timeorder < 0 || numtimeorders < 1 || timeorder >= numtimeorders)
     return seterr_msg("timeorder must lie in [0, numtimeorders)", 2);
   if (CUf[1] != 0.0 || (timeorder < numtimeorders - 1 && (Cunew[0] != 0.0 || Cunew[1] != 0.0 || Cunew[2] != 0.0)))
@@ -270,6 +275,34 @@ extern "C" int harm_b200_advance(harm_ctx* c, int precision, int guess, int time
   CK(cudaMemcpyAsync(c->d_dt, c->h_scal, sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemsetAsync(c->d_stats, 0, 5 * sizeof(double), c->stream));
   if (substep(c, precision, guess, timeorder, numtimeorders, d_pi, d_pb, d_pf, d_pflag, CUf, Cunew, c->d_dtslots, true))
+    return 1;
+  if (hp_copy_ghosts(c, d_pb, d_pf)) return 1;
+  if (hp_finalize_dt(c, nullptr, c->d_ndt, 1)) return 1;
+  CK(cudaMemcpyAsync(c->h_scal + 1, c->d_ndt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(c->h_scal + 8, c->d_stats, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (int rc = check_status(c)) return rc;
+  if (ndt) *ndt = c->h_scal[1];
+  add_stats(c, stats, (double)d.n1 * d.n2 * d.n3, guess);
+  return 0;
+}
+
+// advance() with the RK step's conserved arrays (advance.c:85-91): every setup_rktimestep
+// coefficient set, U_f and ucum carried across the substeps in the caller's d_uf, d_ucum
+extern "C" int harm_b200_advance_u(harm_ctx* c, int precision, int guess, int timeorder, int numtimeorders,
+                                   const double* d_pi, const double* d_pb, double* d_pf, int8_t* d_pflag,
+                                   double* d_ui, double* d_uf, double* d_ucum, double dt, const double CUf[4],
+                                   const double Cunew[4], double* ndt, harm_stats* stats) {
+  if (timeorder < 0 || numtimeorders < 1 || timeorder >= numtimeorders)
+    return seterr_msg("timeorder must lie in [0, numtimeorders)", 2);
+  if (!d_ui || !d_uf || !d_ucum) return seterr_msg("null conserved array", 1);
+  Dims d = dims_of(c->g);
+  c->h_scal[0] = dt;
+  CK(cudaMemcpyAsync(c->d_dt, c->h_scal, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->d_stats, 0, 5 * sizeof(double), c->stream));
+  double* const u[3] = {d_ui, d_uf, d_ucum};
+  if (substep(c, precision, guess, timeorder, numtimeorders, d_pi, d_pb, d_pf, d_pflag, CUf, Cunew, c->d_dtslots, true,
+              nullptr, u))
     return 1;
   if (hp_copy_ghosts(c, d_pb, d_pf)) return 1;
   if (hp_finalize_dt(c, nullptr, c->d_ndt, 1)) return 1;
@@ -443,9 +476,9 @@ extern "C" int harm_b200_time_stages(harm_ctx* c, int precision, int guess, cons
   c->h_scal[0] = dt;
   CK(cudaMemcpyAsync(c->d_dt, c->h_scal, sizeof(double), cudaMemcpyHostToDevice, c->stream));
   for (int q = 0; q < 5; q++) ms[q] = 0.0;
-  StepCoef sc;
+  StepCoef sc{};
   sc.CUf0 = CUf[0]; sc.CUf2 = CUf[2]; sc.Cun0 = Cun[0]; sc.Cun1 = Cun[1]; sc.Cun2 = Cun[2];
-  sc.finalstep = 0; sc.guess = guess;
+  sc.finalstep = 0; sc.guess = guess; sc.first = 1;
   for (int r = 0; r < reps; r++) {
     CK(cudaEventRecord(ev[0], c->stream));
     if (precision == HARM_PREC_FP64) {

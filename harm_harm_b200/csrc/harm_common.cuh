@@ -870,10 +870,20 @@ __global__ void __launch_bounds__(256) k_emf(Dims d, const T* __restrict__ F1, c
 
 // ------------------------------------------------------------------ update + inversion
 
+// RK coefficients of one substep (setup_rktimestep step_ch.c:1171) and, where the caller keeps
+// the step's conserved arrays (harm_b200_advance_u), their device pointers: ui = primtoU(p_i)
+// is written, uf and ucum are read (from the second substep on) and written, as
+// advance_standard's dUtoU does (advance.c:2046).  Without them the substep's uf and ucum
+// start from zero, which is exact for the coefficient sets that never carry them (TIMEORDER 1,
+// the RK2 midpoint).
 struct StepCoef {
-  double CUf0, CUf2, Cun0, Cun1, Cun2;
+  double CUf0, CUf1, CUf2, Cun0, Cun1, Cun2;
   int finalstep;
   int guess;
+  int first;        // the step's first substep (uf and ucum start from zero)
+  double* ui;       // NULL: no conserved arrays
+  double* uf;
+  double* ucum;
 };
 
 template <typename T>
@@ -1065,10 +1075,21 @@ __global__ void __launch_bounds__(256, HARM_CONSERVED_BLOCKS) k_conserved(Dims d
   const double dt = *dtp;
 #pragma unroll
   for (int p = 0; p < NPR; p++) {
+    const size_t q = (size_t)p * d.cells + id;
     double dU = dU_cell<T>(d, ii, jj, kk, p, F1, F2, F3, emf, idx1, idx2, idx3);
-    double Uf = sc.CUf0 * Ui[p] + sc.CUf2 * dt * (dU + dUg[p]);
-    double ucum = sc.Cun0 * Ui[p] + sc.Cun1 * dt * (dU + dUg[p]) + sc.Cun2 * Uf;
-    Uout[(size_t)p * d.cells + id] = sc.finalstep ? ucum : Uf;
+    if (sc.uf) {  // UFSET, ucum += UCUMUPDATE (global.stepch.h:1, :10) with the caller's arrays
+      const double ufo = sc.first ? 0.0 : sc.uf[q], uco = sc.first ? 0.0 : sc.ucum[q];
+      const double Uf = sc.CUf0 * Ui[p] + sc.CUf1 * ufo + sc.CUf2 * dt * (dU + dUg[p]);
+      const double uc = uco + (sc.Cun0 * Ui[p] + sc.Cun1 * dt * (dU + dUg[p]) + sc.Cun2 * Uf);
+      sc.ui[q] = Ui[p];
+      sc.uf[q] = Uf;
+      sc.ucum[q] = uc;
+      Uout[q] = sc.finalstep ? uc : Uf;
+    } else {
+      double Uf = sc.CUf0 * Ui[p] + sc.CUf2 * dt * (dU + dUg[p]);
+      double ucum = sc.Cun0 * Ui[p] + sc.Cun1 * dt * (dU + dUg[p]) + sc.Cun2 * Uf;
+      Uout[q] = sc.finalstep ? ucum : Uf;
+    }
   }
 }
 
@@ -1115,6 +1136,21 @@ __global__ void __launch_bounds__(256, HARM_CONSERVED_SRC_BLOCKS) k_conserved_sr
   double dUg[NPR];
   if constexpr (STAGE) source_conn<false>(pr, q, g, s_tab, kStageTI, il, dUg);
   else source_conn(pr, q, g, conn, d.plane, c2, dUg);
+  if (sc.uf) {
+    // the caller's conserved arrays: uf and ucum without the flux divergence, which
+    // k_conserved_div adds (both are linear in it)
+    const double dt = *dtp;
+#pragma unroll
+    for (int p = 0; p < NPR; p++) {
+      const size_t q = (size_t)p * d.cells + id;
+      const double ufo = sc.first ? 0.0 : sc.uf[q], uco = sc.first ? 0.0 : sc.ucum[q];
+      const double Uf = sc.CUf0 * Ui[p] + sc.CUf1 * ufo + sc.CUf2 * dt * dUg[p];
+      sc.ui[q] = Ui[p];
+      sc.uf[q] = Uf;
+      sc.ucum[q] = uco + (sc.Cun0 * Ui[p] + sc.Cun1 * dt * dUg[p] + sc.Cun2 * Uf);
+    }
+    return;
+  }
   double a, b;
   conserved_ab(sc, a, b);
   const double bdt = b * *dtp;
@@ -1132,6 +1168,19 @@ __global__ void __launch_bounds__(256) k_conserved_div(Dims d, Phys ph, StepCoef
   int ii = i + d.ng, jj = j + d.ng, kk = k + d.ng3;
   const size_t id = cidx(d, ii, jj, kk);
   const double idx1 = 1.0 / ph.dx1, idx2 = 1.0 / ph.dx2, idx3 = 1.0 / ph.dx3;
+  if (sc.uf) {
+    const double dt = *dtp, bf = sc.CUf2 * dt, bc = (sc.Cun1 + sc.Cun2 * sc.CUf2) * dt;
+#pragma unroll
+    for (int p = 0; p < NPR; p++) {
+      const size_t q = (size_t)p * d.cells + id;
+      const double dU = dU_cell<T>(d, ii, jj, kk, p, F1, F2, F3, emf, idx1, idx2, idx3);
+      const double uf = sc.uf[q] + bf * dU, uc = sc.ucum[q] + bc * dU;
+      sc.uf[q] = uf;
+      sc.ucum[q] = uc;
+      U[q] = sc.finalstep ? uc : uf;
+    }
+    return;
+  }
   double a, b;
   conserved_ab(sc, a, b);
   const double bdt = b * *dtp;

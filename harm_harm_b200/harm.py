@@ -201,6 +201,19 @@ class Harm:
                     "advance")
         return ndt.value, st.as_dict()
 
+    def advance_u(self, timeorder: int, numtimeorders: int, pi, pb, pf, pflag, ui, uf, ucum, dt: float, CUf, Cunew,
+                  precision: int = N.HARM_PREC_FP64, guess: int = N.HARM_GUESS_PREV):
+        """one RK substep with the step's conserved arrays ui, uf, ucum (advance.c:85-91): every
+        coefficient set of setup_rktimestep"""
+        CUf = (C.c_double * 4)(*CUf)
+        Cun = (C.c_double * 4)(*Cunew)
+        ndt = C.c_double()
+        st = N.harm_stats()
+        self._check(self._ordered(self.lib.harm_b200_advance_u, self._ctx, precision, guess, timeorder, numtimeorders,
+                                  _ptr(pi), _ptr(pb), _ptr(pf), _ptr(pflag), _ptr(ui), _ptr(uf), _ptr(ucum), dt, CUf, Cun,
+                                  C.byref(ndt), C.byref(st)), "advance_u")
+        return ndt.value, st.as_dict()
+
     def post_fixup(self, pf, pflag, finalstep: int = 1) -> None:
         self._check(self._ordered(self.lib.harm_b200_post_fixup, self._ctx, _ptr(pf), _ptr(pflag), int(finalstep)),
                     "post_fixup")

@@ -219,11 +219,25 @@ int harm_b200_fluxcalc(harm_ctx *ctx, int precision, const double *d_pb,
    d_pflag[k][j][i] (active and ghost layout of P) receives the inversion codes.
    Coefficients: U_f and ucum are formed from U_i and dU of this substep only, which is exact
    for setup_rktimestep's TIMEORDER 1 and RK2 midpoint (CUf[1] = 0; Cunew[0..2] = 0 before
-   the final substep); other sets (TVD RK2, RK3, RK4) return 2. */
+   the final substep); other sets (TVD RK2, RK3, RK4) return 2: they run through
+   harm_b200_advance_u, which takes the RK step's conserved arrays. */
 int harm_b200_advance(harm_ctx *ctx, int precision, int guess, int timeorder,
                       int numtimeorders, const double *d_pi, const double *d_pb,
                       double *d_pf, int8_t *d_pflag, double dt, const double CUf[4],
                       const double Cunew[4], double *ndt, harm_stats *stats);
+
+/* advance() with the RK step's conserved arrays, as advance.c:85-91 takes ui, uf, ucum:
+   d_ui, d_uf, d_ucum are [8][n3e][n2e][n1e] device arrays (UEVOLVE form, active cells used)
+   that the caller keeps across the substeps of one step.  Per active cell: ui = primtoU(pi)
+   (advance.c:454); on the first substep (timeorder 0) uf and ucum start from zero (:407);
+   uf = CUf0 ui + CUf1 uf + CUf2 dt dU and ucum += Cunew0 ui + Cunew1 dt dU + Cunew2 uf
+   (dUtoU advance.c:2046, global.stepch.h:1, :10); the inversion takes ucum on the final
+   substep and uf before.  Every coefficient set of setup_rktimestep (step_ch.c:1171:
+   TIMEORDER 1, 2 midpoint and TVD, 3, 4) runs.  The rest is harm_b200_advance's. */
+int harm_b200_advance_u(harm_ctx *ctx, int precision, int guess, int timeorder, int numtimeorders,
+                        const double *d_pi, const double *d_pb, double *d_pf, int8_t *d_pflag,
+                        double *d_ui, double *d_uf, double *d_ucum, double dt, const double CUf[4],
+                        const double Cunew[4], double *ndt, harm_stats *stats);
 
 /* post_fixup() (fixup.c:53 -> bound_pflag, fixup_utoprim fixup.c:1061) of the final substep
    (finalstep 1) or an earlier one (0): every failed active cell (flag > 0) takes the average

@@ -49,6 +49,9 @@ int orc_fluxcalc(orc *o, const double *pb, double *F1, double *F2, double *F3, d
 int orc_advance(orc *o, int timeorder, int numtimeorders, const double *pi, const double *pb,
                 double *pf, int8_t *pflag, double dt, const double CUf[4],
                 const double Cunew[4], double *ndt, harm_stats *st);
+int orc_advance_u(orc *o, int timeorder, int numtimeorders, const double *pi, const double *pb, double *pf,
+                  int8_t *pflag, double *ui, double *uf, double *ucum, double dt, const double CUf[4],
+                  const double Cunew[4], double *ndt, harm_stats *st);
 int orc_post_fixup(orc *o, double *pf, int8_t *pflag, int finalstep);
 int orc_step(orc *o, double *P, double *dt, harm_stats *st);
 

@@ -59,6 +59,7 @@ def lib() -> C.CDLL:
             "orc_fluxcalc": (I, [C.POINTER(orc), P, P, P, P, P]),
             "orc_advance": (I, [C.POINTER(orc), I, I, P, P, P, P, D, P, P, C.POINTER(D), C.POINTER(N.harm_stats)]),
             "orc_post_fixup": (I, [C.POINTER(orc), P, P, I]),
+            "orc_advance_u": (I, [C.POINTER(orc), I, I, P, P, P, P, P, P, P, D, P, P, P, P]),
             "orc_step": (I, [C.POINTER(orc), P, C.POINTER(D), C.POINTER(N.harm_stats)]),
             "orc_reconstruct_line": (None, [I, I, P, P, P]),
             "orc_paraline_flattener": (None, [I, P, P, P]),
@@ -77,7 +78,9 @@ def lib() -> C.CDLL:
     return _lib
 
 
-def _p(a: np.ndarray) -> int:
+def _p(a):
+    if a is None:
+        return None
     assert a.flags.c_contiguous
     return a.ctypes.data
 
@@ -112,6 +115,17 @@ class Oracle:
         st = N.harm_stats()
         lib().orc_advance(C.byref(self.o), timeorder, numtimeorders, _p(pi), _p(pb), _p(pf), _p(pflag), dt, _p(CUf),
                           _p(Cun), C.byref(ndt), C.byref(st))
+        return ndt.value, st.as_dict()
+
+    def advance_u(self, timeorder, numtimeorders, pi, pb, pf, pflag, ui, uf, ucum, dt, CUf, Cunew):
+        """advance with the RK step's conserved arrays ui, uf, ucum ([8][k][j][i], carried
+        across the substeps by the caller)"""
+        CUf = np.ascontiguousarray(CUf, dtype=np.float64)
+        Cun = np.ascontiguousarray(Cunew, dtype=np.float64)
+        ndt = C.c_double()
+        st = N.harm_stats()
+        lib().orc_advance_u(C.byref(self.o), timeorder, numtimeorders, _p(pi), _p(pb), _p(pf), _p(pflag), _p(ui),
+                            _p(uf), _p(ucum), dt, _p(CUf), _p(Cun), C.byref(ndt), C.byref(st))
         return ndt.value, st.as_dict()
 
     def post_fixup(self, pf, pflag, finalstep: int = 1):

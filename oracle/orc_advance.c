@@ -51,7 +51,19 @@ static void bound_flags(orc *o, int8_t *flag) {
 int orc_advance(orc *o, int timeorder, int numtimeorders, const double *pi, const double *pb,
                 double *pf, int8_t *pflag, double dt, const double CUf[4],
                 const double Cunew[4], double *ndt, harm_stats *st) {
-  (void)timeorder;
+  return orc_advance_u(o, timeorder, numtimeorders, pi, pb, pf, pflag, NULL, NULL, NULL, dt, CUf, Cunew, ndt, st);
+}
+
+/* advance_standard (advance.c:140) with the conserved arrays of the RK step: ui = primtoU(pi)
+   (advance.c:454), uf and ucum zeroed on the first substep (:407), then per cell dUtoU
+   (advance.c:2046): uf = UFSET(CUf, dt, ui, uf, dUriemann, dUgeom), ucum += UCUMUPDATE(Cunew,
+   dt, ui, uf, dUriemann, dUgeom) (global.stepch.h:1, :10), and the inversion of ucum on the
+   final substep, of uf before (:671-679).  ui, uf, ucum NULL: the substep's uf and ucum start
+   from zero (exact for TIMEORDER 1 and the RK2 midpoint, whose coefficients never carry them
+   across substeps). */
+int orc_advance_u(orc *o, int timeorder, int numtimeorders, const double *pi, const double *pb, double *pf,
+                  int8_t *pflag, double *ui, double *uf, double *ucum, double dt, const double CUf[4],
+                  const double Cunew[4], double *ndt, harm_stats *st) {
   const harm_grid *g = &o->g;
   const size_t cells = o->cells, plane = o->plane;
   const int finalstep = (timeorder == numtimeorders - 1);
@@ -90,11 +102,16 @@ int orc_advance(orc *o, int timeorder, int numtimeorders, const double *pi, cons
         o_get_state(prb, &gc, g->gam, &qb);
         o_source(prb, &qb, &gc, conn, dUg);
         for (int p = 0; p < HARM_NPR; p++) {
-          /* UFSET / UCUMUPDATE (global.stepch.h:5,10) with CUf[1]=0 and, for the
-             midpoint RK2, ucum starting from zero on the first substep */
-          double Uf = CUf[0] * Ui[p] + CUf[2] * dt * (dU[p] + dUg[p]);
-          double ucum = Cunew[0] * Ui[p] + Cunew[1] * dt * (dU[p] + dUg[p]) + Cunew[2] * Uf;
-          Uinv[p * cells + id] = finalstep ? ucum : Uf;
+          /* UFSET / UCUMUPDATE (global.stepch.h:1, :10) */
+          const size_t q = p * cells + id;
+          const double ufo = (uf && timeorder > 0) ? uf[q] : 0.0;
+          const double uco = (ucum && timeorder > 0) ? ucum[q] : 0.0;
+          double Uf = CUf[0] * Ui[p] + CUf[1] * ufo + CUf[2] * dt * (dU[p] + dUg[p]);
+          double uc = uco + (Cunew[0] * Ui[p] + Cunew[1] * dt * (dU[p] + dUg[p]) + Cunew[2] * Uf);
+          if (ui) ui[q] = Ui[p];
+          if (uf) uf[q] = Uf;
+          if (ucum) ucum[q] = uc;
+          Uinv[q] = finalstep ? uc : Uf;
         }
       }
   /* pf = pb everywhere (copy_3dnpr_fullloop advance.c:654), then invert active cells */

@@ -16,7 +16,8 @@
  *   HREF_LIM        mc | para | paraline | weno5 | weno5bnd   (lim[1..3], default mc;
  *                   weno5 is lim WENO5, weno5bnd lim WENO5BND)
  *   HREF_FLUX       hll | laxf                          (fluxmethod, default hll)
- *   HREF_TIMEORDER  1 | 2                               (TIMEORDER, default 2)
+ *   HREF_TIMEORDER  1 | 2 | 3 | 4                       (TIMEORDER, default 2: setup_rktimestep's
+ *                                                        Euler, RK2 midpoint, TVD RK3, RK4)
  *   HREF_COUR       Courant factor                      (default 0.8)
  *   HREF_SEED       seed of ranc() for the perturbation (default 12345)
  *

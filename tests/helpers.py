@@ -127,3 +127,12 @@ def harm_with_env(g, geom, conn, aux, **env):
                 del os.environ[k]
             else:
                 os.environ[k] = v
+
+
+def divb_rel(grid, geom, P):
+    """max of the corner divergence of sqrt(-g) B relative to max |sqrt(-g) B| / min dx (the
+    size a divergence of the field itself would have)"""
+    g = grid.g
+    U = np.abs(P[5:8] * geom[0, 26][None, None, :, :])
+    dxs = [g.dx[1], g.dx[2]] + ([g.dx[3]] if g.n3 > 1 else [])
+    return float(divb_corner(grid, geom, P).max() / (U.max() / min(dxs)))

@@ -173,10 +173,13 @@ def test_mixed_precision_close_to_fp64(setup, cuda):
 def test_fp64_fma_close_to_fp64(setup, cuda):
     """The FP64 path compiled with FMA contraction and shared reciprocals (the FP64 path at
     its best speed) against the IEEE-ordered FP64 path: the fluxes of one state to 1e-12 of
-    each field's largest face value, five steps to 1e-10 of each field's maximum (WENO5:
-    1e-6, since its SMONO indicator switches a cell between the 5-point and the WENO edge
-    where the edge derivatives are within ~1e-13 of the stencil's magnitude, so round-off
-    differences flip a few cells)."""
+    each field's largest face value, five steps to 1e-10 of each field's maximum.  WENO5's
+    SMONO indicator switches a cell between the 5-point and the WENO edge where the edge
+    derivatives are within ~1e-13 of the stencil's magnitude, and PARALINE's flattener and
+    monotonicity checks compare against thresholds, so there round-off differences flip a few
+    faces: at most 1 % of the faces differ by more than 1e-12, the fluxes agree to 1e-4 in L1
+    for WENO5 and 3e-2 for PARALINE (a flipped flattening of the planted jump moves its faces'
+    fluxes by up to ~10 %), and the states after five steps to 1e-6."""
     g, geom, conn, aux, P, orc, dev = setup
     Pd = dev_array(cuda, P)
     Fa = [cuda.zeros_like(Pd) for _ in range(3)]
@@ -184,20 +187,26 @@ def test_fp64_fma_close_to_fp64(setup, cuda):
     ndt_a = dev.fluxcalc(Pd, *Fa, precision=HARM_PREC_FP64)
     ndt_b = dev.fluxcalc(Pd, *Fb, precision=HARM_PREC_FP64_FMA)
     nd = 3 if g.g.n3 > 1 else 2
+    switching = g.g.lim in (2, 3)
     for d in range(nd):
         a = Fa[d].cpu().numpy()[faces_of_active(g, d + 1)]
         b = Fb[d].cpu().numpy()[faces_of_active(g, d + 1)]
         for pl in range(8):
-            e = np.abs(a[pl] - b[pl]).max() / max(np.abs(a[pl]).max(), 1e-300)
-            assert e < 1e-12, (d + 1, pl, e)
-        assert abs(ndt_a[d] - ndt_b[d]) <= 1e-12 * ndt_a[d]
+            scale = max(np.abs(a[pl]).max(), 1e-300)
+            diff = np.abs(a[pl] - b[pl])
+            if switching:
+                assert (diff > 1e-12 * scale).mean() <= 0.01, (d + 1, pl, (diff > 1e-12 * scale).mean())
+                assert diff.sum() <= (1e-4 if g.g.lim == 2 else 3e-2) * max(np.abs(a[pl]).sum(), 1e-300), (d + 1, pl)
+            else:
+                assert diff.max() / scale < 1e-12, (d + 1, pl, diff.max() / scale)
+        assert abs(ndt_a[d] - ndt_b[d]) <= (1e-6 if switching else 1e-12) * ndt_a[d]
     dt0 = 1.0 / sum(1.0 / x for x in ndt_a[:nd])
     Pa, Pb = Pd.clone(), Pd.clone()
     dta, sta = dev.step_ch(Pa, dt0, precision=HARM_PREC_FP64, nsteps=5)
     dtb, stb = dev.step_ch(Pb, dt0, precision=HARM_PREC_FP64_FMA, nsteps=5)
     a = Pa.cpu().numpy()[(slice(None),) + g.active]
     b = Pb.cpu().numpy()[(slice(None),) + g.active]
-    tol = 1e-6 if g.g.lim == 2 else 1e-10
+    tol = 1e-6 if switching else 1e-10
     for pl in range(8):
         e = np.abs(a[pl] - b[pl]).max() / max(np.abs(a[pl]).max(), 1e-300)
         assert e < tol, (pl, e)

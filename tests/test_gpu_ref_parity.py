@@ -206,3 +206,44 @@ def test_live_post_fixup_planted_failures_device(cuda, name, finalstep):
         assert (fd.cpu().numpy()[g.active] == flr[g.active]).all()
     finally:
         h.close()
+
+
+@pytest.mark.parametrize("timeorder", [3, 4])
+def test_live_rk_steps_device(cuda, timeorder):
+    """TVD RK3 and RK4 through harm_b200_advance_u (the RK step's conserved arrays ui, uf, ucum
+    carried by the caller across the substeps, as HARM's advance() takes them): four full steps
+    of the 2-D MC torus from the reference's initial state equal the reference's states, dt and
+    Newton counts; the mixed path's steps stay within 1e-4 of each field's largest value"""
+    from test_ref_pins import RK_WIRING, normwise, rk_step
+    from oracle import ref as R
+    from harm_harm_b200 import HARM_PREC_MIXED
+    n1, n2, n3, ng = 64, 64, 1, 4
+    if not R.available(n1, n2, n3, ng):
+        pytest.skip("reference binary not built")
+    g = Grid.torus(n1, n2, n3, lim=0)
+    rr = R.RefRun(R.run(n1, n2, n3, ng, lim=0, nsteps=4, every=1, timeorder=timeorder, substeps=(1,)), g)
+    coefs = [(rr.sub(1, s, "args")[4:8].copy(), rr.sub(1, s, "args")[8:12].copy()) for s in range(timeorder)]
+    h = Harm(g, rr.geom, rr.conn, rr.aux)
+    act = (slice(None),) + g.active
+    try:
+        for precision in (0, HARM_PREC_MIXED):
+            P = dev(cuda, rr.state(0))
+            h.bound_prim(P)
+            dt = rr.dt0
+
+            def adv(s, n, pi, pb, pf, flag, ui, uf, ucum, dt_, CUf, Cun):
+                return h.advance_u(s, n, pi, pb, pf, flag, ui, uf, ucum, dt_, CUf, Cun, precision=precision)
+
+            for s in range(1, 5):
+                ndt, iters = rk_step(adv, h.bound_prim, h.post_fixup, P, dt, coefs, RK_WIRING[timeorder], P.shape)
+                dt = min(ndt, g.g.safe * dt)
+                b = rr.state(s)[act]
+                a = P.cpu().numpy()[act]
+                tol = 1e-12 if precision == 0 else 1e-4
+                for pl in range(8):
+                    assert normwise(a[pl], b[pl]) < tol, (precision, s, pl, normwise(a[pl], b[pl]))
+                if precision == 0:
+                    assert abs(iters - rr.steps[s, 2]) <= 1e-4 * rr.steps[s, 2], (s, iters, rr.steps[s, 2])
+                    assert abs(dt - rr.dt_of_step(s + 1)) <= 1e-13 * dt if s < 4 else True
+    finally:
+        h.close()

@@ -318,3 +318,64 @@ def test_live_post_fixup_planted_failures(name, finalstep):
     assert (flo[g.active] == flr[g.active]).all()
     # the planted cells were changed where the reference changed them
     assert (np.abs(out[act] - P[act]).max(axis=0) > 0).sum() > 30
+
+
+# ------------------------------------------------------------------ higher-order RK steps
+
+# setup_rktimestep (step_ch.c:1171) wiring of each substep's p_i, p_b, p_f among p and the
+# two scratch states pk[0], pk[1]: 0 = p, 1 = pk[0], 2 = pk[1]
+RK_WIRING = {3: ((0, 0, 1), (0, 1, 2), (0, 2, 0)),
+             4: ((0, 0, 1), (0, 1, 2), (0, 2, 1), (0, 1, 0))}
+
+
+def rk_step(adv, bound, post_fixup, P, dt, coefs, wiring, shape):
+    """one full step of HARM's step_ch_simplempi loop (step_ch.c:524-830) with the RK step's
+    conserved arrays ui, uf, ucum carried across the substeps: per substep advance, bound_prim,
+    post_fixup, bound_prim; returns the next dt (post_stepch) and the Newton iterations"""
+    if isinstance(P, np.ndarray):
+        states = [P, np.zeros_like(P), np.zeros_like(P)]
+        ui, uf, ucum = (np.zeros(shape) for _ in range(3))
+        flag = np.zeros(P.shape[1:], np.int8)
+    else:  # torch CUDA tensors (the device path)
+        import torch
+        states = [P, torch.zeros_like(P), torch.zeros_like(P)]
+        ui, uf, ucum = (torch.zeros_like(P) for _ in range(3))
+        flag = torch.zeros(P.shape[1:], dtype=torch.int8, device=P.device)
+    n = len(wiring)
+    ndt, iters = 1e300, 0.0
+    for s, (i, b, f) in enumerate(wiring):
+        CUf, Cun = coefs[s]
+        nd, st = adv(s, n, states[i], states[b], states[f], flag, ui, uf, ucum, dt, CUf, Cun)
+        ndt = min(ndt, nd)
+        iters += st["newton_iters"]
+        bound(states[f])
+        post_fixup(states[f], flag, 1 if s == n - 1 else 0)
+        bound(states[f])
+    return ndt, iters
+
+
+@pytest.mark.parametrize("timeorder", [3, 4])
+def test_live_rk_steps(timeorder):
+    """TVD RK3 and RK4 (TIMEORDER 3 and 4 of setup_rktimestep, which carry U_f and ucum across
+    the substeps): four full steps of the 2-D MC torus from the reference's initial state equal
+    the reference's states, dt and Newton iteration counts"""
+    n1, n2, n3, ng = 64, 64, 1, 4
+    if not R.available(n1, n2, n3, ng):
+        pytest.skip("reference binary not built (oracle/ref/build.sh needs the reference sources)")
+    g = Grid.torus(n1, n2, n3, lim=0)
+    rr = R.RefRun(R.run(n1, n2, n3, ng, lim=0, nsteps=4, every=1, timeorder=timeorder, substeps=(1,)), g)
+    coefs = [(rr.sub(1, s, "args")[4:8].copy(), rr.sub(1, s, "args")[8:12].copy()) for s in range(timeorder)]
+    orc = O.Oracle(g, rr.geom, rr.conn, rr.aux)
+    P = rr.state(0)
+    orc.bound_prim(P)
+    dt = rr.dt0
+    act = (slice(None),) + g.active
+    for s in range(1, 5):
+        assert abs(dt - rr.dt_of_step(s)) <= 1e-13 * dt, (s, dt, rr.dt_of_step(s))
+        ndt, iters = rk_step(orc.advance_u, orc.bound_prim, orc.post_fixup, P, dt, coefs, RK_WIRING[timeorder],
+                             P.shape)
+        assert iters == rr.steps[s, 2], (s, iters, rr.steps[s, 2])
+        dt = min(ndt, g.g.safe * dt)
+        b = rr.state(s)[act]
+        for pl in range(8):
+            assert normwise(P[act][pl], b[pl]) < 1e-12, (s, pl, normwise(P[act][pl], b[pl]))
