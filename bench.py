@@ -432,21 +432,40 @@ def run_ours(args, ws, rank, local):
         value_prev = ws * zones * args.steps / (msp * 1e-3)
     # div B of the headline path's state after its warm-up and timed steps
     divb_abs, divb_rel = divb_max(g, torch.from_numpy(np.ascontiguousarray(geom[0, 26])).to(Pm.device), Pm)
-    # accuracy of the headline path against the FP64 path after the same steps
+    # accuracy of the headline path against the FP64 path after the same number of steps, each
+    # path with its own CFL dt (their states then also differ by the offset of their simulation
+    # times), and with the FP64 path's dt sequence for both (the error of the arithmetic alone)
+    def steps_of(P, precision, g_, dts=None):
+        dt, used = dt0, []
+        for s in range(args.err_steps):
+            dt_in = dts[s] if dts is not None else dt
+            dt, _ = dev.step_ch(P, dt_in, precision=precision, guess=g_, nsteps=1, stats=False)
+            used.append(dt_in)
+        return used
+
     Pa, Pb = Pd.clone(), Pd.clone()
-    dev.step_ch(Pa, dt0, precision=HARM_PREC_FP64, nsteps=args.err_steps, stats=False)
-    dev.step_ch(Pb, dt0, precision=prec, guess=guess, nsteps=args.err_steps, stats=False)
+    dts64 = steps_of(Pa, HARM_PREC_FP64, HARM_GUESS_PREV)
+    dtsm = steps_of(Pb, prec, guess)
     act = (slice(None),) + g.active
     a, b = Pa.cpu().numpy()[act], Pb.cpu().numpy()[act]
     fields = (("rho", 0), ("u", 1), ("U1", 2), ("U2", 3), ("U3", 4), ("B1", 5), ("B2", 6), ("B3", 7))
-    l1 = {nm: float(np.abs(a[pl] - b[pl]).mean() / max(np.abs(a[pl]).mean(), 1e-300)) for nm, pl in fields}
-    linf = {nm: float(np.abs(a[pl] - b[pl]).max() / max(np.abs(a[pl]).max(), 1e-300)) for nm, pl in fields}
     # the velocity and field vectors measured by their length in the metric (|x|^2 = g_ij x^i x^j
     # at the cell centre): a component that is small where the vector is not (u~^2, B^3 of a
     # poloidal loop) is judged against the vector it belongs to
     gc = geom[0][:, g.active[1], g.active[2]][:, None]
-    for nm, p0 in (("U_vec", 2), ("B_vec", 5)):
-        l1[nm], linf[nm] = vector_errors(gc, a[p0:p0 + 3], b[p0:p0 + 3])
+
+    def field_errors(x, y):
+        e1 = {nm: float(np.abs(x[pl] - y[pl]).mean() / max(np.abs(x[pl]).mean(), 1e-300)) for nm, pl in fields}
+        ei = {nm: float(np.abs(x[pl] - y[pl]).max() / max(np.abs(x[pl]).max(), 1e-300)) for nm, pl in fields}
+        for nm, p0 in (("U_vec", 2), ("B_vec", 5)):
+            e1[nm], ei[nm] = vector_errors(gc, x[p0:p0 + 3], y[p0:p0 + 3])
+        return e1, ei
+
+    l1, linf = field_errors(a, b)
+    t_offset = (sum(dtsm) - sum(dts64)) / sum(dts64)
+    Pb.copy_(Pd)
+    steps_of(Pb, prec, guess, dts64)
+    l1_same, linf_same = field_errors(a, Pb.cpu().numpy()[act])
     # the round-off floor of the same evolution: the FP64 build with FMA contraction against
     # the IEEE-ordered one
     Pb.copy_(Pd)
@@ -499,6 +518,8 @@ def run_ours(args, ws, rank, local):
             "fp64_ieee_value": value64i, "speedup_vs_fp64_ieee": value / value64i,
             "plain_guess_value": value_prev if guess == HARM_GUESS_MLP else value,
             "l1_rel_err_vs_fp64": l1, "linf_rel_err_vs_fp64": linf, "err_steps": args.err_steps,
+            "sim_time_offset_vs_fp64": t_offset,
+            "l1_rel_err_vs_fp64_same_dt": l1_same, "linf_rel_err_vs_fp64_same_dt": linf_same,
             "l1_rel_err_fp64_fma_vs_fp64": l1_fma,
             "divb_max": {"abs": divb_abs, "rel": divb_rel,
                          "of": "Toth corner divergence of sqrt(-g) B after the timed steps, rel to max|sqrt(-g) B|/min dx"},

@@ -68,6 +68,7 @@ _DEVICE_SIGS = {
     "harm_b200_to_harm_layout": (Ip, [P, P, P]),
     "harm_b200_flags_to_harm": (Ip, [P, P, P, Ip]),
     "harm_b200_flags_from_harm": (Ip, [P, P, P, Ip]),
+    "harm_b200_mixed_reciprocal": (Ip, [P, P, P, C.c_size_t]),
     "harm_b200_step_host_harm": (Ip, [P, Ip, Ip, P, C.POINTER(D), C.POINTER(harm_stats)]),
     "harm_b200_step": (Ip, [P, Ip, Ip, P, C.POINTER(D), C.POINTER(harm_stats)]),
     "harm_b200_step_n": (Ip, [P, Ip, Ip, P, Ip, C.POINTER(D), C.POINTER(harm_stats)]),

@@ -164,3 +164,20 @@ int hp_update_mixed(harm_ctx* c, const StepCoef& sc, const double* pi, const dou
   CK(cudaGetLastError());
   return 0;
 }
+
+// The reciprocal of this path's inversion (frcp, harm_invert.cuh) over n device values, so
+// that its error against IEEE division can be checked over the operand range.
+__global__ void k_mixed_reciprocal(const double* __restrict__ b, double* __restrict__ r, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    r[i] = frcp(b[i]);
+}
+
+extern "C" int harm_b200_mixed_reciprocal(harm_ctx* c, const double* d_b, double* d_r, size_t n) {
+  if (!c || (n && (!d_b || !d_r))) return hb_setmsg("null argument", 1);
+  if (n == 0) return 0;
+  const size_t blocks = std::min<size_t>((n + 255) / 256, (size_t)4 * (c->num_sms > 0 ? c->num_sms : 1));
+  k_mixed_reciprocal<<<(unsigned)blocks, 256, 0, c->stream>>>(d_b, d_r, n);
+  c->launches++;
+  CK(cudaGetLastError());
+  return 0;
+}

@@ -258,6 +258,12 @@ class Harm:
         self._check(self._ordered(self.lib.harm_b200_flags_from_harm, self._ctx, _ptr(harm_pflag), _ptr(pflag), numpflags),
                     "flags_from_harm")
 
+    def mixed_reciprocal(self, b, r) -> None:
+        """r = the mixed inversion's reciprocal of b (device float64 arrays of equal size)"""
+        assert b.numel() == r.numel()
+        self._check(self._ordered(self.lib.harm_b200_mixed_reciprocal, self._ctx, _ptr(b), _ptr(r), b.numel()),
+                    "mixed_reciprocal")
+
     def Utoprimgen(self, U, geomrec, P, pflag, iters=None, guess: int = N.HARM_GUESS_PREV) -> None:
         n = U.shape[-1]
         self._check(self._ordered(self.lib.harm_b200_utoprimgen_points, self._ctx, n, guess, _ptr(U), _ptr(geomrec), _ptr(P),

@@ -281,6 +281,14 @@ int harm_b200_to_harm_layout(harm_ctx *ctx, const double *d_P, double *d_harm);
 int harm_b200_flags_to_harm(harm_ctx *ctx, const int8_t *d_pflag, int32_t *d_harm_pflag, int numpflags);
 int harm_b200_flags_from_harm(harm_ctx *ctx, const int32_t *d_harm_pflag, int8_t *d_pflag, int numpflags);
 
+/* The FP64 reciprocal that HARM_PREC_MIXED's inversion uses in place of IEEE division
+   (utoprim_jon.c's divisions in the Newton residual): the hardware approximation
+   rcp.approx.ftz.f64 refined by two Newton-Raphson steps, r[i] ~ 1/b[i] for n device
+   values, on the context's stream.  Within one ulp of the IEEE quotient where b and 1/b are
+   normal; flush-to-zero at the edges: a subnormal or zero b gives NaN, a b whose reciprocal
+   is subnormal gives 0. */
+int harm_b200_mixed_reciprocal(harm_ctx *ctx, const double *d_b, double *d_r, size_t n);
+
 /* harm_b200_step_host over a host array in HARM's layout (step_ch_full step_ch.c:35 with
    HARM's own p array): one copy per k-slab, each slab converted on the device as it arrives
    (ahead of the first substep's flux tiles that stage it), the state converted back and

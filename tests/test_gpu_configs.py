@@ -5,9 +5,10 @@ lengths, through the C ABI:
   C1  3-D 192x96x64, WENO5, FP64: device and oracle after 20 RK2 steps (the oracle's share
       of the 200-step configuration that runs in seconds on the host), 1e-10 relative, div B
       at round-off on the device;
-  C2  3-D 256x128x64, WENO5, mixed precision against the FP64 device path after 500 steps
-      with the CFL dt: per-field L1 and Linf of rho, u and the metric length of the
-      velocity and field vectors, against the bounds measured for the mixed path;
+  C2  3-D 256x128x64, WENO5, mixed precision against the FP64 device path after 500 steps,
+      with the FP64 path's dt sequence for both and with each path's own CFL dt: per-field
+      L1 and Linf of rho, u and the metric length of the velocity and field vectors, against
+      the bounds measured for the mixed path;
   C4  3-D 384x192x128, WENO5, mixed precision with the learned start (the benchmark's
       configuration), 1000 steps: finite, no failed inversion, div B at round-off, at most
       1% fallbacks from the learned start; and against the FP64 device path after 10 steps.
@@ -21,9 +22,11 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-# L1 bounds of the mixed path against the FP64 path after 500 steps of C2 (measured values
-# with a factor of ~2 of margin)
-C2_L1_BOUND = {"rho": 1e-4, "u": 1e-3, "v": 1e-2, "B": 1e-3}
+# L1 bounds of the mixed path against the FP64 path after 500 steps of C2, each path with its
+# own CFL dt (measured: rho 1.5e-6, u 1.3e-6, v 4.2e-4, B 2.6e-5) and with the FP64 path's dt
+# sequence for both
+C2_L1_BOUND = {"rho": 1e-5, "u": 1e-5, "v": 2e-3, "B": 1e-4}
+C2_SAME_DT_BOUND = {"rho": 1e-6, "u": 1e-6, "v": 1e-3, "B": 1e-4}
 
 
 def _initial_dt(orc, P):
@@ -87,30 +90,49 @@ def _field_errors(g, geom, a, b):
 
 
 def test_mixed_c2_500_steps(cuda):
-    """C2 at its stated length: the mixed path against the FP64 path after 500 CFL steps"""
+    """C2 at its stated length: the mixed path against the FP64 path after 500 steps.  With
+    the FP64 path's dt sequence for both, the difference is the FP32 arithmetic's alone: per
+    field L1 within C2_SAME_DT_BOUND.  With each path's own CFL dt the two runs also reach
+    different simulation times (the dt-setting faces near the horizon differ in the first
+    ~100 steps of the transient, by ~0.4 % on average): the time offset stays below 1 %, the
+    dts of the last 100 steps agree to 1e-3 on average, and L1 stays within C2_L1_BOUND."""
     torch = cuda
     g, geom, conn, aux, P = make_torus(256, 128, 64, lim=2)
     dev = Harm(g, geom, conn, aux)
     try:
-        Pa = torch.from_numpy(P).cuda()
-        dev.bound_prim(Pa)
-        F = [torch.empty_like(Pa) for _ in range(3)]
-        ndt = dev.fluxcalc(Pa, *F)
+        P0 = torch.from_numpy(P).cuda()
+        dev.bound_prim(P0)
+        F = [torch.empty_like(P0) for _ in range(3)]
+        ndt = dev.fluxcalc(P0, *F)
         del F
         dt0 = 1.0 / sum(1.0 / x for x in ndt)
-        Pb = Pa.clone()
-        dta, _ = dev.step_ch(Pa, dt0, precision=HARM_PREC_FP64, nsteps=500, stats=False)
-        dtb, st = dev.step_ch(Pb, dt0, precision=HARM_PREC_MIXED, nsteps=500)
+
+        def run(prec, dts=None):
+            Px, dt, used = P0.clone(), dt0, []
+            for s in range(500):
+                dt_in = dts[s] if dts is not None else dt
+                dt, st = dev.step_ch(Px, dt_in, precision=prec, nsteps=1)
+                assert st["inversion_failures"] == 0
+                used.append(dt_in)
+            return Px, np.array(used)
+
+        Pa, dta = run(HARM_PREC_FP64)
+        Pb, dtb = run(HARM_PREC_MIXED)
+        Pc, _ = run(HARM_PREC_MIXED, dta)
         act = (slice(None),) + g.active
-        a, b = Pa.cpu().numpy()[act], Pb.cpu().numpy()[act]
-        assert np.all(np.isfinite(b))
-        err = _field_errors(g, geom, a, b)
-        print("C2 500 steps, mixed against FP64 (L1, Linf):", err)
-        for nm, (l1, linf) in err.items():
-            assert l1 <= C2_L1_BOUND[nm], (nm, l1)
-        assert abs(dta - dtb) <= 1e-3 * dta
-        assert st["inversion_failures"] == 0
-        assert divb_rel(g, geom, Pb.cpu().numpy()) < 1e-12
+        a = Pa.cpu().numpy()[act]
+        for name, Px, bound in (("CFL dt", Pb, C2_L1_BOUND), ("same dt", Pc, C2_SAME_DT_BOUND)):
+            b = Px.cpu().numpy()[act]
+            assert np.all(np.isfinite(b))
+            err = _field_errors(g, geom, a, b)
+            print("C2 500 steps, mixed against FP64, %s (L1, Linf):" % name, err)
+            for nm, (l1, linf) in err.items():
+                assert l1 <= bound[nm], (name, nm, l1)
+            assert divb_rel(g, geom, Px.cpu().numpy()) < 1e-12
+        t_off = (dtb.sum() - dta.sum()) / dta.sum()
+        late = float(np.abs(dtb[-100:] / dta[-100:] - 1).mean())
+        print("C2 simulation-time offset %.3g, mean |dt/dt_fp64 - 1| over the last 100 steps %.3g" % (t_off, late))
+        assert abs(t_off) < 1e-2 and late < 1e-3
     finally:
         dev.close()
 

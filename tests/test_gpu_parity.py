@@ -179,7 +179,8 @@ def test_fp64_fma_close_to_fp64(setup, cuda):
     monotonicity checks compare against thresholds, so there round-off differences flip a few
     faces: at most 1 % of the faces differ by more than 1e-12, the fluxes agree to 1e-4 in L1
     for WENO5 and 3e-2 for PARALINE (a flipped flattening of the planted jump moves its faces'
-    fluxes by up to ~10 %), and the states after five steps to 1e-6."""
+    fluxes by up to ~10 %), and the states after five steps to 1e-5 of each field's maximum
+    (measured up to 1.8e-6 for PARALINE)."""
     g, geom, conn, aux, P, orc, dev = setup
     Pd = dev_array(cuda, P)
     Fa = [cuda.zeros_like(Pd) for _ in range(3)]
@@ -206,7 +207,7 @@ def test_fp64_fma_close_to_fp64(setup, cuda):
     dtb, stb = dev.step_ch(Pb, dt0, precision=HARM_PREC_FP64_FMA, nsteps=5)
     a = Pa.cpu().numpy()[(slice(None),) + g.active]
     b = Pb.cpu().numpy()[(slice(None),) + g.active]
-    tol = 1e-6 if switching else 1e-10
+    tol = 1e-5 if switching else 1e-10
     for pl in range(8):
         e = np.abs(a[pl] - b[pl]).max() / max(np.abs(a[pl]).max(), 1e-300)
         assert e < tol, (pl, e)
@@ -242,3 +243,40 @@ def test_mixed_tma_staging_equals_plain_loads(cuda, lim, monkeypatch):
             assert l1 < 1e-7 and mx < 1e-6, (lim, n3, pl, l1, mx)
         a.close()
         b.close()
+
+
+def test_mixed_inversion_reciprocal(cuda):
+    """The mixed inversion's FP64 reciprocal (rcp.approx.ftz.f64 and two Newton-Raphson steps)
+    against IEEE 1/b: within one ulp for normal operands with normal reciprocals, over every
+    binade of that range and densely over the operands the Newton residual divides by (W, X,
+    gamma^2, 1+gamma, E''); at the flush-to-zero edges NaN for a zero or subnormal operand and
+    0 where the reciprocal would be subnormal."""
+    from helpers import make_torus
+    torch = cuda
+    g, geom, conn, aux, _ = make_torus(16, 16, 1)
+    dev = Harm(g, geom, conn, aux)
+    try:
+        rng = np.random.default_rng(7)
+        m = rng.uniform(1.0, 2.0, 2_000_000)
+        e = rng.integers(-1022, 1022, m.size)
+        wide = np.ldexp(m, e) * rng.choice([-1.0, 1.0], m.size)
+        dense = np.concatenate([10.0 ** rng.uniform(-12, 12, 1_000_000), 1.0 + rng.uniform(0, 625, 500_000),
+                                -(10.0 ** rng.uniform(-12, 12, 500_000))])
+        for b in (wide, dense):
+            bd = torch.from_numpy(b).cuda()
+            r = torch.empty_like(bd)
+            dev.mixed_reciprocal(bd, r)
+            got = r.cpu().numpy()
+            ref = 1.0 / b
+            assert np.all(np.sign(got) == np.sign(ref))
+            ulps = np.abs(got.view(np.int64) - ref.view(np.int64))
+            assert ulps.max() <= 1, (ulps.max(), b[np.argmax(ulps)])
+        edge = np.array([0.0, -0.0, 5e-324, 2.0 ** -1030, -(2.0 ** -1023), 2.0 ** 1022 * 1.5, -(2.0 ** 1023)])
+        bd = torch.from_numpy(edge).cuda()
+        r = torch.empty_like(bd)
+        dev.mixed_reciprocal(bd, r)
+        got = r.cpu().numpy()
+        assert np.all(np.isnan(got[:5])), got
+        assert np.all(got[5:] == 0.0), got
+    finally:
+        dev.close()
