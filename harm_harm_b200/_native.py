@@ -73,6 +73,7 @@ _DEVICE_SIGS = {
     "harm_b200_step": (Ip, [P, Ip, Ip, P, C.POINTER(D), C.POINTER(harm_stats)]),
     "harm_b200_step_n": (Ip, [P, Ip, Ip, P, Ip, C.POINTER(D), C.POINTER(harm_stats)]),
     "harm_b200_step_host": (Ip, [P, Ip, Ip, P, C.POINTER(D), C.POINTER(harm_stats)]),
+    "harm_b200_step_host_n": (Ip, [P, Ip, Ip, P, Ip, C.POINTER(D), C.POINTER(harm_stats)]),
     "harm_b200_utoprimgen_points": (Ip, [P, C.c_size_t, Ip, P, P, P, P, P]),
     "harm_b200_time_stages": (Ip, [P, Ip, Ip, P, D, Ip, C.POINTER(D)]),
     "harm_b200_fluxcalc_noalloc": (Ip, [C.POINTER(harm_grid), P, P, P, P, P, C.POINTER(D), P]),

@@ -156,6 +156,12 @@ extern "C" int harm_b200_destroy(harm_ctx* c) {
     cudaEventDestroy(c->entry_ev);
     for (int s = 0; s < HARM_H2D_SLABS; s++) cudaEventDestroy(c->slab_ev[s]);
   }
+  if (c->d2h_stream) {
+    cudaStreamSynchronize(c->d2h_stream);
+    cudaStreamDestroy(c->d2h_stream);
+    cudaEventDestroy(c->done_ev);
+    for (int s = 0; s < HARM_H2D_SLABS; s++) cudaEventDestroy(c->d2h_ev[s]);
+  }
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return 0;
@@ -366,7 +372,10 @@ extern "C" int harm_b200_step(harm_ctx* c, int precision, int guess, double* d_P
 // stream's earlier work
 // harm_layout: h_P is in HARM's [k][j][i][pl] layout (one copy per slab into d_Paos, converted
 // into d_Pdev on the context stream after the slab's event)
-static int h2d_slabs(harm_ctx* c, const double* h_P, SlabWait* sw, bool harm_layout = false) {
+// after_slab (optional): per slab, an event the slab's copy waits for (the previous step's
+// D2H of the same slab, which wrote the host values this copy reads)
+static int h2d_slabs(harm_ctx* c, const double* h_P, SlabWait* sw, bool harm_layout = false,
+                     const cudaEvent_t* after_slab = nullptr) {
   if (!c->copy_stream) {
     CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&c->entry_ev, cudaEventDisableTiming));
@@ -380,6 +389,7 @@ static int h2d_slabs(harm_ctx* c, const double* h_P, SlabWait* sw, bool harm_lay
   for (int s = 0; s < nslab; s++) {
     const int z0 = s * planes, z1 = (z0 + planes < n3e) ? z0 + planes : n3e;
     const size_t off = (size_t)z0 * c->plane, bytes = (size_t)(z1 - z0) * c->plane * sizeof(double);
+    if (after_slab) CK(cudaStreamWaitEvent(c->copy_stream, after_slab[s], 0));
     if (harm_layout) {
       CK(cudaMemcpyAsync(c->d_Paos + NPR * off, h_P + NPR * off, NPR * bytes, cudaMemcpyHostToDevice, c->copy_stream));
     } else {
@@ -429,6 +439,62 @@ static int step_host(harm_ctx* c, int precision, int guess, double* h_P, double*
   if (int rc = check_status(c)) return rc;
   *dt = c->h_scal[0];
   add_stats(c, stats, 2.0 * (double)d.n1 * d.n2 * d.n3, guess);
+  return 0;
+}
+
+// D2H of the state d_Pdev into h_P in the slabs of h2d_slabs, on the D2H stream once the
+// context stream's work so far (the step) is done; an event after each slab
+static int d2h_slabs(harm_ctx* c, double* h_P) {
+  if (!c->d2h_stream) {
+    CK(cudaStreamCreateWithFlags(&c->d2h_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->done_ev, cudaEventDisableTiming));
+    for (int s = 0; s < HARM_H2D_SLABS; s++) CK(cudaEventCreateWithFlags(&c->d2h_ev[s], cudaEventDisableTiming));
+  }
+  const int n3e = c->g.n3e;
+  const int planes = (n3e + HARM_H2D_SLABS - 1) / HARM_H2D_SLABS;
+  const int nslab = (n3e + planes - 1) / planes;
+  CK(cudaEventRecord(c->done_ev, c->stream));
+  CK(cudaStreamWaitEvent(c->d2h_stream, c->done_ev, 0));
+  for (int s = 0; s < nslab; s++) {
+    const int z0 = s * planes, z1 = (z0 + planes < n3e) ? z0 + planes : n3e;
+    const size_t off = (size_t)z0 * c->plane, bytes = (size_t)(z1 - z0) * c->plane * sizeof(double);
+    for (int p = 0; p < NPR; p++)
+      CK(cudaMemcpyAsync(h_P + (size_t)p * c->cells + off, c->d_Pdev + (size_t)p * c->cells + off, bytes,
+                         cudaMemcpyDeviceToHost, c->d2h_stream));
+    CK(cudaEventRecord(c->d2h_ev[s], c->d2h_stream));
+  }
+  return 0;
+}
+
+// nsteps full steps over a host array, each step's state copied in from h_P and back out to
+// it.  Step n's copy out runs in k-slabs on the D2H stream; step n+1's copy in of a slab waits
+// only for the copy out of the same slab (the host values it reads), so the two PCIe
+// directions overlap, and step n+1's first flux tiles start on the slabs already back.
+extern "C" int harm_b200_step_host_n(harm_ctx* c, int precision, int guess, double* h_P, int nsteps, double* dt,
+                                     harm_stats* stats) {
+  if (!c || !h_P || !dt) return hb_setmsg("null argument", 1);
+  if (nsteps < 1) return hb_setmsg("nsteps must be at least 1", 2);
+  if (int rc = check_guess(c, guess)) return rc;
+  if (int rc = check_precision(precision)) return rc;
+  Dims d = dims_of(c->g);
+  const size_t bytes = NPR * c->cells * sizeof(double);
+  if (!c->d_Pdev) CK(cudaMalloc(&c->d_Pdev, bytes));
+  c->h_scal[0] = *dt;
+  CK(cudaMemcpyAsync(c->d_dt, c->h_scal, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (stats) CK(cudaMemsetAsync(c->d_stats, 0, 5 * sizeof(double), c->stream));
+  for (int n = 0; n < nsteps; n++) {
+    SlabWait sw;
+    if (int rc = h2d_slabs(c, h_P, &sw, false, n > 0 ? c->d2h_ev : nullptr)) return rc;
+    if (enqueue_step(c, precision, guess, c->d_Pdev, stats != nullptr, &sw)) return 1;
+    if (int rc = d2h_slabs(c, h_P)) return rc;
+  }
+  CK(cudaMemcpyAsync(c->h_scal, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (stats) CK(cudaMemcpyAsync(c->h_scal + 8, c->d_stats, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaStreamSynchronize(c->d2h_stream));
+  if (int rc = check_status(c)) return rc;
+  *dt = c->h_scal[0];
+  add_stats(c, stats, 2.0 * nsteps * (double)d.n1 * d.n2 * d.n3, guess);
   return 0;
 }
 

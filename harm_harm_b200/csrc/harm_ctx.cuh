@@ -28,6 +28,9 @@ struct harm_ctx {
   cudaStream_t copy_stream;             // host-buffer entry point: H2D of the state
   cudaEvent_t slab_ev[HARM_H2D_SLABS];  // recorded on copy_stream after each slab
   cudaEvent_t entry_ev;                 // recorded on stream before the copies start
+  cudaStream_t d2h_stream;              // multi-step host-buffer entry point: D2H of the state
+  cudaEvent_t d2h_ev[HARM_H2D_SLABS];   // recorded on d2h_stream after each slab
+  cudaEvent_t done_ev;                  // recorded on stream when a step's state is final
   size_t plane, cells;
   // metric tables (FP64, plus an FP32 copy for the mixed-precision flux path)
   double* d_geom;

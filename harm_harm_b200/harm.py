@@ -234,6 +234,16 @@ class Harm:
                     "step_ch_host")
         return d.value, st.as_dict()
 
+    def step_ch_host_n(self, P_host: np.ndarray, dt: float, precision: int = N.HARM_PREC_FP64,
+                       guess: int = N.HARM_GUESS_PREV, nsteps: int = 1):
+        """nsteps steps over a host array, each copying the state in and out, with the copies
+        of consecutive steps overlapped"""
+        d = C.c_double(dt)
+        st = N.harm_stats()
+        self._check(self._ordered(self.lib.harm_b200_step_host_n, self._ctx, precision, guess, _ptr(P_host), nsteps,
+                                  C.byref(d), C.byref(st)), "step_ch_host_n")
+        return d.value, st.as_dict()
+
     def step_ch_host_harm(self, P_harm: np.ndarray, dt: float, precision: int = N.HARM_PREC_FP64,
                           guess: int = N.HARM_GUESS_PREV):
         """one step over a host array in HARM's [k][j][i][pl] layout"""

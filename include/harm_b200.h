@@ -267,6 +267,15 @@ int harm_b200_step_n(harm_ctx *ctx, int precision, int guess, double *d_P, int n
 int harm_b200_step_host(harm_ctx *ctx, int precision, int guess, double *h_P, double *dt,
                         harm_stats *stats);
 
+/* nsteps such steps over the host array h_P (each step copies the state in from h_P and back
+   out to it, as nsteps calls of harm_b200_step_host would), pipelined across steps: a step's
+   copy out runs in k-slabs on a second copy stream and the next step's copy in of each slab
+   starts as soon as that slab is back on the host, so the two PCIe directions overlap and the
+   next step's first flux tiles start on the slabs already resident.  Results are those of
+   harm_b200_step_n; *dt in: first step, out: the next step. */
+int harm_b200_step_host_n(harm_ctx *ctx, int precision, int guess, double *h_P, int nsteps,
+                          double *dt, harm_stats *stats);
+
 /* ------------------------------------------------------------------------------------
  * HARM's own array layout.  HARM stores primitives, conserved variables and fluxes as
  * FTYPE [N3M][N2M][N1M][NPR] (ORDERSTORAGE 5, global.storage.h:320-340) and its flags as

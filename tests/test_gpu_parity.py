@@ -180,7 +180,8 @@ def test_fp64_fma_close_to_fp64(setup, cuda):
     faces: at most 1 % of the faces differ by more than 1e-12, the fluxes agree to 1e-4 in L1
     for WENO5 and 3e-2 for PARALINE (a flipped flattening of the planted jump moves its faces'
     fluxes by up to ~10 %), and the states after five steps to 1e-5 of each field's maximum
-    (measured up to 1.8e-6 for PARALINE)."""
+    (of the largest component of its vector for velocity and field; measured up to 1.8e-6
+    for PARALINE)."""
     g, geom, conn, aux, P, orc, dev = setup
     Pd = dev_array(cuda, P)
     Fa = [cuda.zeros_like(Pd) for _ in range(3)]
@@ -209,7 +210,10 @@ def test_fp64_fma_close_to_fp64(setup, cuda):
     b = Pb.cpu().numpy()[(slice(None),) + g.active]
     tol = 1e-5 if switching else 1e-10
     for pl in range(8):
-        e = np.abs(a[pl] - b[pl]).max() / max(np.abs(a[pl]).max(), 1e-300)
+        # a velocity or field component against its vector's largest component (B3 of the
+        # poloidal loop starts at zero, and its own maximum stays tiny in 2-D)
+        grp = slice(pl, pl + 1) if pl < 2 else slice(2, 5) if pl < 5 else slice(5, 8)
+        e = np.abs(a[pl] - b[pl]).max() / max(np.abs(a[grp]).max(), 1e-300)
         assert e < tol, (pl, e)
     assert abs(dta - dtb) <= tol * dta
     assert abs(stb["newton_iters"] - sta["newton_iters"]) <= 0.01 * sta["newton_iters"]

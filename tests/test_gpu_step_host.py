@@ -1,4 +1,5 @@
-"""harm_b200_step_host (the host-buffer entry point) against harm_b200_step on the same state.
+"""harm_b200_step_host and harm_b200_step_host_n (the host-buffer entry points) against
+harm_b200_step on the same state.
 The host entry point copies the state in slabs of k-planes and starts the first substep's
 flux tiles of each slab while later slabs are still in flight; the results must be those of
 the device-array step, bit for bit, including the x3 tile rows that wait for planes of later
@@ -34,6 +35,32 @@ def test_step_host_equals_device_step(cuda, shape, lim, precision, pinned):
     # a second step from the result: the copy stream and its events are reused
     dt_d2, _ = dev.step_ch(Pd, dt_d, precision=precision)
     dt_h2, _ = dev.step_ch_host(Ph, dt_h, precision=precision)
+    assert np.array_equal(Pd.cpu().numpy(), Ph) and dt_h2 == dt_d2
+    dev.close()
+
+
+@pytest.mark.parametrize("shape,lim", [((24, 16, 96), 2), ((64, 64, 1), 0)])
+@pytest.mark.parametrize("precision", [HARM_PREC_FP64, HARM_PREC_MIXED])
+@pytest.mark.parametrize("pinned", [True, False])
+def test_step_host_n_equals_device_steps(cuda, shape, lim, precision, pinned):
+    """harm_b200_step_host_n: four steps whose copies out and in overlap (the next step's
+    copy in of a slab waits only for the copy out of that slab) equal four device-array
+    steps bit for bit, dt and Newton counts included; a second call reuses the streams."""
+    g, geom, conn, aux, P = make_torus(*shape, lim=lim)
+    dev = Harm(g, geom, conn, aux)
+    Pd = cuda.from_numpy(P.copy()).cuda()
+    dev.bound_prim(Pd)
+    Ph = cuda.from_numpy(Pd.cpu().numpy())
+    if pinned:
+        Ph = Ph.pin_memory()
+    Ph = Ph.numpy()
+    dt_d, st_d = dev.step_ch(Pd, 1e-3, precision=precision, nsteps=4)
+    dt_h, st_h = dev.step_ch_host_n(Ph, 1e-3, precision=precision, nsteps=4)
+    assert np.array_equal(Pd.cpu().numpy(), Ph)
+    assert dt_h == dt_d
+    assert st_h["newton_iters"] == st_d["newton_iters"]
+    dt_d2, _ = dev.step_ch(Pd, dt_d, precision=precision, nsteps=3)
+    dt_h2, _ = dev.step_ch_host_n(Ph, dt_h, precision=precision, nsteps=3)
     assert np.array_equal(Pd.cpu().numpy(), Ph) and dt_h2 == dt_d2
     dev.close()
 
