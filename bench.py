@@ -65,18 +65,23 @@ def update_kernel_bytes_per_cell(n3: int, precision: int) -> float:
     return 64 + 64 + 15 * w + 3 * w + 64 + 1 + 94 * 8 / n3
 
 
-def flux_bytes_per_cell(n3: int, precision: int) -> float:
-    """Algorithmic bytes of the three flux kernels per active cell: each direction reads the
-    8 FP64 primitives once (64 B) and writes 8 fluxes (FP32 in the mixed path: 32 B, FP64:
-    64 B), plus the face metric record (28 values per (i,j), reused along phi)."""
+def flux_bytes_per_cell(n3: int, precision: int, lim: str = "weno5") -> float:
+    """Algorithmic bytes of the flux stage per active cell: each direction reads the 8 FP64
+    primitives once (64 B) and writes 8 fluxes (FP32 in the mixed path: 32 B, FP64: 64 B),
+    plus the face metric record (28 values per (i,j), reused along phi).  WENO5 adds the cell
+    pass: it reads the primitives once (64 B) and writes the 9 dP line quantities, of which
+    each direction reads back its 3."""
     w = 4 if precision == 1 else 8
-    return 3 * (64 + 8 * w + 28 * w / n3)
+    b = 3 * (64 + 8 * w + 28 * w / n3)
+    if lim == "weno5":
+        b += 64 + 9 * w + 3 * 3 * w
+    return b
 
 
-# DRAM traffic of the flux stage (three k_fluxt launches; ncu dram__bytes_read.sum +
+# DRAM traffic of the flux stage (k_cellprep and three k_fluxt launches; ncu dram__bytes_read.sum +
 # dram__bytes_write.sum) per active cell, measured on the 192x96x64 torus and scaled to a
 # workload by its cell count
-FLUX_TRAFFIC_PER_CELL = {("weno5", "mixed"): 293.6}
+FLUX_TRAFFIC_PER_CELL = {("weno5", "mixed"): 450.8}
 
 
 def clock_sampler(stop: threading.Event, out: list, dev: int):
@@ -476,7 +481,7 @@ def run_ours(args, ws, rank, local):
     # stage times and roofline of the dominant kernels
     stages = dev.time_stages(Pm, dt0, precision=prec, guess=guess, reps=3)
     peaks = measured_peaks()
-    flux_bytes = flux_bytes_per_cell(n3, prec) * zones
+    flux_bytes = flux_bytes_per_cell(n3, prec, LIMNAME[lim]) * zones
     ach_flux = flux_bytes / (stages["flux"] * 1e-3) / 1e9
     upd_bytes = update_kernel_bytes_per_cell(n3, prec) * zones
     ach = upd_bytes / (stages["update_invert"] * 1e-3) / 1e9
@@ -544,10 +549,11 @@ def run_ours(args, ws, rank, local):
                          "frac": ach_flux / peaks["hbm_gbs"], "peak_src": peaks["src"],
                          "traffic": (FLUX_TRAFFIC_PER_CELL[(LIMNAME[lim], args.precision)] * zones
                                      if (LIMNAME[lim], args.precision) in FLUX_TRAFFIC_PER_CELL else None),
-                         "unit_of_launch": "one flux stage (three k_fluxt launches, all directions)",
-                         "algorithmic_bytes_per_cell": flux_bytes_per_cell(n3, prec),
-                         "limiter": "instruction issue, not HBM: 76 % of issue slots, FMA 56 %, ALU 50 % "
-                                    "(ncu, WENO5 FP32 tile kernel, 192x96x64)"},
+                         "unit_of_launch": "one flux stage (the WENO5 cell pass k_cellprep and three k_fluxt "
+                                           "launches, all directions)",
+                         "algorithmic_bytes_per_cell": flux_bytes_per_cell(n3, prec, LIMNAME[lim]),
+                         "limiter": "instruction issue, not HBM: 75 % of issue slots, ALU 56 %, FMA 52 %, "
+                                    "DRAM 6 % (ncu, WENO5 FP32 tile kernel, 192x96x64)"},
             "roofline_update_invert": {"bound": "hbm",
                                        "kernel": "conserved update + learned start + k_invert + k_invert_rare",
                                        "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
