@@ -285,15 +285,18 @@ def cpu_baseline_sample(args, lim) -> dict:
 
 def train_guess(dev, Pd, dt0, prec, args):
     """The plain method runs `train_steps` steps from the initial state; after each, its
-    (U, P) pairs are dumped (every `stride`-th cell); the network is trained on them."""
+    (U, P) pairs are dumped (every `stride`-th cell); `synth_pairs` synthetic states on the
+    grid's metric are added (harm_b200_mlp_synth: rho, u/rho, sigma log-uniform, Lorentz factor
+    uniform to 50, isotropic directions); the network is trained on both."""
     import torch
     from harm_harm_b200 import HARM_GUESS_PREV
     g = dev.grid.g
     ncell = g.n1 * g.n2 * g.n3
     stride = max(1, (ncell * args.train_steps) // args.train_pairs)
     cap = ncell // stride + 1
-    feat = torch.zeros((cap * args.train_steps, 10), device="cuda", dtype=torch.float32)
-    targ = torch.zeros((cap * args.train_steps, 2), device="cuda", dtype=torch.float32)
+    nsyn = max(0, args.synth_pairs)
+    feat = torch.zeros((cap * args.train_steps + nsyn, 10), device="cuda", dtype=torch.float32)
+    targ = torch.zeros((cap * args.train_steps + nsyn, 2), device="cuda", dtype=torch.float32)
     P = Pd.clone()
     dt, n = dt0, 0
     t0 = time.perf_counter()
@@ -301,6 +304,10 @@ def train_guess(dev, Pd, dt0, prec, args):
         dt, _ = dev.step_ch(P, dt, precision=prec, guess=HARM_GUESS_PREV, stats=False)
         n += dev.mlp_dump(P, feat[n:n + cap], targ[n:n + cap], stride=stride, phase=s % stride)
     del P
+    ndump = n
+    if nsyn:
+        dev.mlp_synth(feat[n:n + nsyn], targ[n:n + nsyn], seed=args.seed)
+        n += nsyn
     feat, targ = feat[:n].contiguous(), targ[:n].contiguous()
     norm = torch.zeros(24, device="cuda", dtype=torch.float32)
     params = torch.zeros(9154, device="cuda", dtype=torch.float32)
@@ -311,7 +318,7 @@ def train_guess(dev, Pd, dt0, prec, args):
     torch.cuda.synchronize()
     t2 = time.perf_counter()
     dev.mlp_set(params, norm, args.start_bias)
-    return {"pairs": n, "dump_steps": args.train_steps, "dump_stride": stride, "adam_steps": args.train_iters,
+    return {"pairs": n, "dumped_pairs": ndump, "synthetic_pairs": nsyn, "dump_steps": args.train_steps, "dump_stride": stride, "adam_steps": args.train_iters,
             "batch": 8192, "dump_s": round(t1 - t0, 3), "train_s": round(t2 - t1, 3),
             "loss_first": float(hist[0]), "loss_last100": float(hist[-100:].mean()), "start_bias": args.start_bias}
 
@@ -589,6 +596,7 @@ def main():
     ap.add_argument("--train-steps", type=int, default=4, help="plain steps whose (U,P) pairs train the guess")
     ap.add_argument("--train-pairs", type=int, default=2000000, help="pairs dumped over those steps")
     ap.add_argument("--train-iters", type=int, default=15000, help="Adam steps of the training")
+    ap.add_argument("--synth-pairs", type=int, default=2000000, help="synthetic (U,P) pairs added to the training set")
     ap.add_argument("--start-bias", type=float, default=0.0, help="added to the predicted log(W'/D)")
     ap.add_argument("--seed", type=int, default=12345)
     ap.add_argument("--err-steps", type=int, default=100, help="steps of the mixed-vs-FP64 error measurement")
