@@ -224,14 +224,19 @@ struct ReconGeom<HARM_LIM_PARALINE> {
 
 template <int LIM, typename T>
 struct FluxTile {
-  static constexpr int A = 32;                                 // faces along DIR
+  static constexpr int A = 32;                                 // threads (faces) along DIR
   static constexpr int NT = 8;                                 // transverse lines
   static constexpr int H = ReconGeom<LIM>::H;
-  static constexpr int NL = A + H + ReconGeom<LIM>::X;         // staged cells along DIR
   static constexpr int VB = (sizeof(T) == 4) ? 8 : 4;          // primitives per stage
+  // faces a tile can hold along DIR: the FP32 tiles (all primitives staged at once) hold one
+  // more than their threads, so that the last tile of a sweep of n*A + 1 faces (a grid of n*A
+  // cells) takes the last face itself instead of a tile row of one face; the tile's threads
+  // tid < NT compute that face, one per line
+  static constexpr int AF = (VB == NPR) ? A + 1 : A;
+  static constexpr int NL = AF + H + ReconGeom<LIM>::X;        // staged cells along DIR
   static constexpr int NW = (LIM == HARM_LIM_WENO5) ? 4 : 0;   // WENO5: 3 weights + SMONO per cell
   static constexpr int PLANE = NL * NT;               // staged values of one primitive
-  static constexpr int PE = (A + 1) * NT;              // edge values: cells H-1 .. H+A-1
+  static constexpr int PE = (AF + 1) * NT;             // edge values: cells H-1 .. H+AF-1
   static constexpr int PW = (NL - 4) * NT;             // WENO5 weights: cells 2 .. NL-3
   static constexpr int NF = (LIM == HARM_LIM_PARALINE) ? 1 : 0;  // PARALINE: V, P, Fi planes
   static constexpr int ND = (LIM == HARM_LIM_WENO5) ? 1 : 0;     // WENO5: dP of the edge cells
@@ -458,7 +463,7 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
                                                unsigned long long* __restrict__ dtslot,
                                                const T* __restrict__ L = nullptr) {
   using TL = FluxTile<LIM, T>;
-  constexpr int A = TL::A, NT = TL::NT, H = TL::H, NL = TL::NL, VB = TL::VB, PL = TL::PLANE, PE = TL::PE, PW = TL::PW;
+  constexpr int A = TL::A, AF = TL::AF, NT = TL::NT, H = TL::H, NL = TL::NL, VB = TL::VB, PL = TL::PLANE, PE = TL::PE, PW = TL::PW;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   T* s_y = reinterpret_cast<T*>(smem_raw);   // [VB][plane]
   T* s_el = s_y + VB * PL;                    // left edge of each cell, [VB][PE]
@@ -470,8 +475,8 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
   T* s_dP = s_w + VB * PW * TL::NW + TL::NF * (2 * PL + PE);  // WENO5: dP of the edge cells, [PE]
   // a plane is [NT][NL] for DIR 1 and [NL][NT] otherwise: the index along i is contiguous
   auto sx = [](int c, int t) -> int { return (DIR == 1) ? t * NL + c : c * NT + t; };
-  // edge planes hold cells H-1 .. H+A-1, weight planes cells 2 .. NL-3, in the same layout
-  auto ex = [](int c, int t) -> int { return (DIR == 1) ? t * (A + 1) + c - (H - 1) : (c - (H - 1)) * NT + t; };
+  // edge planes hold cells H-1 .. H+AF-1, weight planes cells 2 .. NL-3, in the same layout
+  auto ex = [](int c, int t) -> int { return (DIR == 1) ? t * (AF + 1) + c - (H - 1) : (c - (H - 1)) * NT + t; };
   auto wx = [](int c, int t) -> int { return (DIR == 1) ? t * (NL - 4) + c - 2 : (c - 2) * NT + t; };
   // item idx over VB x nc cells (from c0) x NT lines, fastest along i
   auto split = [](int idx, int c0, int nc, int& v, int& c, int& t) {
@@ -537,9 +542,9 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
       s_P[sx(cl, ct)] = pt;
     }
     __syncthreads();
-    for (int idx = tid; idx < (A + 1) * NT; idx += 256) {
+    for (int idx = tid; idx < (AF + 1) * NT; idx += 256) {
       int v, c, t;
-      split(idx, H - 1, A + 1, v, c, t);
+      split(idx, H - 1, AF + 1, v, c, t);
       T vv[7], pp[7];
 #pragma unroll
       for (int q = 0; q < 7; q++) {
@@ -554,7 +559,7 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
   // primitives and the cell-centre metric, into the edge planes, then dP of each edge cell.
   // From L where the cell pass computed them; otherwise here: with all primitives staged at
   // once (FP32) from the staged tile below, else (FP64, two groups) loaded here.
-  constexpr int DPC = A + 3;  // cells with line quantities per line
+  constexpr int DPC = AF + 3;  // cells with line quantities per line
   auto weno_line = [&](int cl, int ct, const T* pc) {
     const int lext = min(max(l0 - H + cl + ngL, 0), nLe - 1);
     const int text = min(max(t0 + ct + d.ng, 0), nTe - 1);
@@ -580,7 +585,7 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
         s_el[3 * PL + si] = __ldg(Lq + 2 * d.cells + cid);
       }
       __syncthreads();
-      weno_dp_edges<A, NT, H, PL, T>(s_el, s_dP, tid, sx, ex, split);
+      weno_dp_edges<AF, NT, H, PL, T>(s_el, s_dP, tid, sx, ex, split);
     } else if constexpr (VB < NPR) {
       for (int idx = tid; idx < DPC * NT; idx += 256) {
         int v, cl, ct;
@@ -594,7 +599,7 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
         weno_line(cl, ct, pc);
       }
       __syncthreads();
-      weno_dp_edges<A, NT, H, PL, T>(s_el, s_dP, tid, sx, ex, split);
+      weno_dp_edges<AF, NT, H, PL, T>(s_el, s_dP, tid, sx, ex, split);
     }
   }
   T pl[NPR], pr[NPR];
@@ -625,14 +630,14 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
             weno_line(cl, ct, pc);
           }
           __syncthreads();
-          weno_dp_edges<A, NT, H, PL, T>(s_el, s_dP, tid, sx, ex, split);
+          weno_dp_edges<AF, NT, H, PL, T>(s_el, s_dP, tid, sx, ex, split);
         }
       }
-      weno_tile_edges<VB, A, NT, H, NL, PL, PE, PW, T>(s_y, s_w, s_el, s_er, s_dP, tid, sx, ex, wx, split);
+      weno_tile_edges<VB, AF, NT, H, NL, PL, PE, PW, T>(s_y, s_w, s_el, s_er, s_dP, tid, sx, ex, wx, split);
     } else if (LIM == HARM_LIM_PARA) {
-      for (int idx = tid; idx < VB * (A + 1) * NT; idx += 256) {
+      for (int idx = tid; idx < VB * (AF + 1) * NT; idx += 256) {
         int v, c, t;
-        split(idx, H - 1, A + 1, v, c, t);
+        split(idx, H - 1, AF + 1, v, c, t);
         const T* y = s_y + v * PL;
         T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
         T yl, yr;
@@ -641,9 +646,9 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
         s_er[v * PE + ex(c, t)] = yr;
       }
     } else if (LIM == HARM_LIM_PARALINE) {
-      for (int idx = tid; idx < VB * (A + 1) * NT; idx += 256) {
+      for (int idx = tid; idx < VB * (AF + 1) * NT; idx += 256) {
         int v, c, t;
-        split(idx, H - 1, A + 1, v, c, t);
+        split(idx, H - 1, AF + 1, v, c, t);
         const T* y = s_y + v * PL;
         T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
         T yl, yr;
@@ -652,9 +657,9 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
         s_er[v * PE + ex(c, t)] = yr;
       }
     } else {
-      for (int idx = tid; idx < VB * (A + 1) * NT; idx += 256) {
+      for (int idx = tid; idx < VB * (AF + 1) * NT; idx += 256) {
         int v, c, t;
-        split(idx, H - 1, A + 1, v, c, t);
+        split(idx, H - 1, AF + 1, v, c, t);
         const T* y = s_y + v * PL;
         const T y0 = y[sx(c, t)];
         T dq = mc_slope(y[sx(c - 1, t)], y0, y[sx(c + 1, t)]);
@@ -679,6 +684,24 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
     else { ii = text; jj = o + d.ng; }
     dtij = face_hll<DIR, T, GT>(d, ph, geom, F, id, ii, jj, pl, pr);
   }
+  if constexpr (AF > A) {
+    // the tile's face A (the sweep's last face), on line tid, by the threads tid < NT; the
+    // edge planes still hold every primitive (one staging group)
+    if (tid < NT && l0 + A == lhi && t0 + tid <= thi) {
+#pragma unroll
+      for (int v = 0; v < NPR; v++) {
+        pl[v] = s_er[v * PE + ex(H + A - 1, tid)];
+        pr[v] = s_el[v * PE + ex(H + A, tid)];
+      }
+      const int lext = l0 + A + ngL, text = t0 + tid + d.ng;
+      const size_t id = cell_index(lext, text);
+      int ii, jj;
+      if (DIR == 1) { ii = lext; jj = text; }
+      else if (DIR == 2) { ii = text; jj = lext; }
+      else { ii = text; jj = o + d.ng; }
+      dtij = fmin(dtij, face_hll<DIR, T, GT>(d, ph, geom, F, id, ii, jj, pl, pr));
+    }
+  }
   // block minimum and one atomic per block
   __shared__ double red[8];
 #pragma unroll
@@ -693,12 +716,21 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
   }
 }
 
-template <int DIR, int LIM>
+// tiles along a sweep of n faces: ceil(n / A), or with room for one more face in the last
+// tile (FluxTile::AF), ceil((n - 1) / A), whose last tile holds 2 .. A+1 faces
+template <int LIM, typename T>
+static inline int fluxt_tiles(int n) {
+  constexpr int A = FluxTile<LIM, T>::A;
+  if (FluxTile<LIM, T>::AF > A) return n >= 2 ? (n - 1 + A - 1) / A : 1;
+  return (n + A - 1) / A;
+}
+
+template <int DIR, int LIM, typename T>
 static inline dim3 fluxt_grid(const FaceBox& fb) {
-  constexpr int A = 32, NT = 8;
-  if (DIR == 1) return dim3((fb.cnt[0] + A - 1) / A, (fb.cnt[1] + NT - 1) / NT, fb.cnt[2]);
-  if (DIR == 2) return dim3((fb.cnt[0] + NT - 1) / NT, (fb.cnt[1] + A - 1) / A, fb.cnt[2]);
-  return dim3((fb.cnt[0] + NT - 1) / NT, (fb.cnt[2] + A - 1) / A, fb.cnt[1]);
+  constexpr int NT = FluxTile<LIM, T>::NT;
+  if (DIR == 1) return dim3(fluxt_tiles<LIM, T>(fb.cnt[0]), (fb.cnt[1] + NT - 1) / NT, fb.cnt[2]);
+  if (DIR == 2) return dim3((fb.cnt[0] + NT - 1) / NT, fluxt_tiles<LIM, T>(fb.cnt[1]), fb.cnt[2]);
+  return dim3((fb.cnt[0] + NT - 1) / NT, fluxt_tiles<LIM, T>(fb.cnt[2]), fb.cnt[1]);
 }
 
 // the face box restricted to active-relative k indices [klo, khi] (index 2: k for every
@@ -766,7 +798,7 @@ static inline cudaError_t launch_fluxt(const Dims& d, const Phys& ph, const Face
     cudaError_t e = raise_smem_limit_once(raised, (const void*)k_fluxt<DIR, LIM, T, GT>, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  k_fluxt<DIR, LIM, T, GT><<<fluxt_grid<DIR, LIM>(fb), 256, smem, st>>>(d, ph, fb, P, geom, F, dtslot, L);
+  k_fluxt<DIR, LIM, T, GT><<<fluxt_grid<DIR, LIM, T>(fb), 256, smem, st>>>(d, ph, fb, P, geom, F, dtslot, L);
   return cudaGetLastError();
 }
 
@@ -804,16 +836,20 @@ static inline cudaError_t launch_flux_slabs(const Dims& d, const Phys& ph, const
       if ((e = launch_fluxt<2, LIM, T, GT>(d, ph, sb, pb, geom, F2, slots + 1, st, L)) != cudaSuccess) return e;
       launches++;
     }
-    // x3 tile rows: a row from face f0 stages planes up to f0 + ng3 + A + X - 1 (clamped)
+    // x3 tile rows: a row of faces f0 .. last stages planes up to last + ng3 + X (clamped);
+    // a row of tiles with room for one more face takes the sweep's last face when it is the
+    // only one left after it
     while (d.n3 > 1 && f3 <= b3.hi[2]) {
-      int top = f3 + d.ng3 + A + X - 1;
+      int last = f3 + A - 1;
+      if (FluxTile<LIM, T>::AF > A && b3.hi[2] - last == 1) last = b3.hi[2];
+      int top = last + d.ng3 + X;
       if (top > d.n3e - 1) top = d.n3e - 1;
       if (top >= resident && s + 1 < sw.nslab) break;
-      if (face_box_k(b3, f3, f3 + A - 1, &sb)) {
+      if (face_box_k(b3, f3, last, &sb)) {
         if ((e = launch_fluxt<3, LIM, T, GT>(d, ph, sb, pb, geom, F3, slots + 2, st, L)) != cudaSuccess) return e;
         launches++;
       }
-      f3 += A;
+      f3 = last + 1;
     }
   }
   return cudaSuccess;

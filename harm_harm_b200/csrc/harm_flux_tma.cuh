@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(256, TmaOcc<LIM>::blocks) k_fluxt_tma(Dims d, 
   using T = float;
   using TL = FluxTile<LIM, T>;
   using TB = TmaBox<DIR, LIM>;
-  constexpr int A = TL::A, NT = TL::NT, H = TL::H, NL = TL::NL, PL = TL::PLANE, PE = TL::PE, PW = TL::PW;
+  constexpr int A = TL::A, AF = TL::AF, NT = TL::NT, H = TL::H, NL = TL::NL, PL = TL::PLANE, PE = TL::PE, PW = TL::PW;
   static_assert(TL::VB == NPR, "the FP32 tile holds all primitives at once");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double* raw = reinterpret_cast<double*>(smem_raw);
@@ -83,8 +83,9 @@ __global__ void __launch_bounds__(256, TmaOcc<LIM>::blocks) k_fluxt_tma(Dims d, 
   __shared__ int s_ok;
   __shared__ double red[8];
   auto sx = [](int c, int t) -> int { return (DIR == 1) ? t * NL + c : c * NT + t; };
-  // edge planes hold cells H-1 .. H+A-1, weight planes cells 2 .. NL-3, in the same layout
-  auto ex = [](int c, int t) -> int { return (DIR == 1) ? t * (A + 1) + c - (H - 1) : (c - (H - 1)) * NT + t; };
+  // edge planes hold cells H-1 .. H+AF-1, weight planes cells 2 .. NL-3, in the same layout
+  // (this kernel's tiles hold A faces; the edge planes have room for the AF of k_fluxt's)
+  auto ex = [](int c, int t) -> int { return (DIR == 1) ? t * (AF + 1) + c - (H - 1) : (c - (H - 1)) * NT + t; };
   auto wx = [](int c, int t) -> int { return (DIR == 1) ? t * (NL - 4) + c - 2 : (c - 2) * NT + t; };
   auto split = [](int idx, int c0, int nc, int& v, int& c, int& t) {
     if (DIR == 1) {
@@ -183,12 +184,12 @@ __global__ void __launch_bounds__(256, TmaOcc<LIM>::blocks) k_fluxt_tma(Dims d, 
         weno_line_cell<DIR, PL, T>(s_el, sx(cl, ct), pc, g, (T)ph.gam);
       }
       __syncthreads();
-      weno_dp_edges<A, NT, H, PL, T>(s_el, s_dP, tid, sx, ex, split);
-      weno_tile_edges<NPR, A, NT, H, NL, PL, PE, PW, T>(s_y, s_w, s_el, s_er, s_dP, tid, sx, ex, wx, split);
+      weno_dp_edges<AF, NT, H, PL, T>(s_el, s_dP, tid, sx, ex, split);
+      weno_tile_edges<NPR, AF, NT, H, NL, PL, PE, PW, T>(s_y, s_w, s_el, s_er, s_dP, tid, sx, ex, wx, split);
     } else if (LIM == HARM_LIM_PARA) {
-      for (int idx = tid; idx < NPR * (A + 1) * NT; idx += 256) {
+      for (int idx = tid; idx < NPR * (AF + 1) * NT; idx += 256) {
         int v, c, t;
-        split(idx, H - 1, A + 1, v, c, t);
+        split(idx, H - 1, AF + 1, v, c, t);
         const T* y = s_y + v * PL;
         T u5[5] = {y[sx(c - 2, t)], y[sx(c - 1, t)], y[sx(c, t)], y[sx(c + 1, t)], y[sx(c + 2, t)]};
         T yl, yr;
@@ -197,9 +198,9 @@ __global__ void __launch_bounds__(256, TmaOcc<LIM>::blocks) k_fluxt_tma(Dims d, 
         s_er[v * PE + ex(c, t)] = yr;
       }
     } else {
-      for (int idx = tid; idx < NPR * (A + 1) * NT; idx += 256) {
+      for (int idx = tid; idx < NPR * (AF + 1) * NT; idx += 256) {
         int v, c, t;
-        split(idx, H - 1, A + 1, v, c, t);
+        split(idx, H - 1, AF + 1, v, c, t);
         const T* y = s_y + v * PL;
         const T y0 = y[sx(c, t)];
         T dq = mc_slope(y[sx(c - 1, t)], y0, y[sx(c + 1, t)]);
