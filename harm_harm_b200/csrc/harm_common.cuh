@@ -455,6 +455,14 @@ __device__ __forceinline__ double face_hll(const Dims& d, const Phys& ph, const 
 #else
 #define HARM_FLUXT_LB __launch_bounds__(256)
 #endif
+// DIR 2 and 3 tiles: how far their first line (i) is moved below the face box so that the
+// extended index of every tile's first line is a multiple of NT
+template <int NT>
+__host__ __device__ __forceinline__ int fluxt_tshift(const FaceBox& fb, int ng) {
+  static_assert((NT & (NT - 1)) == 0, "NT is a power of two");
+  return (fb.lo[0] + ng) & (NT - 1);
+}
+
 // L (WENO5, optional): the dP line quantities of every extended cell from k_cellprep,
 // [3 (DIR-1) + q][cells] for q = par, veff, upar; where null, the kernel computes them.
 template <int DIR, int LIM, typename T, typename GT, int TU = HARM_TU>
@@ -493,21 +501,25 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
     }
   };
   const int tid = threadIdx.x;
-  // tile origin in active-relative face coordinates, and this thread's face
+  // tile origin in active-relative face coordinates, and this thread's face.  For DIR 2 and 3
+  // the NT lines are consecutive i: their origin is moved down to an extended i that is a
+  // multiple of NT (fluxt_tshift), so that each staged row of NT values starts on a 32-byte
+  // sector (FP32 rows: one sector, FP64 rows: two); the lanes below the face box do no face.
   int l0, t0, o, lme, tme;
   if (DIR == 1) {
     l0 = blockIdx.x * A + fb.lo[0]; t0 = blockIdx.y * NT + fb.lo[1]; o = blockIdx.z + fb.lo[2];
     lme = tid % A; tme = tid / A;
   } else if (DIR == 2) {
-    t0 = blockIdx.x * NT + fb.lo[0]; l0 = blockIdx.y * A + fb.lo[1]; o = blockIdx.z + fb.lo[2];
+    t0 = blockIdx.x * NT + fb.lo[0] - fluxt_tshift<NT>(fb, d.ng); l0 = blockIdx.y * A + fb.lo[1]; o = blockIdx.z + fb.lo[2];
     lme = tid / NT; tme = tid % NT;
   } else {
-    t0 = blockIdx.x * NT + fb.lo[0]; l0 = blockIdx.y * A + fb.lo[2]; o = blockIdx.z + fb.lo[1];
+    t0 = blockIdx.x * NT + fb.lo[0] - fluxt_tshift<NT>(fb, d.ng); l0 = blockIdx.y * A + fb.lo[2]; o = blockIdx.z + fb.lo[1];
     lme = tid / NT; tme = tid % NT;
   }
   const int lhi = fb.hi[DIR - 1];
   const int thi = (DIR == 1) ? fb.hi[1] : fb.hi[0];
-  const bool valid = (l0 + lme <= lhi) && (t0 + tme <= thi);
+  const int tlo = (DIR == 1) ? fb.lo[1] : fb.lo[0];
+  const bool valid = (l0 + lme <= lhi) && (t0 + tme <= thi) && (t0 + tme >= tlo);
   // extended-grid extents along DIR and along the transverse tile axis
   const int ngL = (DIR == 3) ? d.ng3 : d.ng;
   const int nLe = (DIR == 1) ? d.n1e : (DIR == 2) ? d.n2e : d.n3e;
@@ -687,7 +699,7 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
   if constexpr (AF > A) {
     // the tile's face A (the sweep's last face), on line tid, by the threads tid < NT; the
     // edge planes still hold every primitive (one staging group)
-    if (tid < NT && l0 + A == lhi && t0 + tid <= thi) {
+    if (tid < NT && l0 + A == lhi && t0 + tid <= thi && t0 + tid >= tlo) {
 #pragma unroll
       for (int v = 0; v < NPR; v++) {
         pl[v] = s_er[v * PE + ex(H + A - 1, tid)];
@@ -726,11 +738,12 @@ static inline int fluxt_tiles(int n) {
 }
 
 template <int DIR, int LIM, typename T>
-static inline dim3 fluxt_grid(const FaceBox& fb) {
+static inline dim3 fluxt_grid(const FaceBox& fb, int ng) {
   constexpr int NT = FluxTile<LIM, T>::NT;
   if (DIR == 1) return dim3(fluxt_tiles<LIM, T>(fb.cnt[0]), (fb.cnt[1] + NT - 1) / NT, fb.cnt[2]);
-  if (DIR == 2) return dim3((fb.cnt[0] + NT - 1) / NT, fluxt_tiles<LIM, T>(fb.cnt[1]), fb.cnt[2]);
-  return dim3((fb.cnt[0] + NT - 1) / NT, fluxt_tiles<LIM, T>(fb.cnt[2]), fb.cnt[1]);
+  const int nx = (fb.cnt[0] + fluxt_tshift<NT>(fb, ng) + NT - 1) / NT;
+  if (DIR == 2) return dim3(nx, fluxt_tiles<LIM, T>(fb.cnt[1]), fb.cnt[2]);
+  return dim3(nx, fluxt_tiles<LIM, T>(fb.cnt[2]), fb.cnt[1]);
 }
 
 // the face box restricted to active-relative k indices [klo, khi] (index 2: k for every
@@ -798,7 +811,7 @@ static inline cudaError_t launch_fluxt(const Dims& d, const Phys& ph, const Face
     cudaError_t e = raise_smem_limit_once(raised, (const void*)k_fluxt<DIR, LIM, T, GT>, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  k_fluxt<DIR, LIM, T, GT><<<fluxt_grid<DIR, LIM, T>(fb), 256, smem, st>>>(d, ph, fb, P, geom, F, dtslot, L);
+  k_fluxt<DIR, LIM, T, GT><<<fluxt_grid<DIR, LIM, T>(fb, d.ng), 256, smem, st>>>(d, ph, fb, P, geom, F, dtslot, L);
   return cudaGetLastError();
 }
 
