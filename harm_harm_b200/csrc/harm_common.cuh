@@ -228,11 +228,10 @@ struct FluxTile {
   static constexpr int NT = 8;                                 // transverse lines
   static constexpr int H = ReconGeom<LIM>::H;
   static constexpr int VB = (sizeof(T) == 4) ? 8 : 4;          // primitives per stage
-  // faces a tile can hold along DIR: the FP32 tiles (all primitives staged at once) hold one
-  // more than their threads, so that the last tile of a sweep of n*A + 1 faces (a grid of n*A
-  // cells) takes the last face itself instead of a tile row of one face; the tile's threads
-  // tid < NT compute that face, one per line
-  static constexpr int AF = (VB == NPR) ? A + 1 : A;
+  // faces a tile can hold along DIR: one more than its threads, so that the last tile of a
+  // sweep of n*A + 1 faces (a grid of n*A cells) takes the last face itself instead of a tile
+  // row of one face; the tile's threads tid < NT compute that face, one per line
+  static constexpr int AF = A + 1;
   static constexpr int NL = AF + H + ReconGeom<LIM>::X;        // staged cells along DIR
   static constexpr int NW = (LIM == HARM_LIM_WENO5) ? 4 : 0;   // WENO5: 3 weights + SMONO per cell
   static constexpr int PLANE = NL * NT;               // staged values of one primitive
@@ -448,8 +447,9 @@ __device__ __forceinline__ double face_hll(const Dims& d, const Phys& ph, const 
 }
 
 // HARM_FLUXT_MINB: resident blocks per SM the tiled flux kernel is compiled for (the mixed
-// path's FP32 tiles: 3, at most 85 registers with every staging load in flight); unset, the
-// compiler's choice (the FP64 tiles need ~160 registers)
+// path's FP32 tiles: 3, at most 85 registers with every staging load in flight; the FP64
+// tiles: 2, 128 registers with spills, faster than the ~160 registers and 1 block per SM the
+// compiler picks on its own); unset, the compiler's choice
 #ifdef HARM_FLUXT_MINB
 #define HARM_FLUXT_LB __launch_bounds__(256, HARM_FLUXT_MINB)
 #else
@@ -615,6 +615,7 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
     }
   }
   T pl[NPR], pr[NPR];
+  __shared__ T s_xl[NPR * NT], s_xr[NPR * NT];  // edge values of the tile's face A
 #pragma unroll
   for (int p0 = 0; p0 < NPR; p0 += VB) {
     if (p0 > 0) __syncthreads();
@@ -685,6 +686,13 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
       pl[p0 + v] = s_er[v * PE + ex(H + lme - 1, tme)];
       pr[p0 + v] = s_el[v * PE + ex(H + lme, tme)];
     }
+    if (tid < NT) {  // the edge values of face A of line tid, read back by the same thread below
+#pragma unroll
+      for (int v = 0; v < VB; v++) {
+        s_xl[(p0 + v) * NT + tid] = s_er[v * PE + ex(H + A - 1, tid)];
+        s_xr[(p0 + v) * NT + tid] = s_el[v * PE + ex(H + A, tid)];
+      }
+    }
   }
   double dtij = 1.e300;
   if (valid) {
@@ -696,14 +704,14 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
     else { ii = text; jj = o + d.ng; }
     dtij = face_hll<DIR, T, GT>(d, ph, geom, F, id, ii, jj, pl, pr);
   }
-  if constexpr (AF > A) {
-    // the tile's face A (the sweep's last face), on line tid, by the threads tid < NT; the
-    // edge planes still hold every primitive (one staging group)
+  {
+    // the tile's face A (the sweep's last face), on line tid, by the threads tid < NT, from
+    // the edge values each of them kept from every staging group
     if (tid < NT && l0 + A == lhi && t0 + tid <= thi && t0 + tid >= tlo) {
 #pragma unroll
       for (int v = 0; v < NPR; v++) {
-        pl[v] = s_er[v * PE + ex(H + A - 1, tid)];
-        pr[v] = s_el[v * PE + ex(H + A, tid)];
+        pl[v] = s_xl[v * NT + tid];
+        pr[v] = s_xr[v * NT + tid];
       }
       const int lext = l0 + A + ngL, text = t0 + tid + d.ng;
       const size_t id = cell_index(lext, text);
@@ -728,13 +736,13 @@ __global__ void HARM_FLUXT_LB k_fluxt(Dims d, Phys ph, FaceBox fb, const double*
   }
 }
 
-// tiles along a sweep of n faces: ceil(n / A), or with room for one more face in the last
-// tile (FluxTile::AF), ceil((n - 1) / A), whose last tile holds 2 .. A+1 faces
+// tiles along a sweep of n faces, with room for one more face in the last tile
+// (FluxTile::AF): ceil((n - 1) / A), whose last tile holds 2 .. A+1 faces
 template <int LIM, typename T>
 static inline int fluxt_tiles(int n) {
   constexpr int A = FluxTile<LIM, T>::A;
-  if (FluxTile<LIM, T>::AF > A) return n >= 2 ? (n - 1 + A - 1) / A : 1;
-  return (n + A - 1) / A;
+  static_assert(FluxTile<LIM, T>::AF == A + 1, "the last tile holds up to A+1 faces");
+  return n >= 2 ? (n - 1 + A - 1) / A : 1;
 }
 
 template <int DIR, int LIM, typename T>
@@ -854,7 +862,7 @@ static inline cudaError_t launch_flux_slabs(const Dims& d, const Phys& ph, const
     // only one left after it
     while (d.n3 > 1 && f3 <= b3.hi[2]) {
       int last = f3 + A - 1;
-      if (FluxTile<LIM, T>::AF > A && b3.hi[2] - last == 1) last = b3.hi[2];
+      if (b3.hi[2] - last == 1) last = b3.hi[2];
       int top = last + d.ng3 + X;
       if (top > d.n3e - 1) top = d.n3e - 1;
       if (top >= resident && s + 1 < sw.nslab) break;

@@ -23,6 +23,9 @@
 //     own stream before returning ndt.
 // The kernels are the FP64 path's, compiled the same way (no FMA contraction), so the
 // results equal harm_b200_fluxcalc's.
+#ifndef HARM_FLUXT_MINB
+#define HARM_FLUXT_MINB 2  // the FP64 flux tiles at 2 blocks per SM, as in harm_path_fp64.cu
+#endif
 #include <mutex>
 #include "harm_common.cuh"
 

@@ -6,6 +6,12 @@
 // FMA contraction and the inversion's shared reciprocals (HARM_FP64_FMA_TU): the FP64 path as
 // fast as the compiler makes it, for comparisons of speed (HARM_PREC_FP64_FMA); this build
 // (HARM_PREC_FP64) performs the CPU restatement's IEEE operations in its order.
+// FP64 flux tiles at 2 resident blocks per SM (128 registers; harm_common.cuh): left to
+// itself the compiler can take ~160 registers and 1 block per SM, which halves the resident
+// warps (40.1 ms of flux per substep at 384x192x128 instead of 24.6)
+#ifndef HARM_FLUXT_MINB
+#define HARM_FLUXT_MINB 2
+#endif
 #include <algorithm>
 #include "harm_common.cuh"
 #include "harm_mlp_tc.cuh"
