@@ -81,7 +81,7 @@ def flux_bytes_per_cell(n3: int, precision: int, lim: str = "weno5") -> float:
 # DRAM traffic of the flux stage (k_cellprep and three k_fluxt launches; ncu dram__bytes_read.sum +
 # dram__bytes_write.sum) per active cell, measured on the 192x96x64 torus and scaled to a
 # workload by its cell count
-FLUX_TRAFFIC_PER_CELL = {("weno5", "mixed"): 447.2}
+FLUX_TRAFFIC_PER_CELL = {("weno5", "mixed"): 449.0}
 
 
 def clock_sampler(stop: threading.Event, out: list, dev: int):
