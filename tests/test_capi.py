@@ -44,3 +44,15 @@ def test_grid_setup_matches_reference_rules():
     x1h = g.startx[1] + (6 + 0.25) * g.dx[1]
     assert abs(math.exp(x1h) - g.Rhor) < 1e-12
     assert abs(math.exp(g.startx[1] + 192 * g.dx[1]) - 40.0) < 1e-12
+
+
+def test_host_entry_points_reject_null_arguments():
+    """The multi-step host-buffer step and the mixed reciprocal check their arguments before
+    any CUDA call (so this runs without a GPU): a null context is an error (1) with its text."""
+    import ctypes as C
+    dev = N.device_lib()
+    dt = C.c_double(1e-3)
+    assert dev.harm_b200_step_host_n(None, 1, 0, None, 4, C.byref(dt), None) == 1
+    assert b"null" in dev.harm_b200_last_error()
+    assert dev.harm_b200_mixed_reciprocal(None, None, None, 8) == 1
+    assert dt.value == 1e-3
